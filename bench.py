@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""k-NN benchmark: queries/second on one or more B200s, one JSON line.
+
+Workload (default ``mixture256``): ref_nb = 1,048,576 reference points,
+query_nb = 16,384 queries, dim = 256, k = 100, a seeded Gaussian mixture of
+1024 unit-norm centres (sigma 0.1).  A "step" is one k-NN pass of the query
+batch over the whole reference set.  Inputs are larger than L2 (the
+reference set alone is 1 GiB), so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* ``--impl ours`` (default): ``value`` = device-resident throughput (inputs
+  already in HBM, CUDA events on the launching stream, max over ranks);
+  ``e2e`` = the same metric through the drop-in host entry point
+  ``knn_cuda_global`` with pinned host buffers, every host<->device copy
+  inside the timed region.  ``roofline`` reports the dominant kernel against
+  the FP32 CUDA-core peak measured on the same GPU in the same run.
+  ``cpu_baseline`` = the reference's own knn_c on the host cores (rank 0).
+* ``--impl reference``: the reference's own CPU implementation (knn_c,
+  code/test.cpp:129-175, built from its sources into oracle/_ref) on all
+  host threads, each step a bounded sample of queries over the full
+  reference set.
+
+Multi-GPU: one process per GPU (torchrun); every rank runs its own query
+batch against a replica of the reference set (queries are independent, no
+data-path collective): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "knn-cuda_b200")
+for _p in (PKG, ROOT):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+import workloads  # noqa: E402
+
+METRIC = "kNN queries/sec (N=1M,d=256,k=100): FP32 exact vs BF16+rerank @ recall=1.0"
+UNIT = "queries/s"
+
+# DRAM traffic (read + write bytes) per launch of the dominant kernel, from
+# the ncu capture summarised in profiles/ (None until captured for a kernel).
+NCU_TRAFFIC_BYTES = {}
+
+
+def parse_args(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", default="mixture256", choices=sorted(workloads.WORKLOADS))
+    p.add_argument("--queries", type=int, default=0, help="override query_nb per rank")
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--cpu-seconds", type=float, default=15.0,
+                   help="target CPU time of the bounded knn_c sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+
+    def init(self, backend="nccl"):
+        import torch
+
+        if torch.cuda.is_available():
+            torch.cuda.set_device(self.local_rank)
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            import torch.distributed as dist
+
+            dist.barrier(device_ids=[self.local_rank] if torch.cuda.is_available() else None)
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 9:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        load = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own knn_c (oracle/_ref), all host threads
+# ---------------------------------------------------------------------------
+def cpu_sample_rate(ref, query, k, seconds_target: float, max_rounds: int = 1):
+    """Time the reference knn_c on a bounded query sample; returns
+    (queries/s, threads, sample description, kind)."""
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    fn = oracle.ref_knn_c if kind == "reference" else oracle.knn_c
+    # calibrate with one query per thread
+    qn = min(threads, query.shape[1])
+    t0 = time.perf_counter()
+    fn(ref, np.ascontiguousarray(query[:, :qn]), k, threads=threads)
+    t1 = time.perf_counter() - t0
+    per_round = max(qn, int(qn * max(1.0, seconds_target / max(t1, 1e-3))))
+    per_round = min(per_round, query.shape[1])
+    rates = []
+    for _ in range(max_rounds):
+        t0 = time.perf_counter()
+        fn(ref, np.ascontiguousarray(query[:, :per_round]), k, threads=threads)
+        rates.append(per_round / (time.perf_counter() - t0))
+    desc = (f"first {per_round} queries of the workload against all {ref.shape[1]} reference "
+            f"points, {threads} threads over contiguous query slices; per-query cost is "
+            f"independent of the other queries, so queries/s scales to the full batch")
+    return rates, threads, desc, kind, per_round
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+def run_ours(args, D: Dist):
+    import torch
+
+    import knncuda
+
+    D.init("nccl")
+    dev = torch.device(f"cuda:{D.local_rank}")
+    w = workloads.WORKLOADS[args.workload]
+    qn = args.queries or w.query_nb
+    ref, query = workloads.generate(w, query_nb=qn)
+    dim, N = ref.shape
+    k = w.k
+    # pinned host copies (e2e) and device-resident copies (value)
+    ref_h = torch.from_numpy(ref).pin_memory()
+    qry_h = torch.from_numpy(query).pin_memory()
+    ref_d = ref_h.to(dev)
+    qry_d = qry_h.to(dev)
+    dist_d = torch.empty((k, qn), dtype=torch.float32, device=dev)
+    idx_d = torch.empty((k, qn), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        knncuda.knn_device(ref_d, qry_d, k, "global", dist_d, idx_d, stream)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    if knncuda.sync_status() != 0:
+        raise RuntimeError("device status error during warm-up")
+    fp32_peak = knncuda.measure_fp32_peak(8192)
+
+    clocks = ClockSampler(D.local_rank)
+    D.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    D.barrier()
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    if knncuda.sync_status() != 0:
+        raise RuntimeError("device status error in timed region")
+    ms_step = D.max(ms_total / args.steps)
+
+    # end to end through the drop-in host entry point (pinned buffers)
+    ref_np, qry_np = ref_h.numpy(), qry_h.numpy()
+    out_d = torch.empty((k, qn), dtype=torch.float32).pin_memory().numpy()
+    out_i = torch.empty((k, qn), dtype=torch.int32).pin_memory().numpy()
+    knncuda.knn_cuda_global(ref_np, N, qry_np, qn, dim, k, out_d, out_i)   # warm (allocs)
+    D.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        if not knncuda.knn_cuda_global(ref_np, N, qry_np, qn, dim, k, out_d, out_i):
+            raise RuntimeError("knn_cuda_global failed")
+    e2e_s = D.max((time.perf_counter() - t0) / args.e2e_steps)
+    # the device-resident and host paths must agree
+    if not (np.array_equal(out_i, idx_d.cpu().numpy()) and
+            np.array_equal(out_d, dist_d.cpu().numpy())):
+        raise RuntimeError("host entry point and device path disagree")
+
+    splits = knncuda.plan_splits(N, qn, dim, k)
+    launches_per_step = 1 + (1 if splits > 1 else 0)
+    flops = 3.0 * dim * N * qn          # sub + mul + add per pair-dimension
+    achieved = flops / (ms_step * 1e-3)
+    value = D.world * qn / (ms_step * 1e-3)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D.world,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian mixture, 1024 unit-norm centres, sigma 0.1)",
+        "impl": "ours",
+        "config": dict(w.describe(), query_nb=qn, tier="exact-fp32 (knn_cuda_global path)",
+                       parallelism=f"query-sharded replicas x{D.world}",
+                       l2="inputs larger than L2 (1 GiB reference set); no flush"),
+        "e2e": {"value": D.world * qn / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": int(ref.nbytes + query.nbytes),
+                "d2h_bytes_per_step": int(out_d.nbytes + out_i.nbytes),
+                "api": "knn_cuda_global (drop-in C-ABI, pinned host buffers)",
+                "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved / 1e12,
+                     "peak": fp32_peak / 1e12, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak if fp32_peak > 0 else None,
+                     "traffic": NCU_TRAFFIC_BYTES.get("knn_exact_kernel"),
+                     "kernel": "knn_exact_kernel<8,128>",
+                     "algorithmic": "3*dim flops per (query, reference) pair",
+                     "peak_source": "FP32 FMA throughput measured in this run "
+                                    "(knnb200_measure_fp32_peak, 2 flops per FMA)"},
+        "clocks": clk,
+    }
+    if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
+        rates, threads, desc, kind, qs = cpu_sample_rate(ref, query, k, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rates[0], "unit": UNIT, "cores": threads,
+                                "kind": kind, "sample": desc}
+    if D.rank == 0:
+        print(json.dumps(line), flush=True)
+    D.close()
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU implementation on all host threads
+# ---------------------------------------------------------------------------
+def run_reference(args, D: Dist):
+    if D.rank != 0:
+        return
+    from oracle import oracle
+
+    w = workloads.WORKLOADS[args.workload]
+    qn = args.queries or w.query_nb
+    ref, query = workloads.generate(w, query_nb=qn)
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    fn = oracle.ref_knn_c if kind == "reference" else oracle.knn_c
+    # each step: a bounded sample of queries sized to about cpu_seconds / 3
+    qs = min(threads, qn)
+    t0 = time.perf_counter()
+    fn(ref, np.ascontiguousarray(query[:, :qs]), w.k, threads=threads)
+    t1 = time.perf_counter() - t0
+    per_step = min(qn, max(qs, int(qs * max(1.0, (args.cpu_seconds / 3) / max(t1, 1e-3)))))
+    sample = np.ascontiguousarray(query[:, :per_step])
+    for _ in range(args.warmup):
+        fn(ref, sample, w.k, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        fn(ref, sample, w.k, threads=threads)
+        times.append(time.perf_counter() - t0)
+    s = sum(times) / len(times)
+    value = per_step / s
+    desc = (f"{per_step} queries per step against all {ref.shape[1]} reference points, "
+            f"{threads} threads over contiguous query slices (reference knn_c, "
+            f"code/test.cpp:129-175)")
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": dict(w.describe(), query_nb=qn, sample_queries_per_step=per_step),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    D = Dist()
+    if args.impl == "reference":
+        run_reference(args, D)
+    else:
+        run_ours(args, D)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,97 @@
+/*
+ * knn_b200.h -- C ABI of libknnb200.so (extern "C", plain pointers and sizes).
+ *
+ * Layout conventions (the reference's, README.md "Data storage"):
+ *   a point set of n points in dim dimensions is a dim x n row-major FP32
+ *   array, x[d*ld + i] with ld >= n (ld = n for the host entry points);
+ *   results are k x query_nb row-major, dist[j*out_ld + i], index likewise,
+ *   ascending distance with ties ordered by ascending index.
+ *
+ * Return codes of the int-returning functions: KNNB200_OK (0) or one of the
+ * KNNB200_E* codes below; knnb200_status_string() names them.
+ */
+#ifndef KNNB200_KNN_B200_H
+#define KNNB200_KNN_B200_H
+
+#include <stddef.h>
+
+#ifndef KNNB200_API
+#define KNNB200_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KNNB200_OK 0
+#define KNNB200_EINVAL 1        /* invalid argument (sizes, k, pointers, alignment) */
+#define KNNB200_ENODEV 2        /* no CUDA device */
+#define KNNB200_ENOMEM 3        /* device allocation failed */
+#define KNNB200_ELAUNCH 4       /* kernel launch failed */
+#define KNNB200_ETIMEOUT 5      /* a kernel wait hit its time limit and returned early */
+#define KNNB200_ECUDA 6         /* other CUDA runtime error */
+#define KNNB200_EUNSUPPORTED 7  /* shape not supported by the requested method */
+#define KNNB200_ESCRATCH 8      /* caller-provided scratch too small */
+#define KNNB200_ETENSORMAP 9    /* TMA descriptor could not be encoded */
+
+/* Methods for the device entry points. */
+#define KNNB200_METHOD_GLOBAL 0   /* fused exact FP32 direct form (knn_cuda_global) */
+#define KNNB200_METHOD_TEXTURE 1  /* same kernel as GLOBAL (knn_cuda_texture) */
+#define KNNB200_METHOD_CUBLAS 2   /* expansion method (knn_cublas) */
+
+/* C-linkage aliases of the three drop-in entry points of knncuda.h.
+ * Replace knn_cuda_global / knn_cuda_texture / knn_cublas,
+ * code/knncuda.h:14-21, :37-44, :61-68; identical arguments and semantics
+ * (bool result as int: 1 success, 0 failure with "ERROR: ..." on stdout). */
+KNNB200_API int knnb200_cuda_global(const float *ref, int ref_nb, const float *query, int query_nb,
+                        int dim, int k, float *knn_dist, int *knn_index);
+KNNB200_API int knnb200_cuda_texture(const float *ref, int ref_nb, const float *query, int query_nb,
+                         int dim, int k, float *knn_dist, int *knn_index);
+KNNB200_API int knnb200_cublas(const float *ref, int ref_nb, const float *query, int query_nb, int dim,
+                   int k, float *knn_dist, int *knn_index);
+
+/* Device-resident variant of the same computation: every pointer is device
+ * memory on the current device, work is queued on `stream` (a cudaStream_t,
+ * NULL = legacy default stream) and the call returns without synchronising.
+ * It replaces the compute part of the reference host bodies
+ * (code/knncuda.cu:352-394 and :709-805) for callers whose data already
+ * lives in HBM.  ref_ld / query_ld are row pitches in elements (multiples of
+ * 4, base pointers 16-byte aligned); out_ld >= query_nb.  Scratch comes from
+ * a per-device library workspace (grown with cudaMalloc when needed, so the
+ * first call of a new size may synchronise the device); consecutive calls on
+ * one device are ordered by the library so they never share scratch.
+ * Device-side status (a timed-out wait) is reported by knnb200_sync_status. */
+KNNB200_API int knnb200_knn_device(const float *ref, int ref_nb, long long ref_ld, const float *query,
+                       int query_nb, long long query_ld, int dim, int k, int method,
+                       float *knn_dist, int *knn_index, long long out_ld, void *stream);
+
+/* Synchronise `stream` and return the status of the last device-resident
+ * call on the current device (KNNB200_OK or KNNB200_ETIMEOUT / ECUDA). */
+KNNB200_API int knnb200_sync_status(void *stream);
+
+/* Bytes of scratch the device entry point needs for this shape and method. */
+KNNB200_API size_t knnb200_scratch_bytes(int ref_nb, int query_nb, int dim, int k, int method);
+
+/* Number of reference splits the exact kernel uses for this shape. */
+KNNB200_API int knnb200_plan_splits(int ref_nb, int query_nb, int dim, int k);
+
+/* Free the current device's workspace (the next call re-allocates). */
+KNNB200_API void knnb200_release_workspace(void);
+
+/* Human-readable name of a KNNB200_* code. */
+KNNB200_API const char *knnb200_status_string(int code);
+
+/* Calibration: FP32 CUDA-core multiply-add throughput of the current device
+ * in FLOP/s (2 flops per multiply-add), measured by a packed-FMA kernel of
+ * `iters` inner iterations on `stream`; synchronises; -1 on error.  Used as
+ * the roofline denominator of the FP32 direct-form path. */
+KNNB200_API double knnb200_measure_fp32_peak(int iters, void *stream);
+
+/* Library version string. */
+KNNB200_API const char *knnb200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KNNB200_KNN_B200_H */

@@ -1,0 +1,490 @@
+// knn_exact.cu -- fused exact FP32 k-NN (direct form) for sm_100a.
+//
+// Replaces the reference chain compute_distances (code/knncuda.cu:20-91) ->
+// modified_insertion_sort (:143-189) -> compute_sqrt (:200-205) with ONE
+// kernel: the ref_nb x query_nb distance matrix never reaches HBM.
+//
+//   * A CTA owns BQ queries (one query tile) and one contiguous slice
+//     ("split") of the reference set.  Reference tiles of 256 points x 16
+//     dimensions and the matching 16 x BQ query slab are brought into shared
+//     memory by TMA (one producer warp, a 4-stage mbarrier ring).
+//   * 8 consumer warps; warp w owns QPW queries, lane l owns the 8
+//     reference points {4l..4l+3, 128+4l..128+4l+3} of each tile, so every
+//     lane accumulates a QPW x 8 block of squared distances in registers as
+//     sum_d (r_d - q_d)^2 with one rounding per sub and one fused
+//     multiply-add per dimension, in increasing d -- the arithmetic and
+//     order of the reference's compute_distances inner loop
+//     (code/knncuda.cu:77-80), so squared distances are bit-identical to it.
+//   * Selection is warp-local.  Each query keeps its k smallest
+//     (distance, index) keys sorted in shared memory and a threshold tau =
+//     the k-th key in registers.  After each half tile the warp ballots the
+//     keys below tau into a candidate buffer and merges them into the list by
+//     rank counting (no sort network).  Ordering by the 64-bit key
+//     (distance bits, index) reproduces the reference's tie rule: equal
+//     distances keep the lower index (code/knncuda.cu:172, :178).
+//   * With one split the kernel writes sqrt(distance) and the index straight
+//     into the k x query_nb output; with several splits it writes each
+//     split's sorted keys to scratch and knn_merge_splits_kernel merges them.
+#include <algorithm>
+#include <cstdio>
+
+#include "knn_common.cuh"
+#include "knn_kernels.h"
+
+namespace knnb200 {
+
+constexpr int EX_BR = 256;       // reference points per tile
+constexpr int EX_BD = 16;        // dimensions per pipeline stage
+constexpr int EX_CB = 128;       // candidate slots per query (one half tile)
+constexpr int EX_WARPS = 8;      // consumer warps
+constexpr int EX_THREADS = (EX_WARPS + 1) * 32;
+constexpr int EX_STAGES = 4;
+
+template <int QPW, int KCAP>
+struct ExCfg {
+    static constexpr int BQ = QPW * EX_WARPS;
+    static constexpr int Q_FLOATS = EX_BD * BQ;
+    static constexpr int R_FLOATS = EX_BD * EX_BR;
+    static constexpr int STAGE_FLOATS = Q_FLOATS + R_FLOATS;
+    static constexpr int STAGE_BYTES = STAGE_FLOATS * 4;
+    static constexpr int REGION = KCAP + EX_CB;   // keys per query: list + candidates
+    static constexpr size_t LIST_BYTES = (size_t)BQ * REGION * 8;
+    static constexpr size_t BAR_OFFSET = (size_t)EX_STAGES * STAGE_BYTES + LIST_BYTES;
+    static constexpr size_t SMEM = 1024 + BAR_OFFSET + 2 * EX_STAGES * 8 + 16;
+    static_assert(STAGE_BYTES % 1024 == 0, "stage alignment");
+    static_assert(KCAP % 32 == 0 && (KCAP & (KCAP - 1)) == 0, "KCAP power of two >= 32");
+};
+
+KNN_DI void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(EX_WARPS * 32) : "memory"); }
+
+// Number of elements of the sorted array L[0..n) (n a power of two) below x.
+template <int n>
+KNN_DI int rank_pow2(const unsigned long long *L, unsigned long long x) {
+    int pos = 0;
+#pragma unroll
+    for (int step = n / 2; step >= 1; step >>= 1)
+        if (L[pos + step - 1] < x) pos += step;
+    return pos + (L[pos] < x ? 1 : 0);
+}
+
+// Merge c unsorted candidate keys (L[KCAP .. KCAP+c)) into the sorted list
+// L[0..k) held by one warp.  Every key's final position is its rank in the
+// union: list element at p -> p + #(candidates below it); candidate x ->
+// #(list below x) + #(candidates below x).  Keys are unique (distinct
+// indices), so the positions form a permutation; positions >= k are dropped.
+template <int KCAP>
+KNN_DI void warp_merge(unsigned long long *L, int c, int k, int lane) {
+    constexpr int LPL = KCAP / 32;
+    constexpr int CPL = EX_CB / 32;
+    const unsigned long long *C = L + KCAP;
+    unsigned long long lv[LPL], cv[CPL];
+    int lp[LPL], cp[CPL];
+#pragma unroll
+    for (int a = 0; a < LPL; ++a) {
+        lv[a] = L[a * 32 + lane];
+        lp[a] = a * 32 + lane;
+    }
+#pragma unroll
+    for (int b = 0; b < CPL; ++b) {
+        const int t = b * 32 + lane;
+        cv[b] = t < c ? C[t] : kKeyInf;
+        cp[b] = rank_pow2<KCAP>(L, cv[b]);
+    }
+    for (int t = 0; t < c; ++t) {
+        const unsigned long long x = C[t];
+#pragma unroll
+        for (int a = 0; a < LPL; ++a) lp[a] += x < lv[a] ? 1 : 0;
+#pragma unroll
+        for (int b = 0; b < CPL; ++b) cp[b] += x < cv[b] ? 1 : 0;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int a = 0; a < LPL; ++a)
+        if (lp[a] < k) L[lp[a]] = lv[a];
+#pragma unroll
+    for (int b = 0; b < CPL; ++b)
+        if (b * 32 + lane < c && cp[b] < k) L[cp[b]] = cv[b];
+    __syncwarp();
+}
+
+// Filter one half tile (4 reference points per lane) against each query's
+// threshold, append survivors to the candidate buffers and merge.
+// d2(i, j) gives the squared distance of query i to the lane's j-th point.
+template <int QPW, int KCAP, typename D2>
+KNN_DI void select_half(unsigned long long *wl, unsigned long long (&tau)[QPW], D2 d2,
+                        uint32_t rbase, int N, int k, int lane) {
+    constexpr int REGION = KCAP + EX_CB;
+    uint32_t pm[QPW];
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) {
+        pm[i] = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t idx = rbase + j;
+            const bool p = (idx < (uint32_t)N) && make_key(d2(i, j), idx) < tau[i];
+            pm[i] |= (p ? 1u : 0u) << j;
+            any |= p;
+        }
+    }
+    if (!__any_sync(0xffffffffu, any)) return;
+    const unsigned lt = (1u << lane) - 1u;
+    int cnt[QPW];
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) {
+        unsigned long long *cb = wl + i * REGION + KCAP;
+        int c = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const bool p = (pm[i] >> j) & 1u;
+            const unsigned m = __ballot_sync(0xffffffffu, p);
+            if (p) cb[c + __popc(m & lt)] = make_key(d2(i, j), rbase + j);
+            c += __popc(m);
+        }
+        cnt[i] = c;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) {
+        if (cnt[i] > 0) {
+            unsigned long long *L = wl + i * REGION;
+            warp_merge<KCAP>(L, cnt[i], k, lane);
+            tau[i] = L[k - 1];
+        }
+    }
+}
+
+template <int QPW, int KCAP>
+__global__ void __launch_bounds__(EX_THREADS, 1)
+    knn_exact_kernel(const __grid_constant__ CUtensorMap tm_ref,
+                     const __grid_constant__ CUtensorMap tm_qry, ExactArgs a) {
+    using C = ExCfg<QPW, KCAP>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    float *stages = reinterpret_cast<float *>(base);
+    unsigned long long *lists =
+        reinterpret_cast<unsigned long long *>(base + (size_t)EX_STAGES * C::STAGE_BYTES);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + C::BAR_OFFSET);
+    uint64_t *empty = full + EX_STAGES;
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + EX_STAGES);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qtile = blockIdx.x, split = blockIdx.y;
+    const int t0 = (int)((long long)a.n_rtiles * split / a.n_splits);
+    const int t1 = (int)((long long)a.n_rtiles * (split + 1) / a.n_splits);
+    const int total = (t1 - t0) * a.n_dchunks;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < EX_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], EX_WARPS);
+        }
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    if (warp == EX_WARPS) {
+        // ---------------- producer warp: one thread issues all TMA loads ----
+        if (lane == 0) {
+            prefetch_tensormap(&tm_ref);
+            prefetch_tensormap(&tm_qry);
+            int issued = 0;
+            for (int it = 0; it < total; ++it) {
+                const int s = it % EX_STAGES;
+                if (it >= EX_STAGES && !mbar_wait(&empty[s], ((it / EX_STAGES) - 1) & 1)) {
+                    atomicMax(a.status, (int)kDevTimeoutEmpty);
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*abort_flag) break;
+                float *qs = stages + (size_t)s * C::STAGE_FLOATS;
+                float *rs = qs + C::Q_FLOATS;
+                const int rt = t0 + it / a.n_dchunks, dc = it % a.n_dchunks;
+                mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
+                tma_load_2d(qs, &tm_qry, &full[s], qtile * C::BQ, dc * EX_BD);
+                tma_load_2d(rs, &tm_ref, &full[s], rt * EX_BR, dc * EX_BD);
+                issued = it + 1;
+            }
+            // Never leave with copies in flight: wait for the last issued stages.
+            for (int it = max(0, issued - EX_STAGES); it < issued; ++it)
+                if (!mbar_wait(&full[it % EX_STAGES], (it / EX_STAGES) & 1))
+                    atomicMax(a.status, (int)kDevTimeoutDrain);
+        }
+        return;
+    }
+
+    // -------------------- consumer warps ------------------------------------
+    unsigned long long *wl = lists + (size_t)warp * QPW * C::REGION;
+    for (int i = lane; i < QPW * C::REGION; i += 32) wl[i] = kKeyInf;
+    __syncwarp();
+    unsigned long long tau[QPW];
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) tau[i] = kKeyInf;
+
+    int it = 0;
+    bool alive = true;
+    for (int rt = t0; rt < t1 && alive; ++rt) {
+        f32x2_t acc[QPW][4];
+#pragma unroll
+        for (int i = 0; i < QPW; ++i)
+#pragma unroll
+            for (int p = 0; p < 4; ++p) acc[i][p] = 0ull;
+
+        for (int dc = 0; dc < a.n_dchunks; ++dc, ++it) {
+            const int s = it % EX_STAGES;
+            const bool got = mbar_wait(&full[s], (it / EX_STAGES) & 1);
+            // warp-uniform decision: every lane leaves together or none does
+            const bool timed_out = __any_sync(0xffffffffu, !got);
+            if (timed_out || __any_sync(0xffffffffu, *abort_flag != 0)) {
+                if (lane == 0) {
+                    if (timed_out) atomicMax(a.status, (int)kDevTimeoutFull);
+                    *abort_flag = 1;
+                }
+                alive = false;
+                break;
+            }
+            const float *qs = stages + (size_t)s * C::STAGE_FLOATS + warp * QPW;
+            const float *rs = stages + (size_t)s * C::STAGE_FLOATS + C::Q_FLOATS + lane * 4;
+#pragma unroll
+            for (int dd = 0; dd < EX_BD; ++dd) {
+                const float4 ra = *reinterpret_cast<const float4 *>(rs + dd * EX_BR);
+                const float4 rb = *reinterpret_cast<const float4 *>(rs + dd * EX_BR + 128);
+                float qv[QPW];
+#pragma unroll
+                for (int i = 0; i < QPW; i += 4) {
+                    const float4 q4 = *reinterpret_cast<const float4 *>(qs + dd * C::BQ + i);
+                    qv[i] = q4.x;
+                    qv[i + 1] = q4.y;
+                    qv[i + 2] = q4.z;
+                    qv[i + 3] = q4.w;
+                }
+                const f32x2_t r0 = f2_pack(ra.x, ra.y), r1 = f2_pack(ra.z, ra.w);
+                const f32x2_t r2 = f2_pack(rb.x, rb.y), r3 = f2_pack(rb.z, rb.w);
+#pragma unroll
+                for (int i = 0; i < QPW; ++i) {
+                    const f32x2_t qq = f2_pack(qv[i], qv[i]);
+                    f32x2_t t;
+                    t = f2_sub(r0, qq); acc[i][0] = f2_fma(t, t, acc[i][0]);
+                    t = f2_sub(r1, qq); acc[i][1] = f2_fma(t, t, acc[i][1]);
+                    t = f2_sub(r2, qq); acc[i][2] = f2_fma(t, t, acc[i][2]);
+                    t = f2_sub(r3, qq); acc[i][3] = f2_fma(t, t, acc[i][3]);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        }
+        if (!alive) break;
+
+        const uint32_t rb0 = (uint32_t)rt * EX_BR + lane * 4;
+        select_half<QPW, KCAP>(
+            wl, tau,
+            [&](int i, int j) {
+                return (j & 1) ? f2_hi(acc[i][j >> 1]) : f2_lo(acc[i][j >> 1]);
+            },
+            rb0, a.N, a.k, lane);
+        select_half<QPW, KCAP>(
+            wl, tau,
+            [&](int i, int j) {
+                return (j & 1) ? f2_hi(acc[i][2 + (j >> 1)]) : f2_lo(acc[i][2 + (j >> 1)]);
+            },
+            rb0 + 128, a.N, a.k, lane);
+    }
+
+    consumer_sync();
+    if (*abort_flag) return;
+
+    const int q0 = qtile * C::BQ;
+    if (a.n_splits == 1) {
+        // Epilogue: sqrt and the reference's k x query_nb layout, coalesced
+        // along queries.
+        for (int e = threadIdx.x; e < a.k * C::BQ; e += EX_WARPS * 32) {
+            const int j = e / C::BQ, qi = e - j * C::BQ, q = q0 + qi;
+            if (q < a.Q) {
+                const unsigned long long key = lists[(size_t)qi * C::REGION + j];
+                a.out_dist[(size_t)j * a.ld_out + q] = sqrtf(key_dist2(key));
+                a.out_idx[(size_t)j * a.ld_out + q] = key_index(key);
+            }
+        }
+    } else {
+        for (int i = 0; i < QPW; ++i) {
+            const int q = q0 + warp * QPW + i;
+            if (q >= a.Q) break;
+            unsigned long long *dst = a.part + ((size_t)split * a.Q + q) * a.k;
+            for (int j = lane; j < a.k; j += 32) dst[j] = wl[i * C::REGION + j];
+        }
+    }
+}
+
+// Number of elements of sorted A[0..n) below x.
+KNN_DI int rank_sorted(const unsigned long long *A, int n, unsigned long long x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (A[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Merge the per-split sorted key lists of each query (one warp per query).
+// An element's output position is the sum of its ranks in every list.
+__global__ void knn_merge_splits_kernel(const unsigned long long *__restrict__ part, int S,
+                                        int Q, int k, float *__restrict__ out_dist,
+                                        int *__restrict__ out_idx, long long ld_out) {
+    extern __shared__ unsigned long long msm[];
+    const int wpb = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * wpb + warp;
+    if (q >= Q) return;
+    unsigned long long *L = msm + (size_t)warp * S * k;
+    for (int e = lane; e < S * k; e += 32) {
+        const int t = e / k, j = e - t * k;
+        L[e] = part[((size_t)t * Q + q) * k + j];
+    }
+    __syncwarp();
+    for (int e = lane; e < S * k; e += 32) {
+        const int t = e / k, j = e - t * k;
+        const unsigned long long x = L[e];
+        int pos = j;
+        for (int u = 0; u < S && pos < k; ++u)
+            if (u != t) pos += rank_sorted(L + (size_t)u * k, k, x);
+        if (pos < k) {
+            out_dist[(size_t)pos * ld_out + q] = sqrtf(key_dist2(x));
+            out_idx[(size_t)pos * ld_out + q] = key_index(x);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+struct ExactShape {
+    int qpw, kcap, bq, splits, n_rtiles, n_dchunks;
+    size_t smem;
+};
+
+template <int QPW, int KCAP>
+void shape_of(ExactShape &s) {
+    using C = ExCfg<QPW, KCAP>;
+    s.qpw = QPW;
+    s.kcap = KCAP;
+    s.bq = C::BQ;
+    s.smem = C::SMEM;
+}
+
+bool choose_shape(int N, int Q, int d, int k, int num_sms, ExactShape &s) {
+    if (k <= 32) shape_of<8, 32>(s);
+    else if (k <= 64) shape_of<8, 64>(s);
+    else if (k <= 128) shape_of<8, 128>(s);
+    else if (k <= 256) shape_of<4, 256>(s);
+    else return false;
+    s.n_rtiles = (N + EX_BR - 1) / EX_BR;
+    s.n_dchunks = (d + EX_BD - 1) / EX_BD;
+    const int qtiles = (Q + s.bq - 1) / s.bq;
+    // Split the reference set so that the grid fills whole waves of one CTA
+    // per SM.  Modelled time: waves x (tiles per split + fixed selection
+    // warm-up cost of about 256/d tiles per split).
+    const double warm = 256.0 / (s.n_dchunks * EX_BD);
+    int best = 1;
+    double best_t = 1e300;
+    int max_s = std::min(s.n_rtiles, 64);
+    // keep the per-split partial lists under 1 GiB of scratch
+    const long long per_split = (long long)Q * k * 8;
+    max_s = (int)std::max<long long>(1, std::min<long long>(max_s, (1ll << 30) / per_split));
+    for (int S = 1; S <= max_s; ++S) {
+        const long long ctas = (long long)qtiles * S;
+        const long long waves = (ctas + num_sms - 1) / num_sms;
+        const double t = (double)waves * ((double)s.n_rtiles / S + warm);
+        if (t < best_t * 0.999) {
+            best_t = t;
+            best = S;
+        }
+    }
+    s.splits = best;
+    return true;
+}
+
+template <int QPW, int KCAP>
+cudaError_t launch_t(const CUtensorMap &mr, const CUtensorMap &mq, const ExactArgs &a,
+                     int qtiles, cudaStream_t st) {
+    using C = ExCfg<QPW, KCAP>;
+    auto kern = knn_exact_kernel<QPW, KCAP>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)C::SMEM);
+    if (e != cudaSuccess) return e;
+    dim3 grid(qtiles, a.n_splits);
+    kern<<<grid, EX_THREADS, C::SMEM, st>>>(mr, mq, a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
+    ExactShape s;
+    if (!choose_shape(N, Q, d, k, num_sms, s)) return 0;
+    return s.splits > 1 ? (size_t)s.splits * Q * k * sizeof(unsigned long long) : 0;
+}
+
+bool exact_supported_k(int k) { return k >= 1 && k <= 256; }
+
+int launch_exact(const ExactProblem &p, cudaStream_t st) {
+    ExactShape s;
+    if (!choose_shape(p.N, p.Q, p.d, p.k, p.num_sms, s)) return kErrUnsupported;
+    if (p.force_splits > 0) s.splits = std::min(p.force_splits, s.n_rtiles);
+    const size_t need = s.splits > 1 ? (size_t)s.splits * p.Q * p.k * 8 : 0;
+    if (need > p.scratch_bytes) return kErrScratch;
+
+    CUtensorMap mr, mq;
+    if (!encode_f32_2d(&mr, p.ref, (uint64_t)p.N, (uint64_t)p.d, (uint64_t)p.ldr, EX_BR, EX_BD))
+        return kErrTensorMap;
+    if (!encode_f32_2d(&mq, p.qry, (uint64_t)p.Q, (uint64_t)p.d, (uint64_t)p.ldq, s.bq, EX_BD))
+        return kErrTensorMap;
+
+    ExactArgs a;
+    a.N = p.N;
+    a.Q = p.Q;
+    a.d = p.d;
+    a.k = p.k;
+    a.n_rtiles = s.n_rtiles;
+    a.n_splits = s.splits;
+    a.n_dchunks = s.n_dchunks;
+    a.out_dist = p.out_dist;
+    a.out_idx = p.out_idx;
+    a.ld_out = p.ld_out;
+    a.part = static_cast<unsigned long long *>(p.scratch);
+    a.status = p.status;
+    const int qtiles = (p.Q + s.bq - 1) / s.bq;
+
+    cudaError_t e;
+    switch (s.kcap) {
+        case 32: e = launch_t<8, 32>(mr, mq, a, qtiles, st); break;
+        case 64: e = launch_t<8, 64>(mr, mq, a, qtiles, st); break;
+        case 128: e = launch_t<8, 128>(mr, mq, a, qtiles, st); break;
+        default: e = launch_t<4, 256>(mr, mq, a, qtiles, st); break;
+    }
+    if (e != cudaSuccess) return kErrLaunch;
+    if (s.splits > 1) {
+        const size_t per_warp = (size_t)s.splits * p.k * 8;
+        int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (160u * 1024u) / per_warp));
+        const size_t smem = per_warp * wpb;
+        if (smem > 200u * 1024u) return kErrUnsupported;
+        e = cudaFuncSetAttribute(knn_merge_splits_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return kErrLaunch;
+        knn_merge_splits_kernel<<<(p.Q + wpb - 1) / wpb, wpb * 32, smem, st>>>(
+            a.part, s.splits, p.Q, p.k, p.out_dist, p.out_idx, p.ld_out);
+        if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    }
+    return kOk;
+}
+
+int exact_plan_splits(int N, int Q, int d, int k, int num_sms) {
+    ExactShape s;
+    return choose_shape(N, Q, d, k, num_sms, s) ? s.splits : 0;
+}
+
+}  // namespace knnb200

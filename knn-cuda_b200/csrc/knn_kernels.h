@@ -1,0 +1,65 @@
+// knn_kernels.h -- internal interface between the host runtime (knn_api.cu)
+// and the kernels.  Not installed; the public C-ABI is include/knn_b200.h.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace knnb200 {
+
+// Internal result codes (mirrored by the public KNNB200_* codes).
+enum Result : int {
+    kOk = 0,
+    kErrInvalid = 1,
+    kErrNoDevice = 2,
+    kErrNoMemory = 3,
+    kErrLaunch = 4,
+    kErrDeviceTimeout = 5,
+    kErrCuda = 6,
+    kErrUnsupported = 7,
+    kErrScratch = 8,
+    kErrTensorMap = 9,
+};
+
+// Kernel-side arguments of the fused exact kernel.
+struct ExactArgs {
+    int N, Q, d, k;
+    int n_rtiles, n_splits, n_dchunks;
+    float *out_dist;
+    int *out_idx;
+    long long ld_out;
+    unsigned long long *part;   // [n_splits][Q][k] keys when n_splits > 1
+    int *status;                // device status word (DeviceStatus)
+};
+
+// One exact k-NN problem on device-resident, dim x n row-major inputs.
+struct ExactProblem {
+    const float *ref;   // [d][ldr]
+    int N;
+    long long ldr;
+    const float *qry;   // [d][ldq]
+    int Q;
+    long long ldq;
+    int d, k;
+    float *out_dist;    // [k][ld_out]
+    int *out_idx;
+    long long ld_out;
+    void *scratch;
+    size_t scratch_bytes;
+    int *status;
+    int num_sms;
+    int force_splits;   // 0 = automatic
+};
+
+// Encode a 2-D FP32 tensor map (cols = contiguous axis) with zero OOB fill.
+bool encode_f32_2d(CUtensorMap *map, const void *base, uint64_t cols, uint64_t rows,
+                   uint64_t ld_elems, uint32_t box_cols, uint32_t box_rows);
+
+bool exact_supported_k(int k);
+size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms);
+int exact_plan_splits(int N, int Q, int d, int k, int num_sms);
+int launch_exact(const ExactProblem &p, cudaStream_t st);
+
+}  // namespace knnb200

@@ -1,0 +1,207 @@
+"""Python mirror of the reference interface (code/knncuda.h) over libknnb200.so.
+
+The three functions keep the reference's names, argument order and meaning
+and its error behaviour (a bool result; "ERROR: ..." printed by the library
+on failure):
+
+    knn_cuda_global(ref, ref_nb, query, query_nb, dim, k, knn_dist, knn_index) -> bool
+    knn_cuda_texture(...) -> bool
+    knn_cublas(...) -> bool
+
+``ref`` / ``query`` are float32 arrays holding dim x n row-major points
+(``x[d, i]``, README.md "Data storage"); ``knn_dist`` (float32) and
+``knn_index`` (int32) are preallocated k x query_nb outputs, filled in place.
+
+``knn_device`` is the device-resident path (torch CUDA tensors, no host
+copies, asynchronous on the given stream).
+
+There is no CPU fallback: if libknnb200.so is missing, importing the
+library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libknnb200.so")
+
+METHOD_GLOBAL = 0
+METHOD_TEXTURE = 1
+METHOD_CUBLAS = 2
+METHODS = {"global": METHOD_GLOBAL, "texture": METHOD_TEXTURE, "cublas": METHOD_CUBLAS}
+
+_FP = ctypes.POINTER(ctypes.c_float)
+_IP = ctypes.POINTER(ctypes.c_int)
+_lib = None
+
+# Every extern "C" symbol of include/knn_b200.h and the three C++-linkage
+# symbols of include/knncuda.h.
+C_SYMBOLS = (
+    "knnb200_cuda_global", "knnb200_cuda_texture", "knnb200_cublas", "knnb200_knn_device",
+    "knnb200_sync_status", "knnb200_scratch_bytes", "knnb200_plan_splits",
+    "knnb200_release_workspace", "knnb200_status_string", "knnb200_version",
+    "knnb200_measure_fp32_peak",
+)
+CXX_SYMBOLS = (
+    "_Z15knn_cuda_globalPKfiS0_iiiPfPi",
+    "_Z16knn_cuda_texturePKfiS0_iiiPfPi",
+    "_Z10knn_cublasPKfiS0_iiiPfPi",
+)
+
+
+def lib():
+    """Load libknnb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libknnb200.so not built ({LIB_PATH}); run make -C knn-cuda_b200")
+        L = ctypes.CDLL(LIB_PATH)
+        host_args = [_FP, ctypes.c_int, _FP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _FP, _IP]
+        for name in ("knnb200_cuda_global", "knnb200_cuda_texture", "knnb200_cublas"):
+            fn = getattr(L, name)
+            fn.restype = ctypes.c_int
+            fn.argtypes = host_args
+        L.knnb200_knn_device.restype = ctypes.c_int
+        L.knnb200_knn_device.argtypes = [
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int,
+            ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p]
+        L.knnb200_sync_status.restype = ctypes.c_int
+        L.knnb200_sync_status.argtypes = [ctypes.c_void_p]
+        L.knnb200_scratch_bytes.restype = ctypes.c_size_t
+        L.knnb200_scratch_bytes.argtypes = [ctypes.c_int] * 5
+        L.knnb200_plan_splits.restype = ctypes.c_int
+        L.knnb200_plan_splits.argtypes = [ctypes.c_int] * 4
+        L.knnb200_release_workspace.restype = None
+        L.knnb200_release_workspace.argtypes = []
+        L.knnb200_status_string.restype = ctypes.c_char_p
+        L.knnb200_status_string.argtypes = [ctypes.c_int]
+        L.knnb200_measure_fp32_peak.restype = ctypes.c_double
+        L.knnb200_measure_fp32_peak.argtypes = [ctypes.c_int, ctypes.c_void_p]
+        L.knnb200_version.restype = ctypes.c_char_p
+        L.knnb200_version.argtypes = []
+        _lib = L
+    return _lib
+
+
+def _check_host(ref, ref_nb, query, query_nb, dim, k, knn_dist, knn_index):
+    for name, a, dt in (("ref", ref, np.float32), ("query", query, np.float32),
+                        ("knn_dist", knn_dist, np.float32), ("knn_index", knn_index, np.int32)):
+        if not isinstance(a, np.ndarray) or a.dtype != dt or not a.flags["C_CONTIGUOUS"]:
+            raise TypeError(f"{name} must be a C-contiguous numpy {np.dtype(dt).name} array")
+    if ref.size < dim * ref_nb or query.size < dim * query_nb:
+        raise ValueError("ref/query arrays are smaller than dim x n")
+    if knn_dist.size < k * query_nb or knn_index.size < k * query_nb:
+        raise ValueError("output arrays are smaller than k x query_nb")
+    if not knn_dist.flags["WRITEABLE"] or not knn_index.flags["WRITEABLE"]:
+        raise ValueError("outputs must be writeable")
+
+
+def _host_call(name, ref, ref_nb, query, query_nb, dim, k, knn_dist, knn_index) -> bool:
+    if min(ref_nb, query_nb, dim, k) >= 1:
+        _check_host(ref, ref_nb, query, query_nb, dim, k, knn_dist, knn_index)
+    fn = getattr(lib(), name)
+    p = lambda a, t: a.ctypes.data_as(t) if isinstance(a, np.ndarray) else None
+    return bool(fn(p(ref, _FP), ref_nb, p(query, _FP), query_nb, dim, k, p(knn_dist, _FP),
+                   p(knn_index, _IP)))
+
+
+def knn_cuda_global(ref, ref_nb, query, query_nb, dim, k, knn_dist, knn_index) -> bool:
+    """Mirror of knn_cuda_global (code/knncuda.h:14-21)."""
+    return _host_call("knnb200_cuda_global", ref, ref_nb, query, query_nb, dim, k, knn_dist,
+                      knn_index)
+
+
+def knn_cuda_texture(ref, ref_nb, query, query_nb, dim, k, knn_dist, knn_index) -> bool:
+    """Mirror of knn_cuda_texture (code/knncuda.h:37-44)."""
+    return _host_call("knnb200_cuda_texture", ref, ref_nb, query, query_nb, dim, k, knn_dist,
+                      knn_index)
+
+
+def knn_cublas(ref, ref_nb, query, query_nb, dim, k, knn_dist, knn_index) -> bool:
+    """Mirror of knn_cublas (code/knncuda.h:61-68)."""
+    return _host_call("knnb200_cublas", ref, ref_nb, query, query_nb, dim, k, knn_dist,
+                      knn_index)
+
+
+ENTRY_POINTS = {"global": knn_cuda_global, "texture": knn_cuda_texture, "cublas": knn_cublas}
+
+
+def knn(ref: np.ndarray, query: np.ndarray, k: int, method: str = "global"):
+    """Convenience wrapper: returns (dist, index), each k x query_nb."""
+    ref = np.ascontiguousarray(ref, dtype=np.float32)
+    query = np.ascontiguousarray(query, dtype=np.float32)
+    dim, ref_nb = ref.shape
+    query_nb = query.shape[1]
+    dist = np.empty((k, query_nb), np.float32)
+    idx = np.empty((k, query_nb), np.int32)
+    if not ENTRY_POINTS[method](ref, ref_nb, query, query_nb, dim, k, dist, idx):
+        raise RuntimeError(f"knn_{method} failed")
+    return dist, idx
+
+
+def knn_device(ref, query, k: int, method: str = "global", dist=None, index=None,
+               stream=None):
+    """Device-resident k-NN on torch CUDA tensors shaped (dim, n).
+
+    ``ref`` / ``query`` may be row-pitched views (stride(1) == 1, stride(0) a
+    multiple of 4).  Returns (dist, index) tensors of shape (k, query_nb);
+    queued on ``stream`` (default: torch's current stream), not synchronised.
+    """
+    import torch
+
+    dim, ref_nb = ref.shape
+    query_nb = query.shape[1]
+    if ref.dtype != torch.float32 or query.dtype != torch.float32:
+        raise TypeError("ref/query must be float32")
+    if ref.stride(1) != 1 or query.stride(1) != 1:
+        raise ValueError("ref/query rows must be contiguous")
+    if dist is None:
+        dist = torch.empty((k, query_nb), dtype=torch.float32, device=query.device)
+    if index is None:
+        index = torch.empty((k, query_nb), dtype=torch.int32, device=query.device)
+    if stream is None:
+        stream = torch.cuda.current_stream(query.device)
+    rc = lib().knnb200_knn_device(
+        ref.data_ptr(), ref_nb, ref.stride(0), query.data_ptr(), query_nb, query.stride(0),
+        dim, k, METHODS[method], dist.data_ptr(), index.data_ptr(), dist.stride(0),
+        ctypes.c_void_p(stream.cuda_stream))
+    if rc != 0:
+        raise RuntimeError(f"knnb200_knn_device failed: {status_string(rc)}")
+    return dist, index
+
+
+def sync_status(stream=None) -> int:
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return lib().knnb200_sync_status(ctypes.c_void_p(stream.cuda_stream))
+
+
+def status_string(code: int) -> str:
+    return lib().knnb200_status_string(code).decode()
+
+
+def scratch_bytes(ref_nb, query_nb, dim, k, method="global") -> int:
+    return lib().knnb200_scratch_bytes(ref_nb, query_nb, dim, k, METHODS[method])
+
+
+def plan_splits(ref_nb, query_nb, dim, k) -> int:
+    return lib().knnb200_plan_splits(ref_nb, query_nb, dim, k)
+
+
+def measure_fp32_peak(iters: int = 4096, stream=None) -> float:
+    """FP32 CUDA-core FLOP/s of the current device (packed-FMA calibration kernel)."""
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return lib().knnb200_measure_fp32_peak(iters, ctypes.c_void_p(stream.cuda_stream))
+
+
+def version() -> str:
+    return lib().knnb200_version().decode()
