@@ -87,6 +87,11 @@ KNNB200_API const char *knnb200_status_string(int code);
  * the roofline denominator of the FP32 direct-form path. */
 KNNB200_API double knnb200_measure_fp32_peak(int iters, void *stream);
 
+/* Number of queries of the last knn_cublas-method call on the current device
+ * that failed the tensor-core certification and were recomputed by the exact
+ * kernel (0 when the call ran the exact kernel only). */
+KNNB200_API int knnb200_last_fallback_count(void);
+
 /* Library version string. */
 KNNB200_API const char *knnb200_version(void);
 

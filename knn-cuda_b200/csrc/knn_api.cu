@@ -39,17 +39,17 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
     return fn;
 }
 
-bool encode_f32_2d(CUtensorMap *map, const void *base, uint64_t cols, uint64_t rows,
-                   uint64_t ld_elems, uint32_t box_cols, uint32_t box_rows) {
+bool encode_2d(CUtensorMap *map, CUtensorMapDataType dtype, int elem_bytes, const void *base,
+               uint64_t cols, uint64_t rows, uint64_t ld_elems, uint32_t box_cols,
+               uint32_t box_rows, CUtensorMapSwizzle swizzle) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = get_encode_fn();
     if (!enc) return false;
     cuuint64_t dims[2] = {cols, rows};
-    cuuint64_t strides[1] = {ld_elems * sizeof(float)};
+    cuuint64_t strides[1] = {ld_elems * (uint64_t)elem_bytes};
     cuuint32_t box[2] = {box_cols, box_rows};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), dims,
-                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    CUresult r = enc(map, dtype, 2, const_cast<void *>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
@@ -93,7 +93,9 @@ struct Workspace {
     cudaStream_t stream = nullptr;
     cudaEvent_t last_done = nullptr;   // orders device-resident calls on this device
     Buffer ref, qry, dist, idx, scratch, status;
+    Buffer tcref;                      // prepared reference set of the tensor-core path
     int *status_host = nullptr;        // pinned status word for the host path
+    int *nfail_host = nullptr;         // pinned count of uncertified tensor-core queries
 
     bool setup(int dev) {
         if (init) return true;
@@ -105,6 +107,8 @@ struct Workspace {
             return false;
         if (!status.ensure(sizeof(int))) return false;
         if (cudaMallocHost(reinterpret_cast<void **>(&status_host), sizeof(int)) != cudaSuccess)
+            return false;
+        if (cudaMallocHost(reinterpret_cast<void **>(&nfail_host), sizeof(int)) != cudaSuccess)
             return false;
         init = true;
         return true;
@@ -119,15 +123,44 @@ bool valid_sizes(int ref_nb, int query_nb, int dim, int k) {
     return ref_nb >= 1 && query_nb >= 1 && dim >= 1 && k >= 1 && k <= ref_nb;
 }
 
-size_t scratch_for(int N, int Q, int d, int k, int num_sms) {
+bool use_tc(int method, int N, int Q, int d, int k) {
+    return method == KNNB200_METHOD_CUBLAS && tc_supported(N, Q, d, k);
+}
+
+size_t scratch_for(int method, int N, int Q, int d, int k, int num_sms) {
+    if (use_tc(method, N, Q, d, k)) return tc_scratch_bytes(N, Q, d, k, num_sms);
     return exact_scratch_bytes(N, Q, d, k, num_sms);
 }
 
 // Queue the computation for one problem whose inputs are on the device.
-int enqueue(const ExactProblem &p, int method, cudaStream_t st) {
-    (void)method;   // all methods currently share the exact fused kernel
+// knn_cublas runs the tensor-core expansion path when the shape qualifies
+// (it synchronises the stream once, to recompute uncertified queries);
+// everything else runs the fused exact kernel.
+int enqueue(Workspace &ws, const ExactProblem &p, int method, cudaStream_t st) {
+    *ws.nfail_host = 0;
     if (!exact_supported_k(p.k)) return kErrUnsupported;
-    return launch_exact(p, st);
+    if (!use_tc(method, p.N, p.Q, p.d, p.k)) return launch_exact(p, st);
+    if (!ws.tcref.ensure(tc_ref_bytes(p.N, p.d))) return kErrNoMemory;
+    const TcRefView rv = tc_carve_ref(ws.tcref.ptr, p.N, p.d);
+    int rc = tc_prepare_ref(rv, p.ref, p.N, p.ldr, p.d, st);
+    if (rc != kOk) return rc;
+    TcProblem t;
+    t.ref = p.ref;
+    t.N = p.N;
+    t.ldr = p.ldr;
+    t.qry = p.qry;
+    t.Q = p.Q;
+    t.ldq = p.ldq;
+    t.d = p.d;
+    t.k = p.k;
+    t.out_dist = p.out_dist;
+    t.out_idx = p.out_idx;
+    t.ld_out = p.ld_out;
+    t.scratch = p.scratch;
+    t.scratch_bytes = p.scratch_bytes;
+    t.status = p.status;
+    t.num_sms = p.num_sms;
+    return launch_tc(t, rv, st, ws.nfail_host);
 }
 
 int current_workspace(Workspace *&ws) {
@@ -188,7 +221,7 @@ bool host_entry(int method, const float *ref, int ref_nb, const float *query, in
     }
     const long long ldr = round_up(ref_nb, 64), ldq = round_up(query_nb, 64);
     const size_t out_elems = (size_t)k * query_nb;
-    const size_t scratch = scratch_for(ref_nb, query_nb, dim, k, ws->num_sms);
+    const size_t scratch = scratch_for(method, ref_nb, query_nb, dim, k, ws->num_sms);
     if (!ws->ref.ensure((size_t)dim * ldr * sizeof(float)) ||
         !ws->qry.ensure((size_t)dim * ldq * sizeof(float)) ||
         !ws->dist.ensure(out_elems * sizeof(float)) ||
@@ -227,7 +260,7 @@ bool host_entry(int method, const float *ref, int ref_nb, const float *query, in
     p.status = static_cast<int *>(ws->status.ptr);
     p.num_sms = ws->num_sms;
     p.force_splits = 0;
-    rc = enqueue(p, method, st);
+    rc = enqueue(*ws, p, method, st);
     if (rc != kOk) {
         std::printf("ERROR: Unable to execute kernel (%s)\n", knnb200_status_string(rc));
         cudaGetLastError();
@@ -317,7 +350,7 @@ int knnb200_knn_device(const float *ref, int ref_nb, long long ref_ld, const flo
     int dev = 0;
     cudaGetDevice(&dev);
     if (!ws->setup(dev)) return KNNB200_ECUDA;
-    if (!ws->scratch.ensure(scratch_for(ref_nb, query_nb, dim, k, ws->num_sms)))
+    if (!ws->scratch.ensure(scratch_for(method, ref_nb, query_nb, dim, k, ws->num_sms)))
         return KNNB200_ENOMEM;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // Calls on one device share the workspace scratch: order them.
@@ -340,7 +373,7 @@ int knnb200_knn_device(const float *ref, int ref_nb, long long ref_ld, const flo
     p.status = static_cast<int *>(ws->status.ptr);
     p.num_sms = ws->num_sms;
     p.force_splits = 0;
-    rc = enqueue(p, method, st);
+    rc = enqueue(*ws, p, method, st);
     if (cudaEventRecord(ws->last_done, st) != cudaSuccess && rc == kOk) rc = kErrCuda;
     return rc;
 }
@@ -360,14 +393,13 @@ int knnb200_sync_status(void *stream) {
 }
 
 size_t knnb200_scratch_bytes(int ref_nb, int query_nb, int dim, int k, int method) {
-    (void)method;
     if (!valid_sizes(ref_nb, query_nb, dim, k)) return 0;
     int sms = 148;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaGetLastError();
-    return scratch_for(ref_nb, query_nb, dim, k, sms);
+    return scratch_for(method, ref_nb, query_nb, dim, k, sms);
 }
 
 int knnb200_plan_splits(int ref_nb, int query_nb, int dim, int k) {
@@ -391,6 +423,7 @@ void knnb200_release_workspace(void) {
     ws->dist.release();
     ws->idx.release();
     ws->scratch.release();
+    ws->tcref.release();
 }
 
 const char *knnb200_status_string(int code) {
@@ -407,6 +440,13 @@ const char *knnb200_status_string(int code) {
         case KNNB200_ETENSORMAP: return "TMA descriptor encoding failed";
         default: return "unknown";
     }
+}
+
+int knnb200_last_fallback_count(void) {
+    Workspace *ws = nullptr;
+    if (current_workspace(ws) != kOk || !ws->init) return 0;
+    std::lock_guard<std::mutex> lock(ws->mu);
+    return *ws->nfail_host;
 }
 
 const char *knnb200_version(void) { return "knnb200 0.1.0 (sm_100a)"; }

@@ -434,7 +434,7 @@ bool exact_supported_k(int k) { return k >= 1 && k <= 256; }
 int launch_exact(const ExactProblem &p, cudaStream_t st) {
     ExactShape s;
     if (!choose_shape(p.N, p.Q, p.d, p.k, p.num_sms, s)) return kErrUnsupported;
-    if (p.force_splits > 0) s.splits = std::min(p.force_splits, s.n_rtiles);
+    if (p.force_splits > 0) s.splits = std::min(p.force_splits, std::min(s.n_rtiles, 64));
     const size_t need = s.splits > 1 ? (size_t)s.splits * p.Q * p.k * 8 : 0;
     if (need > p.scratch_bytes) return kErrScratch;
 

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -53,13 +54,56 @@ struct ExactProblem {
     int force_splits;   // 0 = automatic
 };
 
-// Encode a 2-D FP32 tensor map (cols = contiguous axis) with zero OOB fill.
-bool encode_f32_2d(CUtensorMap *map, const void *base, uint64_t cols, uint64_t rows,
-                   uint64_t ld_elems, uint32_t box_cols, uint32_t box_rows);
+// Encode a 2-D tensor map (cols = contiguous axis, row pitch ld_elems) with
+// zero out-of-bounds fill.
+bool encode_2d(CUtensorMap *map, CUtensorMapDataType dtype, int elem_bytes, const void *base,
+               uint64_t cols, uint64_t rows, uint64_t ld_elems, uint32_t box_cols,
+               uint32_t box_rows, CUtensorMapSwizzle swizzle);
+inline bool encode_f32_2d(CUtensorMap *map, const void *base, uint64_t cols, uint64_t rows,
+                          uint64_t ld_elems, uint32_t box_cols, uint32_t box_rows) {
+    return encode_2d(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, cols, rows, ld_elems,
+                     box_cols, box_rows, CU_TENSOR_MAP_SWIZZLE_NONE);
+}
 
 bool exact_supported_k(int k);
 size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms);
 int exact_plan_splits(int N, int Q, int d, int k, int num_sms);
 int launch_exact(const ExactProblem &p, cudaStream_t st);
+
+// Prepared reference set of the tensor-core path (see knn_tc.cu).
+struct TcRefView {
+    __nv_bfloat16 *refB;    // [N][d_pad] BF16, K-major
+    float *refT;            // [N][d_pad] FP32 point-major (re-rank gathers)
+    float *rn;              // [N] squared norms
+    unsigned *rmax_bits;    // largest squared norm (float bits)
+};
+
+struct TcProblem {
+    const float *ref;       // original dim x N FP32 set (exact fallback)
+    int N;
+    long long ldr;
+    const float *qry;       // dim x Q FP32 queries
+    int Q;
+    long long ldq;
+    int d, k;
+    float *out_dist;
+    int *out_idx;
+    long long ld_out;
+    void *scratch;
+    size_t scratch_bytes;
+    int *status;
+    int num_sms;
+};
+
+bool tc_supported(int N, int Q, int d, int k);
+size_t tc_ref_bytes(int N, int d);
+size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms);
+TcRefView tc_carve_ref(void *mem, int N, int d);
+int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, int d,
+                   cudaStream_t st);
+// Queues the tensor-core k-NN; synchronises once to learn how many queries
+// failed certification (written to *host_nfail, pinned) and recomputes them
+// with the exact kernel.
+int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_nfail);
 
 }  // namespace knnb200

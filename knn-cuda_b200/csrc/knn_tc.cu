@@ -1,0 +1,682 @@
+// knn_tc.cu -- the expansion method (knn_cublas) on tcgen05 tensor cores,
+// returning EXACT results.
+//
+// The reference computes D = ||r||^2 - 2 Q^T R + ||q||^2 with cublasSgemm
+// plus norm kernels, sorts the full matrix and adds ||q||^2 to the survivors
+// (code/knncuda.cu:709-794).  Here the contraction runs in BF16 on the 5th-gen
+// tensor cores with FP32 accumulation in TMEM, and the norm add and selection
+// live in the GEMM epilogue; nothing of size ref_nb x query_nb is stored.
+//
+//   prep      reference / query sets -> BF16 point-major (K-major) copies,
+//             FP32 point-major copy of the reference set (for re-ranking),
+//             FP32 squared norms and the largest reference norm.
+//   pass 1    tensor scan of a strided 1/G sample of the reference tiles; each
+//             epilogue thread keeps the KS smallest a = ||r||^2 - 2 r.q of its
+//             query row in registers -> threshold T_q (KS-th smallest over the
+//             sample; over the full set about KS*G points lie below it).
+//   pass 2    tensor scan of all reference tiles; the epilogue emits every
+//             reference with a < T_q into the query's candidate list.
+//   rerank    exact FP32 direct-form distances of the candidates, in the same
+//             arithmetic and order as the fused exact kernel, sorted by
+//             (distance, index).  The result is CERTIFIED when the k-th exact
+//             distance D_k satisfies D_k (1+g) + E_q < T_q + ||q||^2, where
+//             E_q bounds |(BF16 expansion) - (exact squared distance)| for
+//             every reference: then every point that could belong to the
+//             exact top-k was emitted, and the output is bit-identical to
+//             the exact kernel's.  Uncertified queries (sample too small, list
+//             overflow) are recomputed by the exact kernel.
+//
+// Error bound (u = 2^-8, BF16 unit roundoff): |bf16(r).bf16(q) - r.q| <=
+// (2u + u^2) sum|r_i q_i| + FP32 accumulation error <= eps_d ||r|| ||q|| with
+// eps_d = 2^-7 + 2^-16 + d_pad 2^-22 (twice the usual gamma_d margin for the
+// accumulation), so E_q = 2 eps_d ||q|| max||r|| + d_pad 2^-22 (max||r||^2 +
+// ||q||^2) + 2^-20 (|T_q| + ||q||^2) also covers norm and epilogue roundings.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "knn_kernels.h"
+#include "knn_tc.cuh"
+
+namespace knnb200 {
+
+constexpr int TC_BM = 128;            // rows (queries) per MMA tile
+constexpr int TC_QT = 2 * TC_BM;      // queries per CTA (two A tiles share each B tile)
+constexpr int TC_BN = 128;            // reference points per tile
+constexpr int TC_BK = 64;             // K block: 64 bf16 = 128 B (one swizzle row)
+constexpr int TC_KBMAX = 4;           // d_pad <= 256
+constexpr int TC_STAGES = 4;
+constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;   // 16 KB (A or B K-block tile)
+constexpr int TC_KS = 16;             // pass-1 per-row list length
+constexpr int TC_THREADS = 192;       // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
+constexpr uint32_t TC_TMEM_COLS = 512;   // 2 accumulator buffers x 2 A tiles x 128
+constexpr uint32_t TC_IDESC = umma_idesc_bf16(TC_BM, TC_BN);
+
+constexpr size_t TC_OFF_A = 0;
+constexpr size_t TC_OFF_B = (size_t)2 * TC_KBMAX * TC_TILE_BYTES;             // 128 KB
+constexpr size_t TC_OFF_RN = TC_OFF_B + (size_t)TC_STAGES * TC_TILE_BYTES;    // +64 KB
+constexpr size_t TC_OFF_BAR = TC_OFF_RN + 4 * TC_BN * sizeof(float);   // one rn slab per epilogue warp
+constexpr int TC_NBARS = 1 + 2 * TC_STAGES + 2 + 2 + 1;
+constexpr size_t TC_SMEM = 1024 + TC_OFF_BAR + TC_NBARS * 8 + 16;
+
+struct TcArgs {
+    int N, Q, kb_count, n_tiles, n_splits, tile_stride;
+    const float *rn;        // [N] reference squared norms
+    const float *thr;       // pass 2: [Q] thresholds (a units)
+    float *p1;              // pass 1: [n_splits][Q][TC_KS]
+    int *cand;              // pass 2: [Q][cmax]
+    int *count;             // pass 2: [Q]
+    int cmax;
+    int *status;
+};
+
+template <int MODE>   // 0: threshold sample pass, 1: emit pass
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    knn_tc_scan_kernel(const __grid_constant__ CUtensorMap tmA,
+                       const __grid_constant__ CUtensorMap tmB, TcArgs a) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char *sA = base + TC_OFF_A;
+    unsigned char *sB = base + TC_OFF_B;
+    float *rn_s = reinterpret_cast<float *>(base + TC_OFF_RN);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(base + TC_OFF_BAR);
+    uint64_t *a_full = bars;
+    uint64_t *b_full = bars + 1;
+    uint64_t *b_empty = b_full + TC_STAGES;
+    uint64_t *acc_full = b_empty + TC_STAGES;
+    uint64_t *acc_empty = acc_full + 2;
+    uint64_t *drain = acc_empty + 2;
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + TC_NBARS);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qtile = blockIdx.x, split = blockIdx.y;
+    const int KB = a.kb_count;
+    // this CTA's reference tiles: [t0, t1) with t % tile_stride == 0
+    const int t0 = (int)((long long)a.n_tiles * split / a.n_splits);
+    const int t1 = (int)((long long)a.n_tiles * (split + 1) / a.n_splits);
+    const int G = a.tile_stride;
+    const int first = ((t0 + G - 1) / G) * G;
+    const int n_my = first < t1 ? (t1 - first + G - 1) / G : 0;
+
+    if (warp == 0 && lane == 0) {
+        mbar_init(a_full, 1);
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(&b_full[s], 1);
+            mbar_init(&b_empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 4);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+        prefetch_tensormap(&tmA);
+        prefetch_tensormap(&tmB);
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_holder, TC_TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_holder;
+
+    if (warp == 0) {
+        // ------------------------- TMA producer --------------------------
+        if (lane == 0) {
+            int issued = 0;
+            bool a_issued = false;
+            if (n_my > 0) {
+                mbar_arrive_expect_tx(a_full, (uint32_t)(2 * KB * TC_TILE_BYTES));
+                for (int h = 0; h < 2; ++h)
+                    for (int kb = 0; kb < KB; ++kb)
+                        tma_load_2d(sA + (size_t)(h * TC_KBMAX + kb) * TC_TILE_BYTES, &tmA, a_full,
+                                    kb * TC_BK, qtile * TC_QT + h * TC_BM);
+                a_issued = true;
+            }
+            const int total = n_my * KB;
+            for (int it = 0; it < total; ++it) {
+                const int s = it % TC_STAGES;
+                if (it >= TC_STAGES && !mbar_wait(&b_empty[s], ((it / TC_STAGES) - 1) & 1)) {
+                    atomicMax(a.status, (int)kDevTimeoutEmpty);
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*abort_flag) break;
+                const int j = it / KB, kb = it - j * KB;
+                mbar_arrive_expect_tx(&b_full[s], TC_TILE_BYTES);
+                tma_load_2d(sB + (size_t)s * TC_TILE_BYTES, &tmB, &b_full[s], kb * TC_BK,
+                            (first + j * G) * TC_BN);
+                issued = it + 1;
+            }
+            for (int it = max(0, issued - TC_STAGES); it < issued; ++it)
+                if (!mbar_wait(&b_full[it % TC_STAGES], (it / TC_STAGES) & 1))
+                    atomicMax(a.status, (int)kDevTimeoutDrain);
+            if (a_issued && !mbar_wait(a_full, 0)) atomicMax(a.status, (int)kDevTimeoutDrain);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------- MMA issuer ----------------------------
+        if (lane == 0) {
+            bool ok = n_my == 0 || mbar_wait(a_full, 0);
+            bool issued_mma = false;
+            tc_fence_after();
+            for (int j = 0; j < n_my && ok; ++j) {
+                const int b = j & 1;
+                if (j >= 2 && !mbar_wait(&acc_empty[b], ((j >> 1) - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                for (int kb = 0; kb < KB; ++kb) {
+                    const int it = j * KB + kb, s = it % TC_STAGES;
+                    if (!mbar_wait(&b_full[s], (it / TC_STAGES) & 1) || *abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t bdesc = umma_desc_sw128(sB + (size_t)s * TC_TILE_BYTES);
+#pragma unroll
+                    for (int k = 0; k < TC_BK / 16; ++k) {
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const uint64_t adesc = umma_desc_sw128(
+                                sA + (size_t)(h * TC_KBMAX + kb) * TC_TILE_BYTES);
+                            umma_bf16(tmem + (uint32_t)((b * 2 + h) * TC_BM),
+                                      adesc + (uint64_t)(2 * k), bdesc + (uint64_t)(2 * k),
+                                      TC_IDESC, (kb > 0 || k > 0) ? 1u : 0u);
+                        }
+                    }
+                    umma_commit(&b_empty[s]);
+                    issued_mma = true;
+                }
+                if (!ok) break;
+                umma_commit(&acc_full[b]);
+            }
+            if (!ok) {
+                atomicMax(a.status, (int)kDevTimeoutFull);
+                *abort_flag = 1;
+            }
+            // every MMA issued by this thread has completed before teardown
+            if (issued_mma) {
+                umma_commit(drain);
+                if (!mbar_wait(drain, 0)) atomicMax(a.status, (int)kDevTimeoutDrain);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ------------------------- epilogue (4 warps) --------------------
+        const int qd = warp & 3;                  // TMEM lane quadrant of this warp
+        int qrow[2];
+        float thr[2];
+        float L[2][TC_KS];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            qrow[h] = qtile * TC_QT + h * TC_BM + qd * 32 + lane;
+            thr[h] = -INFINITY;
+            if (MODE == 1 && qrow[h] < a.Q) thr[h] = a.thr[qrow[h]];
+#pragma unroll
+            for (int i = 0; i < TC_KS; ++i) L[h][i] = INFINITY;
+        }
+        for (int j = 0; j < n_my; ++j) {
+            const int b = j & 1;
+            const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
+            if (__any_sync(0xffffffffu, !got || *abort_flag != 0)) {
+                if (lane == 0) {
+                    if (!got) atomicMax(a.status, (int)kDevTimeoutFull);
+                    *abort_flag = 1;
+                }
+                break;
+            }
+            tc_fence_after();
+            const int tile = first + j * G;
+            // this warp's copy of the tile's reference norms (padding -> +inf)
+            float *rnb = rn_s + (warp - 2) * TC_BN;
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < TC_BN / 32; ++i) {
+                const int ridx = tile * TC_BN + i * 32 + lane;
+                rnb[i * 32 + lane] = ridx < a.N ? a.rn[ridx] : INFINITY;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+#pragma unroll 1
+                for (int c = 0; c < TC_BN / 32; ++c) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem + ((uint32_t)(qd * 32) << 16) +
+                                  (uint32_t)((b * 2 + h) * TC_BM + c * 32),
+                              v);
+                    tmem_ld_wait(v);
+                    const int cbase = tile * TC_BN + c * 32;
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) {
+                        const float av = fmaf(-2.0f, __uint_as_float(v[e]), rnb[c * 32 + e]);
+                        if (MODE == 1) {
+                            if (av < thr[h]) {
+                                const int pos = atomicAdd(&a.count[qrow[h]], 1);
+                                if (pos < a.cmax)
+                                    a.cand[(size_t)qrow[h] * a.cmax + pos] = cbase + e;
+                            }
+                        } else if (av < L[h][TC_KS - 1]) {
+#pragma unroll
+                            for (int i = TC_KS - 1; i > 0; --i)
+                                L[h][i] = av < L[h][i - 1] ? L[h][i - 1]
+                                                           : (av < L[h][i] ? av : L[h][i]);
+                            L[h][0] = fminf(L[h][0], av);
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[b]);
+        }
+        if (MODE == 0 && !*abort_flag) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (qrow[h] < a.Q) {
+                    float *dst = a.p1 + ((size_t)split * a.Q + qrow[h]) * TC_KS;
+#pragma unroll
+                    for (int i = 0; i < TC_KS; ++i) dst[i] = L[h][i];
+                }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, TC_TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
+// prep kernels
+// ---------------------------------------------------------------------------
+
+// Squared norm of each point of a dim x n set (sequential FP32 fma over d)
+// and the largest squared norm (non-negative float bits compare as unsigned).
+__global__ void tc_norms_kernel(const float *__restrict__ x, int n, long long ld, int d,
+                                float *__restrict__ nrm, unsigned *__restrict__ max_bits) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    float s = 0.f;
+    if (p < n) {
+        for (int dd = 0; dd < d; ++dd) {
+            const float v = x[(size_t)dd * ld + p];
+            s = fmaf(v, v, s);
+        }
+        nrm[p] = s;
+    }
+    unsigned m = __float_as_uint(s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && max_bits) atomicMax(max_bits, m);
+}
+
+// dim x n (row pitch ld) FP32 -> n x d_pad BF16 (and optionally FP32),
+// zero-padded in [d, d_pad).  32 x 32 tiles through shared memory.
+__global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld, int d,
+                               int d_pad, __nv_bfloat16 *__restrict__ xb,
+                               float *__restrict__ xt) {
+    __shared__ float tile[32][33];
+    const int p0 = blockIdx.x * 32, d0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int dd = d0 + ty + 8 * i, p = p0 + tx;
+        tile[ty + 8 * i][tx] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int p = p0 + ty + 8 * i, dd = d0 + tx;
+        if (p < n && dd < d_pad) {
+            const float v = tile[tx][ty + 8 * i];
+            xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(v);
+            if (xt) xt[(size_t)p * d_pad + dd] = v;
+        }
+    }
+}
+
+// T_q = KS-th smallest of the per-split pass-1 lists; resets candidate counts.
+__global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
+                                    float *__restrict__ thr, int *__restrict__ count) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= Q) return;
+    float L[TC_KS];
+#pragma unroll
+    for (int i = 0; i < TC_KS; ++i) L[i] = INFINITY;
+    for (int s = 0; s < S; ++s) {
+        const float *src = p1 + ((size_t)s * Q + q) * TC_KS;
+        for (int i = 0; i < TC_KS; ++i) {
+            const float v = src[i];
+            if (!(v < L[TC_KS - 1])) break;   // lists are ascending
+#pragma unroll
+            for (int t = TC_KS - 1; t > 0; --t)
+                L[t] = v < L[t - 1] ? L[t - 1] : (v < L[t] ? v : L[t]);
+            L[0] = fminf(L[0], v);
+        }
+    }
+    thr[q] = L[TC_KS - 1];
+    count[q] = 0;
+}
+
+// Exact FP32 re-rank of each query's candidates + certification.
+// One block (256 threads) per query.
+__global__ void __launch_bounds__(256)
+    tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
+                     const float *__restrict__ qry, long long ldq, const float *__restrict__ qn,
+                     const unsigned *__restrict__ rmax_bits, const float *__restrict__ thr,
+                     const int *__restrict__ cand, const int *__restrict__ count, int cmax,
+                     int k, float *__restrict__ out_dist, int *__restrict__ out_idx,
+                     long long ld_out, int *__restrict__ fail_list,
+                     int *__restrict__ n_fail) {
+    extern __shared__ unsigned char rsm[];
+    float *qv = reinterpret_cast<float *>(rsm);
+    unsigned long long *keys =
+        reinterpret_cast<unsigned long long *>(rsm + (((size_t)d_pad * 4 + 15) & ~size_t(15)));
+    __shared__ int failed;
+    const int q = blockIdx.x, tid = threadIdx.x;
+    const int c = count[q];
+    if (c > cmax || c < k) {
+        if (tid == 0) fail_list[atomicAdd(n_fail, 1)] = q;
+        return;
+    }
+    for (int dd = tid; dd < d_pad; dd += blockDim.x)
+        qv[dd] = dd < d ? qry[(size_t)dd * ldq + q] : 0.f;
+    int P = 1;
+    while (P < c) P <<= 1;
+    __syncthreads();
+    for (int t = tid; t < P; t += blockDim.x) {
+        unsigned long long key = kKeyInf;
+        if (t < c) {
+            const int r = cand[(size_t)q * cmax + t];
+            const float4 *row = reinterpret_cast<const float4 *>(refT + (size_t)r * d_pad);
+            float acc = 0.f;
+            for (int dd4 = 0; dd4 < d_pad / 4; ++dd4) {
+                const float4 v = __ldg(row + dd4);
+                float t0 = __fsub_rn(v.x, qv[4 * dd4 + 0]);
+                acc = __fmaf_rn(t0, t0, acc);
+                t0 = __fsub_rn(v.y, qv[4 * dd4 + 1]);
+                acc = __fmaf_rn(t0, t0, acc);
+                t0 = __fsub_rn(v.z, qv[4 * dd4 + 2]);
+                acc = __fmaf_rn(t0, t0, acc);
+                t0 = __fsub_rn(v.w, qv[4 * dd4 + 3]);
+                acc = __fmaf_rn(t0, t0, acc);
+            }
+            key = make_key(acc, (uint32_t)r);
+        }
+        keys[t] = key;
+    }
+    __syncthreads();
+    // bitonic sort of keys[0..P), ascending
+    for (int size = 2; size <= P; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = tid; t < P / 2; t += blockDim.x) {
+                const int lo = 2 * t - (t & (stride - 1));
+                const int hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const unsigned long long x = keys[lo], y = keys[hi];
+                if ((x > y) == up) {
+                    keys[lo] = y;
+                    keys[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (tid == 0) {
+        const float dk = key_dist2(keys[k - 1]);
+        const float qq = qn[q];
+        const float r2 = __uint_as_float(*rmax_bits);
+        const float T = thr[q];
+        const float eps = 0.0078125f + 1.52587890625e-05f + (float)d_pad * 2.384185791015625e-07f;
+        const float E = 2.f * eps * sqrtf(qq * r2) +
+                        (float)d_pad * 2.384185791015625e-07f * (r2 + qq) +
+                        9.5367431640625e-07f * (fabsf(T) + qq);
+        const float lhs = dk * (1.f + (float)d_pad * 2.384185791015625e-07f) + E;
+        failed = !(lhs < T + qq);
+        if (failed) fail_list[atomicAdd(n_fail, 1)] = q;
+    }
+    __syncthreads();
+    if (failed) return;
+    for (int j = tid; j < k; j += blockDim.x) {
+        const unsigned long long key = keys[j];
+        out_dist[(size_t)j * ld_out + q] = sqrtf(key_dist2(key));
+        out_idx[(size_t)j * ld_out + q] = key_index(key);
+    }
+}
+
+// Fallback plumbing: gather the uncertified queries into a dense d x m set
+// and scatter the exact results back.
+__global__ void gather_queries_kernel(const float *__restrict__ qry, long long ldq, int d,
+                                      const int *__restrict__ list, int m, float *__restrict__ dst,
+                                      long long ldd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int dd = blockIdx.y;
+    if (i < m) dst[(size_t)dd * ldd + i] = qry[(size_t)dd * ldq + list[i]];
+}
+
+__global__ void scatter_results_kernel(const float *__restrict__ sd, const int *__restrict__ si,
+                                       long long lds, const int *__restrict__ list, int m,
+                                       float *__restrict__ out_dist, int *__restrict__ out_idx,
+                                       long long ld_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i < m) {
+        out_dist[(size_t)j * ld_out + list[i]] = sd[(size_t)j * lds + i];
+        out_idx[(size_t)j * ld_out + list[i]] = si[(size_t)j * lds + i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+bool encode_bf16_kmajor(CUtensorMap *m, const void *base, int rows, int d_pad) {
+    return encode_2d(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, (uint64_t)d_pad,
+                     (uint64_t)rows, (uint64_t)d_pad, TC_BK, TC_BM, CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+struct TcPlan {
+    int d_pad, kb, qtiles, n_tiles, splits, stride1, cmax;
+};
+
+TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
+    TcPlan p;
+    p.d_pad = (d + 63) / 64 * 64;
+    p.kb = p.d_pad / 64;
+    p.qtiles = (Q + TC_QT - 1) / TC_QT;
+    p.n_tiles = (N + TC_BN - 1) / TC_BN;
+    // splits: fill whole waves of one CTA per SM, at least 16 tiles per CTA
+    int best = 1;
+    double best_t = 1e300;
+    const int max_s = std::max(1, std::min(256, p.n_tiles / 16));
+    for (int S = 1; S <= max_s; ++S) {
+        const long long ctas = (long long)p.qtiles * S;
+        const double t = (double)((ctas + num_sms - 1) / num_sms) * ((double)p.n_tiles / S + 2.0);
+        if (t < best_t * 0.999) {
+            best_t = t;
+            best = S;
+        }
+    }
+    p.splits = best;
+    // the sample must hold about 2.5k points below T_q: KS * stride >= 2.5k
+    p.stride1 = std::max(16, (5 * k + 2 * TC_KS - 1) / (2 * TC_KS));
+    p.cmax = 4 * TC_KS * p.stride1;
+    return p;
+}
+
+struct Carve {
+    unsigned char *p;
+    size_t used, cap;
+    template <typename T>
+    T *take(size_t count) {
+        used = (used + 255) & ~size_t(255);
+        T *r = reinterpret_cast<T *>(p + used);
+        used += count * sizeof(T);
+        return r;
+    }
+};
+
+}  // namespace
+
+bool tc_supported(int N, int Q, int d, int k) {
+    return d >= 16 && d <= TC_KBMAX * TC_BK && k >= 1 && k <= 128 && N >= 32768 && Q >= 1;
+}
+
+size_t tc_ref_bytes(int N, int d) {
+    const int d_pad = (d + 63) / 64 * 64;
+    return (size_t)N * d_pad * 2 + (size_t)N * d_pad * 4 + (size_t)N * 4 + 4 * 256;
+}
+
+static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
+    const long long ldf = (Q + 3) / 4 * 4;
+    return (size_t)d * ldf * 4 + (size_t)k * ldf * 8 + exact_scratch_bytes(N, Q, d, k, num_sms) +
+           4 * 256;
+}
+
+size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
+    const TcPlan p = plan_tc(N, Q, d, k, num_sms);
+    size_t b = (size_t)p.qtiles * TC_QT * p.d_pad * 2 + (size_t)Q * 4 * 4 + 16;
+    b += (size_t)p.splits * Q * TC_KS * 4;
+    b += (size_t)Q * p.cmax * 4;
+    b += fallback_bytes(N, Q, d, k, num_sms);   // worst case: every query uncertified
+    return b + 16 * 256;
+}
+
+int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, int d,
+                   cudaStream_t st) {
+    const int d_pad = (d + 63) / 64 * 64;
+    if (cudaMemsetAsync(v.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess) return kErrCuda;
+    tc_norms_kernel<<<(N + 255) / 256, 256, 0, st>>>(ref, N, ldr, d, v.rn, v.rmax_bits);
+    dim3 g((N + 31) / 32, d_pad / 32);
+    tc_pack_kernel<<<g, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, v.refB, v.refT);
+    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
+}
+
+TcRefView tc_carve_ref(void *mem, int N, int d) {
+    const int d_pad = (d + 63) / 64 * 64;
+    Carve cv{static_cast<unsigned char *>(mem), 0, 0};
+    TcRefView v;
+    v.refB = cv.take<__nv_bfloat16>((size_t)N * d_pad);
+    v.refT = cv.take<float>((size_t)N * d_pad);
+    v.rn = cv.take<float>(N);
+    v.rmax_bits = cv.take<unsigned>(1);
+    return v;
+}
+
+int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_nfail) {
+    const TcPlan p = plan_tc(P.N, P.Q, P.d, P.k, P.num_sms);
+    if (!tc_supported(P.N, P.Q, P.d, P.k)) return kErrUnsupported;
+    Carve cv{static_cast<unsigned char *>(P.scratch), 0, P.scratch_bytes};
+    __nv_bfloat16 *qB = cv.take<__nv_bfloat16>((size_t)p.qtiles * TC_QT * p.d_pad);
+    float *qn = cv.take<float>(P.Q);
+    float *thr = cv.take<float>(P.Q);
+    int *count = cv.take<int>(P.Q);
+    int *fail = cv.take<int>(P.Q);
+    int *nfail = cv.take<int>(4);
+    float *p1 = cv.take<float>((size_t)p.splits * P.Q * TC_KS);
+    int *cand = cv.take<int>((size_t)P.Q * p.cmax);
+    const long long ldf = (P.Q + 3) / 4 * 4;       // fallback buffers, sized for all queries
+    float *qsub = cv.take<float>((size_t)P.d * ldf);
+    float *sd = cv.take<float>((size_t)P.k * ldf);
+    int *si = cv.take<int>((size_t)P.k * ldf);
+    unsigned char *xs = cv.take<unsigned char>(0);
+    const size_t xcap = P.scratch_bytes > cv.used ? P.scratch_bytes - cv.used : 0;
+    if (cv.used > P.scratch_bytes) return kErrScratch;
+
+    // queries: norms + BF16 K-major copy
+    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, qn, nullptr);
+    tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
+        P.qry, P.Q, P.ldq, P.d, p.d_pad, qB, nullptr);
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+
+    CUtensorMap tmA, tmB;
+    if (!encode_bf16_kmajor(&tmA, qB, P.Q, p.d_pad)) return kErrTensorMap;
+    if (!encode_bf16_kmajor(&tmB, R.refB, P.N, p.d_pad)) return kErrTensorMap;
+
+    TcArgs a;
+    a.N = P.N;
+    a.Q = P.Q;
+    a.kb_count = p.kb;
+    a.n_tiles = p.n_tiles;
+    a.n_splits = p.splits;
+    a.rn = R.rn;
+    a.thr = thr;
+    a.p1 = p1;
+    a.cand = cand;
+    a.count = count;
+    a.cmax = p.cmax;
+    a.status = P.status;
+    dim3 grid(p.qtiles, p.splits);
+    cudaError_t e;
+    e = cudaFuncSetAttribute(knn_tc_scan_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TC_SMEM);
+    if (e != cudaSuccess) return kErrLaunch;
+    e = cudaFuncSetAttribute(knn_tc_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TC_SMEM);
+    if (e != cudaSuccess) return kErrLaunch;
+
+    a.tile_stride = p.stride1;
+    knn_tc_scan_kernel<0><<<grid, TC_THREADS, TC_SMEM, st>>>(tmA, tmB, a);
+    tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, p.splits, P.Q, thr, count);
+    a.tile_stride = 1;
+    knn_tc_scan_kernel<1><<<grid, TC_THREADS, TC_SMEM, st>>>(tmA, tmB, a);
+    if (cudaMemsetAsync(nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
+    int cpow = 1;
+    while (cpow < p.cmax) cpow <<= 1;
+    const size_t rsmem = (((size_t)p.d_pad * 4 + 15) & ~size_t(15)) + (size_t)cpow * 8;
+    e = cudaFuncSetAttribute(tc_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)rsmem);
+    if (e != cudaSuccess) return kErrLaunch;
+    tc_rerank_kernel<<<P.Q, 256, rsmem, st>>>(R.refT, P.d, p.d_pad, P.qry, P.ldq, qn,
+                                              R.rmax_bits, thr, cand, count, p.cmax, P.k,
+                                              P.out_dist, P.out_idx, P.ld_out, fail, nfail);
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+
+    // uncertified queries -> exact kernel
+    int nf = 0;
+    if (cudaMemcpyAsync(host_nfail, nfail, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return kErrCuda;
+    nf = *host_nfail;
+    if (nf == 0) return kOk;
+    // as many reference splits as the remaining scratch holds (one split needs none)
+    const long long per_split = (long long)nf * P.k * 8;
+    const int splits = (int)std::max<long long>(
+        1, std::min<long long>(exact_plan_splits(P.N, nf, P.d, P.k, P.num_sms),
+                               (long long)(xcap / per_split)));
+    gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, fail,
+                                                                       nf, qsub, ldf);
+    ExactProblem x;
+    x.ref = P.ref;
+    x.N = P.N;
+    x.ldr = P.ldr;
+    x.qry = qsub;
+    x.Q = nf;
+    x.ldq = ldf;
+    x.d = P.d;
+    x.k = P.k;
+    x.out_dist = sd;
+    x.out_idx = si;
+    x.ld_out = ldf;
+    x.scratch = xs;
+    x.scratch_bytes = xcap;
+    x.status = P.status;
+    x.num_sms = P.num_sms;
+    x.force_splits = splits;
+    int rc = launch_exact(x, st);
+    if (rc != kOk) return rc;
+    scatter_results_kernel<<<dim3((nf + 127) / 128, P.k), 128, 0, st>>>(
+        sd, si, ldf, fail, nf, P.out_dist, P.out_idx, P.ld_out);
+    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
+}
+
+}  // namespace knnb200

@@ -43,7 +43,7 @@ C_SYMBOLS = (
     "knnb200_cuda_global", "knnb200_cuda_texture", "knnb200_cublas", "knnb200_knn_device",
     "knnb200_sync_status", "knnb200_scratch_bytes", "knnb200_plan_splits",
     "knnb200_release_workspace", "knnb200_status_string", "knnb200_version",
-    "knnb200_measure_fp32_peak",
+    "knnb200_measure_fp32_peak", "knnb200_last_fallback_count",
 )
 CXX_SYMBOLS = (
     "_Z15knn_cuda_globalPKfiS0_iiiPfPi",
@@ -81,6 +81,8 @@ def lib():
         L.knnb200_status_string.argtypes = [ctypes.c_int]
         L.knnb200_measure_fp32_peak.restype = ctypes.c_double
         L.knnb200_measure_fp32_peak.argtypes = [ctypes.c_int, ctypes.c_void_p]
+        L.knnb200_last_fallback_count.restype = ctypes.c_int
+        L.knnb200_last_fallback_count.argtypes = []
         L.knnb200_version.restype = ctypes.c_char_p
         L.knnb200_version.argtypes = []
         _lib = L
@@ -201,6 +203,11 @@ def measure_fp32_peak(iters: int = 4096, stream=None) -> float:
     if stream is None:
         stream = torch.cuda.current_stream()
     return lib().knnb200_measure_fp32_peak(iters, ctypes.c_void_p(stream.cuda_stream))
+
+
+def last_fallback_count() -> int:
+    """Queries of the last knn_cublas-method call recomputed by the exact kernel."""
+    return lib().knnb200_last_fallback_count()
 
 
 def version() -> str:

@@ -1,0 +1,110 @@
+"""GPU parity tests of the tensor-core expansion path (knn_cublas).
+
+The BF16 tcgen05 candidate scan is followed by an exact FP32 re-rank in the
+fused exact kernel's arithmetic and a certification against the derived BF16
+error bound; uncertified queries are recomputed by the exact kernel.  So the
+strongest property holds: knn_cublas returns exactly what knn_cuda_global
+returns, bit for bit, on every shape -- certified or not.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from knn_check import check_exact, recall_at_k
+
+pytestmark = pytest.mark.gpu
+THREADS = os.cpu_count() or 4
+
+
+def _uniform(seed, dim, n, q):
+    rng = np.random.default_rng(seed)
+    return rng.random((dim, n), dtype=np.float32), rng.random((dim, q), dtype=np.float32)
+
+
+CASES = [
+    # (seed, ref_nb, query_nb, dim, k)
+    (1, 65536, 300, 64, 16),
+    (2, 65536, 513, 128, 100),
+    (3, 40000, 257, 256, 128),       # ragged N, k at the tensor-path maximum
+    (4, 32768, 1, 32, 1),            # Q = 1, k = 1
+    (5, 70001, 1000, 200, 50),       # d not a multiple of 64
+    (6, 131072, 96, 16, 10),         # smallest tensor-path dim
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"n{c[1]}q{c[2]}d{c[3]}k{c[4]}" for c in CASES])
+def test_cublas_equals_global_bitwise(knncuda, gpu, case):
+    seed, n, q, dim, k = case
+    ref, query = _uniform(seed, dim, n, q)
+    dg, ig = knncuda.knn(ref, query, k, "global")
+    dc, ic = knncuda.knn(ref, query, k, "cublas")
+    assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
+    assert np.array_equal(ic, ig)
+
+
+def test_cublas_exact_vs_fp64_and_reference(knncuda, oracle, gpu):
+    ref, query = _uniform(11, 96, 50000, 64)
+    d, i = knncuda.knn(ref, query, 32, "cublas")
+    gt_d, gt_i = oracle.knn_c(ref, query, 32, threads=THREADS)
+    ok, dacc, iacc = oracle.reference_criterion(d, i, gt_d, gt_i)
+    assert ok, (dacc, iacc)
+    d64, i64 = oracle.knn_f64(ref, query, 32, threads=THREADS)
+    check_exact(d, i, ref, query, d64, i64)
+    assert recall_at_k(i, i64) > 0.999
+
+
+def test_mixture_near_ties(knncuda, oracle, gpu):
+    """Clustered data (sigma 0.05 around 256 centres): dense near-ties."""
+    import workloads
+
+    w = workloads.WORKLOADS["mixture128"]
+    ref, query = workloads.generate(w, ref_nb=131072, query_nb=700)
+    dg, ig = knncuda.knn(ref, query, w.k, "global")
+    dc, ic = knncuda.knn(ref, query, w.k, "cublas")
+    assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
+    assert np.array_equal(ic, ig)
+    sample = np.arange(0, 700, 70)
+    qs = np.ascontiguousarray(query[:, sample])
+    d64, i64 = oracle.knn_f64(ref, qs, w.k, threads=THREADS)
+    check_exact(dc[:, sample], ic[:, sample], ref, qs, d64, i64)
+
+
+def test_headline_workload_mostly_certified(knncuda, gpu):
+    """1M x 256 mixture, k = 100: the BF16 scan certifies almost every query,
+    and the answer is the exact kernel's."""
+    import workloads
+
+    w = workloads.WORKLOADS["mixture256"]
+    ref, query = workloads.generate(w, query_nb=1024)
+    dg, ig = knncuda.knn(ref, query, w.k, "global")
+    dc, ic = knncuda.knn(ref, query, w.k, "cublas")
+    nfail = knncuda.last_fallback_count()
+    assert nfail <= 1024 // 50, nfail
+    assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
+    assert np.array_equal(ic, ig)
+
+
+def test_device_entry_cublas(knncuda, gpu):
+    import torch
+
+    ref, query = _uniform(21, 128, 65536, 200)
+    hd, hi = knncuda.knn(ref, query, 20, "global")
+    r = torch.from_numpy(ref).to(gpu)
+    q = torch.from_numpy(query).to(gpu)
+    d, i = knncuda.knn_device(r, q, 20, "cublas")
+    assert knncuda.sync_status() == 0
+    assert np.array_equal(d.cpu().numpy(), hd)
+    assert np.array_equal(i.cpu().numpy(), hi)
+
+
+def test_fallback_path_exercised(knncuda, gpu):
+    """Uniform data in 256-d with a small reference set: the BF16 error bound
+    is wide relative to the gaps, so many queries miss certification and take
+    the exact fallback; results must still equal knn_cuda_global."""
+    ref, query = _uniform(31, 256, 32768, 400)
+    dg, ig = knncuda.knn(ref, query, 100, "global")
+    dc, ic = knncuda.knn(ref, query, 100, "cublas")
+    assert knncuda.last_fallback_count() > 0
+    assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
+    assert np.array_equal(ic, ig)
