@@ -65,6 +65,26 @@ KNNB200_API int knnb200_knn_device(const float *ref, int ref_nb, long long ref_l
                        int query_nb, long long query_ld, int dim, int k, int method,
                        float *knn_dist, int *knn_index, long long out_ld, void *stream);
 
+/* The exact k-NN of knnb200_knn_device (method GLOBAL) for callers that
+ * cannot allocate device memory: their memory is handed out by their own
+ * pool, or cudaMalloc / cudaFree (which can stall the device) are not
+ * allowed where they call from.  It has no counterpart in the reference
+ * (whose functions allocate and free every buffer per call).  Inputs and
+ * outputs are caller-owned device memory as for knnb200_knn_device; the
+ * per-split scratch is a static 64 MiB device array inside this library,
+ * held on every GPU that loads it until exit.  Shapes needing more scratch
+ * than that (splits * query_nb * k * 8 bytes, splits as reported by
+ * knnb200_plan_splits) are rejected with KNNB200_ESCRATCH.  The first call
+ * on a device looks up the array's device address (make that first call
+ * before any stream capture).  All calls share the array and its status
+ * word: calls that overlap on the GPU race and must be serialised by the
+ * caller.  Returns after the results are written (KNNB200_OK, or
+ * KNNB200_ETIMEOUT if a kernel wait gave up). */
+KNNB200_API int knnb200_knn_device_noalloc(const float *ref, int ref_nb, long long ref_ld,
+                                           const float *query, int query_nb,
+                                           long long query_ld, int dim, int k, float *knn_dist,
+                                           int *knn_index, long long out_ld, void *stream);
+
 /* Synchronise `stream` and return the status of the last device-resident
  * call on the current device (KNNB200_OK or KNNB200_ETIMEOUT / ECUDA). */
 KNNB200_API int knnb200_sync_status(void *stream);

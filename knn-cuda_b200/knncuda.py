@@ -44,6 +44,7 @@ C_SYMBOLS = (
     "knnb200_sync_status", "knnb200_scratch_bytes", "knnb200_plan_splits",
     "knnb200_release_workspace", "knnb200_status_string", "knnb200_version",
     "knnb200_measure_fp32_peak", "knnb200_last_fallback_count",
+    "knnb200_knn_device_noalloc",
 )
 CXX_SYMBOLS = (
     "_Z15knn_cuda_globalPKfiS0_iiiPfPi",
@@ -81,6 +82,11 @@ def lib():
         L.knnb200_status_string.argtypes = [ctypes.c_int]
         L.knnb200_measure_fp32_peak.restype = ctypes.c_double
         L.knnb200_measure_fp32_peak.argtypes = [ctypes.c_int, ctypes.c_void_p]
+        L.knnb200_knn_device_noalloc.restype = ctypes.c_int
+        L.knnb200_knn_device_noalloc.argtypes = [
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int,
+            ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_longlong, ctypes.c_void_p]
         L.knnb200_last_fallback_count.restype = ctypes.c_int
         L.knnb200_last_fallback_count.argtypes = []
         L.knnb200_version.restype = ctypes.c_char_p
