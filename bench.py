@@ -9,13 +9,19 @@ reference set alone is 1 GiB), so no L2 flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-* ``--impl ours`` (default): ``value`` = device-resident throughput (inputs
-  already in HBM, CUDA events on the launching stream, max over ranks);
-  ``e2e`` = the same metric through the drop-in host entry point
-  ``knn_cuda_global`` with pinned host buffers, every host<->device copy
-  inside the timed region.  ``roofline`` reports the dominant kernel against
-  the FP32 CUDA-core peak measured on the same GPU in the same run.
-  ``cpu_baseline`` = the reference's own knn_c on the host cores (rank 0).
+* ``--impl ours`` (default) measures both tiers of the metric on the
+  device-resident entry point (inputs already in HBM, CUDA events on the
+  launching stream, max over ranks): ``exact_fp32`` (the fused direct-form
+  kernel behind knn_cuda_global) and ``bf16_rerank`` (tcgen05 BF16 scan +
+  exact FP32 re-rank behind knn_cublas; its answers are checked identical to
+  the exact tier's and against an FP64 brute force on sampled queries).
+  ``value`` is the bf16_rerank tier; ``e2e`` is the same metric through the
+  drop-in host entry point knn_cublas with pinned host buffers, every
+  host<->device copy inside the timed region.  ``roofline`` reports the
+  pass-2 tensor scan (per-kernel CUDA events inside the library) against the
+  measured bf16 peak; the exact tier carries its own FP32 roofline against
+  the FP32 FMA throughput measured in the same run.  ``cpu_baseline`` = the
+  reference's own knn_c on the host cores (rank 0).
 * ``--impl reference``: the reference's own CPU implementation (knn_c,
   code/test.cpp:129-175, built from its sources into oracle/_ref) on all
   host threads, each step a bounded sample of queries over the full
@@ -208,6 +214,64 @@ def cpu_sample_rate(ref, query, k, seconds_target: float, max_rounds: int = 1):
 # ---------------------------------------------------------------------------
 # our implementation
 # ---------------------------------------------------------------------------
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            m = json.load(f)
+        return {"bf16_tflops": float(m["bf16_tflops"]), "hbm_gbs": float(m["hbm_gbs"]),
+                "source": "measured (MEASURED_PEAKS.json, burst)"}
+    except (OSError, KeyError, ValueError):
+        return {"bf16_tflops": 1590.0, "hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def time_tier(knncuda, torch, D, stream, step, steps, clocks=None):
+    """Run `steps` timed steps; per-step sync to read the library's phase
+    timers.  Returns (ms per step, max over ranks; mean phase ms)."""
+    D.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    knncuda.set_phase_timing(True)
+    phase_sum, fallback = {}, 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+        torch.cuda.synchronize()
+        for k, v in knncuda.last_phase_times().items():
+            phase_sum[k] = phase_sum.get(k, 0.0) + v
+        fallback += knncuda.last_fallback_count()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    knncuda.set_phase_timing(False)
+    D.barrier()
+    clk = clocks.stop() if clocks else None
+    if knncuda.sync_status() != 0:
+        raise RuntimeError("device status error in timed region")
+    ms = D.max(e0.elapsed_time(e1) / steps)
+    return ms, {k: v / steps for k, v in phase_sum.items()}, fallback / steps, clk
+
+
+def fp64_recall(torch, ref_d, qry_d, idx, dist, k, sample):
+    """recall@k and max relative distance error of sampled queries against an
+    FP64 brute force computed on the GPU."""
+    r64 = ref_d.double()
+    hits, worst = 0, 0.0
+    for q in sample:
+        q64 = qry_d[:, q].double()
+        d2 = ((r64 - q64[:, None]) ** 2).sum(0)
+        top = torch.topk(d2, k, largest=False)
+        truth = set(top.indices.tolist())
+        mine = idx[:, q].long()
+        hits += len(truth & set(mine.tolist()))
+        exact = torch.sqrt(d2[mine])
+        rel = ((dist[:, q].double() - exact).abs() / exact.clamp_min(1e-12)).max().item()
+        worst = max(worst, rel)
+    return hits / (k * len(sample)), worst
+
+
 def run_ours(args, D: Dist):
     import torch
 
@@ -225,84 +289,102 @@ def run_ours(args, D: Dist):
     qry_h = torch.from_numpy(query).pin_memory()
     ref_d = ref_h.to(dev)
     qry_d = qry_h.to(dev)
-    dist_d = torch.empty((k, qn), dtype=torch.float32, device=dev)
-    idx_d = torch.empty((k, qn), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    peaks = measured_peaks()
+    warm = max(3, args.warmup)
+    tiers = {}
+    outs = {}
+    for name, method in (("exact_fp32", "global"), ("bf16_rerank", "cublas")):
+        dist_d = torch.empty((k, qn), dtype=torch.float32, device=dev)
+        idx_d = torch.empty((k, qn), dtype=torch.int32, device=dev)
 
-    def step():
-        knncuda.knn_device(ref_d, qry_d, k, "global", dist_d, idx_d, stream)
+        def step(method=method, dist_d=dist_d, idx_d=idx_d):
+            knncuda.knn_device(ref_d, qry_d, k, method, dist_d, idx_d, stream)
 
-    for _ in range(max(3, args.warmup)):
-        step()
-    torch.cuda.synchronize(dev)
-    if knncuda.sync_status() != 0:
-        raise RuntimeError("device status error during warm-up")
-    fp32_peak = knncuda.measure_fp32_peak(8192)
+        for _ in range(warm):
+            step()
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(D.local_rank) if name == "bf16_rerank" else None
+        ms, phases, fb, clk = time_tier(knncuda, torch, D, stream, step, args.steps, clocks)
+        outs[name] = (dist_d, idx_d)
+        tiers[name] = {"value": D.world * qn / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                       "phase_ms": phases, "fallback_queries_per_step": fb}
+        if clk is not None:
+            tiers[name]["clocks"] = clk
 
-    clocks = ClockSampler(D.local_rank)
-    D.barrier()
-    torch.cuda.synchronize(dev)
-    clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    D.barrier()
-    clk = clocks.stop()
-    ms_total = e0.elapsed_time(e1)
-    if knncuda.sync_status() != 0:
-        raise RuntimeError("device status error in timed region")
-    ms_step = D.max(ms_total / args.steps)
+    # identical answers, and recall / error against FP64 on sampled queries
+    same = bool(torch.equal(outs["exact_fp32"][0], outs["bf16_rerank"][0]) and
+                torch.equal(outs["exact_fp32"][1], outs["bf16_rerank"][1]))
+    sample = list(range(0, qn, max(1, qn // 32)))[:32]
+    recall, relerr = fp64_recall(torch, ref_d, qry_d, outs["bf16_rerank"][1],
+                                 outs["bf16_rerank"][0], k, sample)
+    tiers["bf16_rerank"].update(identical_to_exact=same, recall_at_k_fp64=recall,
+                                max_rel_dist_err_fp64=relerr,
+                                fp64_sample_queries=len(sample))
 
-    # end to end through the drop-in host entry point (pinned buffers)
+    # end to end through the drop-in host entry points (pinned buffers)
     ref_np, qry_np = ref_h.numpy(), qry_h.numpy()
     out_d = torch.empty((k, qn), dtype=torch.float32).pin_memory().numpy()
     out_i = torch.empty((k, qn), dtype=torch.int32).pin_memory().numpy()
-    knncuda.knn_cuda_global(ref_np, N, qry_np, qn, dim, k, out_d, out_i)   # warm (allocs)
-    D.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        if not knncuda.knn_cuda_global(ref_np, N, qry_np, qn, dim, k, out_d, out_i):
-            raise RuntimeError("knn_cuda_global failed")
-    e2e_s = D.max((time.perf_counter() - t0) / args.e2e_steps)
-    # the device-resident and host paths must agree
-    if not (np.array_equal(out_i, idx_d.cpu().numpy()) and
-            np.array_equal(out_d, dist_d.cpu().numpy())):
-        raise RuntimeError("host entry point and device path disagree")
+    e2e = {}
+    for name, fn in (("exact_fp32", knncuda.knn_cuda_global),
+                     ("bf16_rerank", knncuda.knn_cublas)):
+        fn(ref_np, N, qry_np, qn, dim, k, out_d, out_i)   # warm (workspace growth)
+        D.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            if not fn(ref_np, N, qry_np, qn, dim, k, out_d, out_i):
+                raise RuntimeError(f"{name} host entry failed")
+        e2e[name] = D.max((time.perf_counter() - t0) / args.e2e_steps)
+        if not (np.array_equal(out_i, outs["exact_fp32"][1].cpu().numpy()) and
+                np.array_equal(out_d, outs["exact_fp32"][0].cpu().numpy())):
+            raise RuntimeError(f"host entry {name} disagrees with the device path")
+        tiers[name]["e2e_value"] = D.world * qn / e2e[name]
 
-    splits = knncuda.plan_splits(N, qn, dim, k)
-    launches_per_step = 1 + (1 if splits > 1 else 0)
-    flops = 3.0 * dim * N * qn          # sub + mul + add per pair-dimension
-    achieved = flops / (ms_step * 1e-3)
-    value = D.world * qn / (ms_step * 1e-3)
+    head = tiers["bf16_rerank"]
+    d_pad = (dim + 63) // 64 * 64
+    pass2_ms = head["phase_ms"].get("tc_pass2")
+    flops = 2.0 * d_pad * N * qn
+    achieved = flops / (pass2_ms * 1e-3) if pass2_ms else None
+    peak = peaks["bf16_tflops"] * 1e12
+    n_fb = head["fallback_queries_per_step"]
+    launches = 8 + (4 if n_fb > 0 else 0)
+    ex = tiers["exact_fp32"]
+    ex_ms = ex["phase_ms"].get("exact_main", ex["ms_per_step"])
+    fp32_peak = knncuda.measure_fp32_peak(8192)
+    ex["roofline"] = {"bound": "fp32", "kernel": "knn_exact_kernel<8,128>",
+                      "achieved": 3.0 * dim * N * qn / (ex_ms * 1e-3) / 1e12,
+                      "peak": fp32_peak / 1e12, "unit": "TFLOP/s",
+                      "frac": 3.0 * dim * N * qn / (ex_ms * 1e-3) / fp32_peak,
+                      "algorithmic": "3*dim flops per (query, reference) pair",
+                      "peak_source": "FP32 FMA throughput measured in this run"}
 
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D.world,
-        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": D.world,
+        "steps": args.steps, "warmup": warm, "ms_per_step": head["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
         "data": "synthetic (seeded Gaussian mixture, 1024 unit-norm centres, sigma 0.1)",
         "impl": "ours",
-        "config": dict(w.describe(), query_nb=qn, tier="exact-fp32 (knn_cuda_global path)",
+        "config": dict(w.describe(), query_nb=qn,
+                       tier="bf16_rerank: tcgen05 BF16 scan + exact FP32 re-rank (knn_cublas)",
                        parallelism=f"query-sharded replicas x{D.world}",
                        l2="inputs larger than L2 (1 GiB reference set); no flush"),
-        "e2e": {"value": D.world * qn / e2e_s, "unit": UNIT,
+        "e2e": {"value": D.world * qn / e2e["bf16_rerank"], "unit": UNIT,
                 "h2d_bytes_per_step": int(ref.nbytes + query.nbytes),
                 "d2h_bytes_per_step": int(out_d.nbytes + out_i.nbytes),
-                "api": "knn_cuda_global (drop-in C-ABI, pinned host buffers)",
-                "ms_per_step": e2e_s * 1e3},
-        "gpu_launches": launches_per_step * args.steps,
-        "roofline": {"bound": "fp32", "achieved": achieved / 1e12,
-                     "peak": fp32_peak / 1e12, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak if fp32_peak > 0 else None,
-                     "traffic": NCU_TRAFFIC_BYTES.get("knn_exact_kernel"),
-                     "kernel": "knn_exact_kernel<8,128>",
-                     "algorithmic": "3*dim flops per (query, reference) pair",
-                     "peak_source": "FP32 FMA throughput measured in this run "
-                                    "(knnb200_measure_fp32_peak, 2 flops per FMA)"},
-        "clocks": clk,
+                "api": "knn_cublas (drop-in C-ABI, pinned host buffers)",
+                "ms_per_step": e2e["bf16_rerank"] * 1e3},
+        "gpu_launches": launches * args.steps,
+        "roofline": {"bound": "tensor", "kernel": "knn_tc_scan_kernel<1> (pass-2 scan)",
+                     "achieved": achieved / 1e12 if achieved else None,
+                     "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                     "frac": achieved / peak if achieved else None,
+                     "traffic": NCU_TRAFFIC_BYTES.get("knn_tc_scan_kernel<1>"),
+                     "algorithmic": "2*d_pad flops per (query, reference) pair, d_pad=256",
+                     "peak_source": peaks["source"]},
+        "clocks": head.get("clocks"),
+        "tiers": tiers,
+        "speedup_bf16_vs_exact": head["value"] / ex["value"],
     }
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
         rates, threads, desc, kind, qs = cpu_sample_rate(ref, query, k, args.cpu_seconds)

@@ -94,6 +94,7 @@ struct Workspace {
     cudaEvent_t last_done = nullptr;   // orders device-resident calls on this device
     Buffer ref, qry, dist, idx, scratch, status;
     Buffer tcref;                      // prepared reference set of the tensor-core path
+    PhaseTimer timer;                  // optional per-phase device timing
     int *status_host = nullptr;        // pinned status word for the host path
     int *nfail_host = nullptr;         // pinned count of uncertified tensor-core queries
 
@@ -110,6 +111,8 @@ struct Workspace {
             return false;
         if (cudaMallocHost(reinterpret_cast<void **>(&nfail_host), sizeof(int)) != cudaSuccess)
             return false;
+        for (int i = 0; i < PhaseTimer::kMaxMarks; ++i)
+            if (cudaEventCreate(&timer.ev[i]) != cudaSuccess) return false;
         init = true;
         return true;
     }
@@ -136,14 +139,18 @@ size_t scratch_for(int method, int N, int Q, int d, int k, int num_sms) {
 // knn_cublas runs the tensor-core expansion path when the shape qualifies
 // (it synchronises the stream once, to recompute uncertified queries);
 // everything else runs the fused exact kernel.
-int enqueue(Workspace &ws, const ExactProblem &p, int method, cudaStream_t st) {
+int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st) {
     *ws.nfail_host = 0;
-    if (!exact_supported_k(p.k)) return kErrUnsupported;
+    if (!exact_supported_k(p0.k)) return kErrUnsupported;
+    ExactProblem p = p0;
+    p.timer = &ws.timer;
+    ws.timer.begin(st);
     if (!use_tc(method, p.N, p.Q, p.d, p.k)) return launch_exact(p, st);
     if (!ws.tcref.ensure(tc_ref_bytes(p.N, p.d))) return kErrNoMemory;
     const TcRefView rv = tc_carve_ref(ws.tcref.ptr, p.N, p.d);
     int rc = tc_prepare_ref(rv, p.ref, p.N, p.ldr, p.d, st);
     if (rc != kOk) return rc;
+    ws.timer.mark(st, kPhaseTcPrepRef);
     TcProblem t;
     t.ref = p.ref;
     t.N = p.N;
@@ -160,6 +167,7 @@ int enqueue(Workspace &ws, const ExactProblem &p, int method, cudaStream_t st) {
     t.scratch_bytes = p.scratch_bytes;
     t.status = p.status;
     t.num_sms = p.num_sms;
+    t.timer = &ws.timer;
     return launch_tc(t, rv, st, ws.nfail_host);
 }
 
@@ -440,6 +448,33 @@ const char *knnb200_status_string(int code) {
         case KNNB200_ETENSORMAP: return "TMA descriptor encoding failed";
         default: return "unknown";
     }
+}
+
+void knnb200_set_phase_timing(int enable) {
+    Workspace *ws = nullptr;
+    if (current_workspace(ws) != kOk) return;
+    std::lock_guard<std::mutex> lock(ws->mu);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!ws->setup(dev)) return;
+    ws->timer.on = enable != 0;
+    ws->timer.marks = 0;
+}
+
+int knnb200_last_phase_times(float *ms, int n) {
+    if (!ms || n <= 0) return 0;
+    for (int i = 0; i < n; ++i) ms[i] = -1.f;
+    Workspace *ws = nullptr;
+    if (current_workspace(ws) != kOk || !ws->init) return 0;
+    std::lock_guard<std::mutex> lock(ws->mu);
+    const PhaseTimer &t = ws->timer;
+    if (t.marks < 2 || cudaEventSynchronize(t.ev[t.marks - 1]) != cudaSuccess) return 0;
+    for (int i = 1; i < t.marks; ++i) {
+        float x = 0.f;
+        if (t.phase[i] < n && cudaEventElapsedTime(&x, t.ev[i - 1], t.ev[i]) == cudaSuccess)
+            ms[t.phase[i]] = (ms[t.phase[i]] < 0.f ? 0.f : ms[t.phase[i]]) + x;
+    }
+    return kNumPhases;
 }
 
 int knnb200_last_fallback_count(void) {

@@ -467,6 +467,7 @@ int launch_exact(const ExactProblem &p, cudaStream_t st) {
         default: e = launch_t<4, 256>(mr, mq, a, qtiles, st); break;
     }
     if (e != cudaSuccess) return kErrLaunch;
+    if (p.timer) p.timer->mark(st, kPhaseExactMain);
     if (s.splits > 1) {
         const size_t per_warp = (size_t)s.splits * p.k * 8;
         int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (160u * 1024u) / per_warp));
@@ -478,6 +479,7 @@ int launch_exact(const ExactProblem &p, cudaStream_t st) {
         knn_merge_splits_kernel<<<(p.Q + wpb - 1) / wpb, wpb * 32, smem, st>>>(
             a.part, s.splits, p.Q, p.k, p.out_dist, p.out_idx, p.ld_out);
         if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+        if (p.timer) p.timer->mark(st, kPhaseExactMerge);
     }
     return kOk;
 }

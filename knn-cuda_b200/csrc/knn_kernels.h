@@ -24,6 +24,39 @@ enum Result : int {
     kErrTensorMap = 9,
 };
 
+// Optional per-phase device timing: CUDA events recorded on the launching
+// stream between the kernels of one call.
+enum Phase : int {
+    kPhaseTcPrepRef = 0,
+    kPhaseTcPrepQuery = 1,
+    kPhaseTcPass1 = 2,
+    kPhaseTcThreshold = 3,
+    kPhaseTcPass2 = 4,
+    kPhaseTcRerank = 5,
+    kPhaseTcFallback = 6,
+    kPhaseExactMain = 7,
+    kPhaseExactMerge = 8,
+    kNumPhases = 9,
+};
+
+struct PhaseTimer {
+    static constexpr int kMaxMarks = 16;
+    bool on = false;
+    int marks = 0;                    // events recorded so far in this call
+    int phase[kMaxMarks];             // phase ended by event i (i >= 1)
+    cudaEvent_t ev[kMaxMarks];
+    void begin(cudaStream_t st) {
+        marks = 0;
+        if (on) cudaEventRecord(ev[marks++], st);
+    }
+    void mark(cudaStream_t st, int ph) {
+        if (on && marks > 0 && marks < kMaxMarks) {
+            phase[marks] = ph;
+            cudaEventRecord(ev[marks++], st);
+        }
+    }
+};
+
 // Kernel-side arguments of the fused exact kernel.
 struct ExactArgs {
     int N, Q, d, k;
@@ -52,6 +85,7 @@ struct ExactProblem {
     int *status;
     int num_sms;
     int force_splits;   // 0 = automatic
+    PhaseTimer *timer = nullptr;
 };
 
 // Encode a 2-D tensor map (cols = contiguous axis, row pitch ld_elems) with
@@ -93,6 +127,7 @@ struct TcProblem {
     size_t scratch_bytes;
     int *status;
     int num_sms;
+    PhaseTimer *timer = nullptr;
 };
 
 bool tc_supported(int N, int Q, int d, int k);

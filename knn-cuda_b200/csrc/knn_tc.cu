@@ -596,6 +596,8 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
         P.qry, P.Q, P.ldq, P.d, p.d_pad, qB, nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    PhaseTimer *tm = P.timer;
+    if (tm) tm->mark(st, kPhaseTcPrepQuery);
 
     CUtensorMap tmA, tmB;
     if (!encode_bf16_kmajor(&tmA, qB, P.Q, p.d_pad)) return kErrTensorMap;
@@ -625,9 +627,12 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
 
     a.tile_stride = p.stride1;
     knn_tc_scan_kernel<0><<<grid, TC_THREADS, TC_SMEM, st>>>(tmA, tmB, a);
+    if (tm) tm->mark(st, kPhaseTcPass1);
     tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, p.splits, P.Q, thr, count);
+    if (tm) tm->mark(st, kPhaseTcThreshold);
     a.tile_stride = 1;
     knn_tc_scan_kernel<1><<<grid, TC_THREADS, TC_SMEM, st>>>(tmA, tmB, a);
+    if (tm) tm->mark(st, kPhaseTcPass2);
     if (cudaMemsetAsync(nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
     int cpow = 1;
     while (cpow < p.cmax) cpow <<= 1;
@@ -639,6 +644,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
                                               R.rmax_bits, thr, cand, count, p.cmax, P.k,
                                               P.out_dist, P.out_idx, P.ld_out, fail, nfail);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    if (tm) tm->mark(st, kPhaseTcRerank);
 
     // uncertified queries -> exact kernel
     int nf = 0;
@@ -672,11 +678,14 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     x.status = P.status;
     x.num_sms = P.num_sms;
     x.force_splits = splits;
+    x.timer = nullptr;
     int rc = launch_exact(x, st);
     if (rc != kOk) return rc;
     scatter_results_kernel<<<dim3((nf + 127) / 128, P.k), 128, 0, st>>>(
         sd, si, ldf, fail, nf, P.out_dist, P.out_idx, P.ld_out);
-    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    if (tm) tm->mark(st, kPhaseTcFallback);
+    return kOk;
 }
 
 }  // namespace knnb200

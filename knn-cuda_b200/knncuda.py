@@ -44,8 +44,10 @@ C_SYMBOLS = (
     "knnb200_sync_status", "knnb200_scratch_bytes", "knnb200_plan_splits",
     "knnb200_release_workspace", "knnb200_status_string", "knnb200_version",
     "knnb200_measure_fp32_peak", "knnb200_last_fallback_count",
-    "knnb200_knn_device_noalloc",
+    "knnb200_knn_device_noalloc", "knnb200_set_phase_timing", "knnb200_last_phase_times",
 )
+PHASES = ("tc_prep_ref", "tc_prep_query", "tc_pass1", "tc_threshold", "tc_pass2", "tc_rerank",
+          "tc_fallback", "exact_main", "exact_merge")
 CXX_SYMBOLS = (
     "_Z15knn_cuda_globalPKfiS0_iiiPfPi",
     "_Z16knn_cuda_texturePKfiS0_iiiPfPi",
@@ -87,6 +89,10 @@ def lib():
             ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int,
             ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_longlong, ctypes.c_void_p]
+        L.knnb200_set_phase_timing.restype = None
+        L.knnb200_set_phase_timing.argtypes = [ctypes.c_int]
+        L.knnb200_last_phase_times.restype = ctypes.c_int
+        L.knnb200_last_phase_times.argtypes = [_FP, ctypes.c_int]
         L.knnb200_last_fallback_count.restype = ctypes.c_int
         L.knnb200_last_fallback_count.argtypes = []
         L.knnb200_version.restype = ctypes.c_char_p
@@ -209,6 +215,17 @@ def measure_fp32_peak(iters: int = 4096, stream=None) -> float:
     if stream is None:
         stream = torch.cuda.current_stream()
     return lib().knnb200_measure_fp32_peak(iters, ctypes.c_void_p(stream.cuda_stream))
+
+
+def set_phase_timing(enable: bool) -> None:
+    lib().knnb200_set_phase_timing(1 if enable else 0)
+
+
+def last_phase_times() -> dict:
+    """{phase name: ms} for the phases the last timed call ran."""
+    buf = (ctypes.c_float * len(PHASES))()
+    lib().knnb200_last_phase_times(buf, len(PHASES))
+    return {name: float(v) for name, v in zip(PHASES, buf) if v >= 0}
 
 
 def last_fallback_count() -> int:
