@@ -107,10 +107,12 @@ KNNB200_API const char *knnb200_status_string(int code);
  * the roofline denominator of the FP32 direct-form path. */
 KNNB200_API double knnb200_measure_fp32_peak(int iters, void *stream);
 
-/* Number of queries of the last knn_cublas-method call on the current device
- * that failed the tensor-core certification and were recomputed by the exact
- * kernel (0 when the call ran the exact kernel only). */
-KNNB200_API int knnb200_last_fallback_count(void);
+/* For the last knn_cublas-method call on the current device: the number of
+ * queries that failed the first tensor-core certification and were scanned a
+ * second time (*second_scan), and of those the number recomputed by the
+ * exact kernel (*exact).  Both 0 when the call ran the exact kernel only.
+ * Either pointer may be NULL. */
+KNNB200_API void knnb200_last_fallback_counts(int *second_scan, int *exact);
 
 /* Per-phase device timing of the calls on the current device (CUDA events on
  * the launching stream between the kernels of a call).  Off by default. */

@@ -96,7 +96,7 @@ struct Workspace {
     Buffer tcref;                      // prepared reference set of the tensor-core path
     PhaseTimer timer;                  // optional per-phase device timing
     int *status_host = nullptr;        // pinned status word for the host path
-    int *nfail_host = nullptr;         // pinned count of uncertified tensor-core queries
+    int *tc_stats = nullptr;           // pinned: [0] second-scan queries, [1] exact fallbacks
 
     bool setup(int dev) {
         if (init) return true;
@@ -109,7 +109,7 @@ struct Workspace {
         if (!status.ensure(sizeof(int))) return false;
         if (cudaMallocHost(reinterpret_cast<void **>(&status_host), sizeof(int)) != cudaSuccess)
             return false;
-        if (cudaMallocHost(reinterpret_cast<void **>(&nfail_host), sizeof(int)) != cudaSuccess)
+        if (cudaMallocHost(reinterpret_cast<void **>(&tc_stats), 4 * sizeof(int)) != cudaSuccess)
             return false;
         for (int i = 0; i < PhaseTimer::kMaxMarks; ++i)
             if (cudaEventCreate(&timer.ev[i]) != cudaSuccess) return false;
@@ -140,7 +140,7 @@ size_t scratch_for(int method, int N, int Q, int d, int k, int num_sms) {
 // (it synchronises the stream once, to recompute uncertified queries);
 // everything else runs the fused exact kernel.
 int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st) {
-    *ws.nfail_host = 0;
+    ws.tc_stats[0] = ws.tc_stats[1] = 0;
     if (!exact_supported_k(p0.k)) return kErrUnsupported;
     ExactProblem p = p0;
     p.timer = &ws.timer;
@@ -168,7 +168,7 @@ int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st) 
     t.status = p.status;
     t.num_sms = p.num_sms;
     t.timer = &ws.timer;
-    return launch_tc(t, rv, st, ws.nfail_host);
+    return launch_tc(t, rv, st, ws.tc_stats);
 }
 
 int current_workspace(Workspace *&ws) {
@@ -477,11 +477,14 @@ int knnb200_last_phase_times(float *ms, int n) {
     return kNumPhases;
 }
 
-int knnb200_last_fallback_count(void) {
+void knnb200_last_fallback_counts(int *second_scan, int *exact) {
+    if (second_scan) *second_scan = 0;
+    if (exact) *exact = 0;
     Workspace *ws = nullptr;
-    if (current_workspace(ws) != kOk || !ws->init) return 0;
+    if (current_workspace(ws) != kOk || !ws->init) return;
     std::lock_guard<std::mutex> lock(ws->mu);
-    return *ws->nfail_host;
+    if (second_scan) *second_scan = ws->tc_stats[0];
+    if (exact) *exact = ws->tc_stats[1];
 }
 
 const char *knnb200_version(void) { return "knnb200 0.1.0 (sm_100a)"; }

@@ -391,7 +391,9 @@ bool choose_shape(int N, int Q, int d, int k, int num_sms, ExactShape &s) {
     const double warm = 256.0 / (s.n_dchunks * EX_BD);
     int best = 1;
     double best_t = 1e300;
-    int max_s = std::min(s.n_rtiles, 64);
+    // up to 256 splits, while each query's merge input (splits * k keys) fits
+    // one warp's shared-memory slab in the merge kernel
+    int max_s = std::min(s.n_rtiles, std::min(256, (160 * 1024) / (8 * k)));
     // keep the per-split partial lists under 1 GiB of scratch
     const long long per_split = (long long)Q * k * 8;
     max_s = (int)std::max<long long>(1, std::min<long long>(max_s, (1ll << 30) / per_split));

@@ -136,9 +136,11 @@ size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms);
 TcRefView tc_carve_ref(void *mem, int N, int d);
 int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, int d,
                    cudaStream_t st);
-// Queues the tensor-core k-NN; synchronises once to learn how many queries
-// failed certification (written to *host_nfail, pinned) and recomputes them
-// with the exact kernel.
-int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_nfail);
+// Queues the tensor-core k-NN.  Synchronises once to learn how many queries
+// failed certification; those get a second scan with thresholds that
+// certify, and queries whose candidate list overflowed are recomputed by the
+// exact kernel.  host_stats (pinned, 3 ints): [0] queries given the second
+// scan, [1] queries recomputed by the exact kernel, [2] scratch.
+int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_stats);
 
 }  // namespace knnb200

@@ -46,7 +46,7 @@ constexpr int TC_QT = 2 * TC_BM;      // queries per CTA (two A tiles share each
 constexpr int TC_BN = 128;            // reference points per tile
 constexpr int TC_BK = 64;             // K block: 64 bf16 = 128 B (one swizzle row)
 constexpr int TC_KBMAX = 4;           // d_pad <= 256
-constexpr int TC_STAGES = 4;
+constexpr int TC_STAGES = 5;
 constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;   // 16 KB (A or B K-block tile)
 constexpr int TC_KS = 16;             // pass-1 per-row list length
 constexpr int TC_THREADS = 192;       // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
@@ -223,6 +223,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
             for (int i = 0; i < TC_KS; ++i) L[h][i] = INFINITY;
         }
+        // Norms of the next tile are fetched into registers before waiting on
+        // its accumulator, so the global-load latency overlaps the wait.
+        float rn_next[TC_BN / 32];
+        auto fetch_rn = [&](int jj) {
+#pragma unroll
+            for (int i = 0; i < TC_BN / 32; ++i) {
+                const int ridx = (first + jj * G) * TC_BN + i * 32 + lane;
+                rn_next[i] = (jj < n_my && ridx < a.N) ? __ldg(a.rn + ridx) : INFINITY;
+            }
+        };
+        fetch_rn(0);
+        float *rnb = rn_s + (warp - 2) * TC_BN;   // this warp's copy of the tile norms
         for (int j = 0; j < n_my; ++j) {
             const int b = j & 1;
             const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
@@ -235,40 +247,60 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             tc_fence_after();
             const int tile = first + j * G;
-            // this warp's copy of the tile's reference norms (padding -> +inf)
-            float *rnb = rn_s + (warp - 2) * TC_BN;
             __syncwarp();
 #pragma unroll
-            for (int i = 0; i < TC_BN / 32; ++i) {
-                const int ridx = tile * TC_BN + i * 32 + lane;
-                rnb[i * 32 + lane] = ridx < a.N ? a.rn[ridx] : INFINITY;
-            }
+            for (int i = 0; i < TC_BN / 32; ++i) rnb[i * 32 + lane] = rn_next[i];
             __syncwarp();
+            fetch_rn(j + 1);
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
 #pragma unroll 1
-                for (int c = 0; c < TC_BN / 32; ++c) {
-                    uint32_t v[32];
-                    tmem_ld32(tmem + ((uint32_t)(qd * 32) << 16) +
-                                  (uint32_t)((b * 2 + h) * TC_BM + c * 32),
-                              v);
-                    tmem_ld_wait(v);
-                    const int cbase = tile * TC_BN + c * 32;
+                for (int c = 0; c < TC_BN / 32; c += 2) {
+                    // two TMEM loads in flight per wait
+                    uint32_t v0[32], v1[32];
+                    const uint32_t tbase = tmem + ((uint32_t)(qd * 32) << 16) +
+                                           (uint32_t)((b * 2 + h) * TC_BM + c * 32);
+                    tmem_ld32(tbase, v0);
+                    tmem_ld32(tbase + 32, v1);
+                    tmem_ld_wait(v0);
+                    tmem_ld_wait(v1);
 #pragma unroll
-                    for (int e = 0; e < 32; ++e) {
-                        const float av = fmaf(-2.0f, __uint_as_float(v[e]), rnb[c * 32 + e]);
-                        if (MODE == 1) {
-                            if (av < thr[h]) {
+                    for (int half = 0; half < 2; ++half) {
+                        const uint32_t *v = half ? v1 : v0;
+                        const float *rc = rnb + (c + half) * 32;
+                        float av[32];
+#pragma unroll
+                        for (int e = 0; e < 32; e += 2) {
+                            const float2 r2 = *reinterpret_cast<const float2 *>(rc + e);
+                            const f32x2_t t = f2_fma(f2_pack(-2.0f, -2.0f),
+                                                     f2_pack(__uint_as_float(v[e]),
+                                                             __uint_as_float(v[e + 1])),
+                                                     f2_pack(r2.x, r2.y));
+                            av[e] = f2_lo(t);
+                            av[e + 1] = f2_hi(t);
+                        }
+                        const float lim = MODE == 1 ? thr[h] : L[h][TC_KS - 1];
+                        uint32_t m = 0;
+#pragma unroll
+                        for (int e = 0; e < 32; ++e) m |= (av[e] < lim ? 1u : 0u) << e;
+                        const int cbase = tile * TC_BN + (c + half) * 32;
+                        while (m) {   // rare after the first tiles
+                            const int e = __ffs(m) - 1;
+                            m &= m - 1;
+                            float x = av[0];
+#pragma unroll
+                            for (int t = 1; t < 32; ++t) x = (t == e) ? av[t] : x;
+                            if (MODE == 1) {
                                 const int pos = atomicAdd(&a.count[qrow[h]], 1);
                                 if (pos < a.cmax)
                                     a.cand[(size_t)qrow[h] * a.cmax + pos] = cbase + e;
-                            }
-                        } else if (av < L[h][TC_KS - 1]) {
+                            } else if (x < L[h][TC_KS - 1]) {
 #pragma unroll
-                            for (int i = TC_KS - 1; i > 0; --i)
-                                L[h][i] = av < L[h][i - 1] ? L[h][i - 1]
-                                                           : (av < L[h][i] ? av : L[h][i]);
-                            L[h][0] = fminf(L[h][0], av);
+                                for (int i = TC_KS - 1; i > 0; --i)
+                                    L[h][i] = x < L[h][i - 1] ? L[h][i - 1]
+                                                              : (x < L[h][i] ? x : L[h][i]);
+                                L[h][0] = fminf(L[h][0], x);
+                            }
                         }
                     }
                 }
@@ -292,6 +324,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     tc_fence_after();
     if (warp == 1) tmem_dealloc(tmem, TC_TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
+// error bound of the BF16 expansion (see the file comment)
+// ---------------------------------------------------------------------------
+KNN_DI float tc_error_bound(float qq, float r2, float T, int d_pad) {
+    const float g = (float)d_pad * 2.384185791015625e-07f;   // d_pad * 2^-22
+    const float eps = 0.0078125f + 1.52587890625e-05f + g;    // 2^-7 + 2^-16 + d_pad 2^-22
+    return 2.f * eps * sqrtf(qq * r2) + g * (r2 + qq) + 9.5367431640625e-07f * (fabsf(T) + qq);
 }
 
 // ---------------------------------------------------------------------------
@@ -342,8 +383,12 @@ __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld,
     }
 }
 
-// T_q = KS-th smallest of the per-split pass-1 lists; resets candidate counts.
+// Emission threshold: the KS-th smallest of the per-split pass-1 lists plus
+// the error bound E_q (so that the k-th exact distance only has to lie below
+// the sample's KS-th approximate one to certify); resets candidate counts.
 __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
+                                    const float *__restrict__ qn,
+                                    const unsigned *__restrict__ rmax_bits, int d_pad,
                                     float *__restrict__ thr, int *__restrict__ count) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= Q) return;
@@ -361,20 +406,27 @@ __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
             L[0] = fminf(L[0], v);
         }
     }
-    thr[q] = L[TC_KS - 1];
+    const float T = L[TC_KS - 1];
+    thr[q] = T + tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T, d_pad);
     count[q] = 0;
 }
 
 // Exact FP32 re-rank of each query's candidates + certification.
-// One block (256 threads) per query.
+// One block (256 threads) per query.  An uncertified query is appended to
+// fail_list and retry[q] receives a threshold for a second scan: when it had
+// at least k candidates, their k-th exact distance D_k bounds the true k-th
+// from above, so every point of the true top-k has a < D_k (1+g) + E -
+// ||q||^2 and a second scan emitting below D_k (1+g) + 2.5 E - ||q||^2 passes
+// the check; with fewer than k candidates the threshold is widened by 8 E;
+// an overflowing list gets NaN (no second scan: exact kernel).
 __global__ void __launch_bounds__(256)
     tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
                      const float *__restrict__ qry, long long ldq, const float *__restrict__ qn,
                      const unsigned *__restrict__ rmax_bits, const float *__restrict__ thr,
                      const int *__restrict__ cand, const int *__restrict__ count, int cmax,
                      int k, float *__restrict__ out_dist, int *__restrict__ out_idx,
-                     long long ld_out, int *__restrict__ fail_list,
-                     int *__restrict__ n_fail) {
+                     long long ld_out, int *__restrict__ fail_list, int *__restrict__ n_fail,
+                     float *__restrict__ retry) {
     extern __shared__ unsigned char rsm[];
     float *qv = reinterpret_cast<float *>(rsm);
     unsigned long long *keys =
@@ -383,7 +435,15 @@ __global__ void __launch_bounds__(256)
     const int q = blockIdx.x, tid = threadIdx.x;
     const int c = count[q];
     if (c > cmax || c < k) {
-        if (tid == 0) fail_list[atomicAdd(n_fail, 1)] = q;
+        if (tid == 0) {
+            fail_list[atomicAdd(n_fail, 1)] = q;
+            // too few candidates: the threshold was low; widen it by 8 E.
+            // An overflowing list goes to the exact kernel (NaN).
+            const float T = thr[q];
+            retry[q] = c < k ? T + 8.f * tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T,
+                                                         d_pad)
+                             : __int_as_float(0x7fc00000);
+        }
         return;
     }
     for (int dd = tid; dd < d_pad; dd += blockDim.x)
@@ -434,13 +494,14 @@ __global__ void __launch_bounds__(256)
         const float qq = qn[q];
         const float r2 = __uint_as_float(*rmax_bits);
         const float T = thr[q];
-        const float eps = 0.0078125f + 1.52587890625e-05f + (float)d_pad * 2.384185791015625e-07f;
-        const float E = 2.f * eps * sqrtf(qq * r2) +
-                        (float)d_pad * 2.384185791015625e-07f * (r2 + qq) +
-                        9.5367431640625e-07f * (fabsf(T) + qq);
-        const float lhs = dk * (1.f + (float)d_pad * 2.384185791015625e-07f) + E;
-        failed = !(lhs < T + qq);
-        if (failed) fail_list[atomicAdd(n_fail, 1)] = q;
+        const float E = tc_error_bound(qq, r2, T, d_pad);
+        const float dkg = dk * (1.f + (float)d_pad * 2.384185791015625e-07f);
+        failed = !(dkg + E < T + qq);
+        if (failed) {
+            fail_list[atomicAdd(n_fail, 1)] = q;
+            const float T2 = dkg - qq;
+            retry[q] = T2 + 2.5f * tc_error_bound(qq, r2, T2, d_pad);
+        }
     }
     __syncthreads();
     if (failed) return;
@@ -470,6 +531,17 @@ __global__ void scatter_results_kernel(const float *__restrict__ sd, const int *
     if (i < m) {
         out_dist[(size_t)j * ld_out + list[i]] = sd[(size_t)j * lds + i];
         out_idx[(size_t)j * ld_out + list[i]] = si[(size_t)j * lds + i];
+    }
+}
+
+// Second-chance scan of the uncertified queries: compact thresholds.
+__global__ void tc_retry_prep_kernel(const int *__restrict__ list, int m,
+                                     const float *__restrict__ retry, float *__restrict__ thr,
+                                     int *__restrict__ count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) {
+        thr[i] = retry[list[i]];
+        count[i] = 0;
     }
 }
 
@@ -543,7 +615,7 @@ static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
 
 size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     const TcPlan p = plan_tc(N, Q, d, k, num_sms);
-    size_t b = (size_t)p.qtiles * TC_QT * p.d_pad * 2 + (size_t)Q * 4 * 4 + 16;
+    size_t b = (size_t)p.qtiles * TC_QT * p.d_pad * 2 + (size_t)Q * 4 * 6 + 16;
     b += (size_t)p.splits * Q * TC_KS * 4;
     b += (size_t)Q * p.cmax * 4;
     b += fallback_bytes(N, Q, d, k, num_sms);   // worst case: every query uncertified
@@ -571,116 +643,174 @@ TcRefView tc_carve_ref(void *mem, int N, int d) {
     return v;
 }
 
-int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_nfail) {
+namespace {
+
+// Pass-2 scan + exact re-rank for a batch of queries whose BF16 copy is qB
+// (rows Q) and whose thresholds are thr.
+int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cudaStream_t st,
+                    const __nv_bfloat16 *qB, int Q, const float *qry, long long ldq,
+                    const float *qn, const float *thr, int *count, int *cand, float *out_dist,
+                    int *out_idx, long long ld_out, int *fail, int *nfail, float *retry) {
+    const TcPlan pb = plan_tc(P.N, Q, P.d, P.k, P.num_sms);
+    CUtensorMap tmA, tmB;
+    if (!encode_bf16_kmajor(&tmA, qB, Q, p.d_pad)) return kErrTensorMap;
+    if (!encode_bf16_kmajor(&tmB, R.refB, P.N, p.d_pad)) return kErrTensorMap;
+    TcArgs a;
+    a.N = P.N;
+    a.Q = Q;
+    a.kb_count = p.kb;
+    a.n_tiles = p.n_tiles;
+    a.n_splits = pb.splits;
+    a.tile_stride = 1;
+    a.rn = R.rn;
+    a.thr = thr;
+    a.p1 = nullptr;
+    a.cand = cand;
+    a.count = count;
+    a.cmax = p.cmax;
+    a.status = P.status;
+    knn_tc_scan_kernel<1><<<dim3(pb.qtiles, pb.splits), TC_THREADS, TC_SMEM, st>>>(tmA, tmB, a);
+    if (P.timer) P.timer->mark(st, kPhaseTcPass2);
+    if (cudaMemsetAsync(nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
+    int cpow = 1;
+    while (cpow < p.cmax) cpow <<= 1;
+    const size_t rsmem = (((size_t)p.d_pad * 4 + 15) & ~size_t(15)) + (size_t)cpow * 8;
+    if (cudaFuncSetAttribute(tc_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)rsmem) != cudaSuccess)
+        return kErrLaunch;
+    tc_rerank_kernel<<<Q, 256, rsmem, st>>>(R.refT, P.d, p.d_pad, qry, ldq, qn, R.rmax_bits,
+                                            thr, cand, count, p.cmax, P.k, out_dist, out_idx,
+                                            ld_out, fail, nfail, retry);
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    if (P.timer) P.timer->mark(st, kPhaseTcRerank);
+    return kOk;
+}
+
+int read_count(const int *dev, int *host_pinned, cudaStream_t st, int &out) {
+    if (cudaMemcpyAsync(host_pinned, dev, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return kErrCuda;
+    out = *host_pinned;
+    return kOk;
+}
+
+}  // namespace
+
+int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_stats) {
+    int *host_tmp = host_stats + 2;
+    host_stats[0] = host_stats[1] = 0;
     const TcPlan p = plan_tc(P.N, P.Q, P.d, P.k, P.num_sms);
     if (!tc_supported(P.N, P.Q, P.d, P.k)) return kErrUnsupported;
     Carve cv{static_cast<unsigned char *>(P.scratch), 0, P.scratch_bytes};
     __nv_bfloat16 *qB = cv.take<__nv_bfloat16>((size_t)p.qtiles * TC_QT * p.d_pad);
     float *qn = cv.take<float>(P.Q);
     float *thr = cv.take<float>(P.Q);
+    float *retry = cv.take<float>(P.Q);
     int *count = cv.take<int>(P.Q);
     int *fail = cv.take<int>(P.Q);
+    int *fail2 = cv.take<int>(P.Q);
     int *nfail = cv.take<int>(4);
     float *p1 = cv.take<float>((size_t)p.splits * P.Q * TC_KS);
     int *cand = cv.take<int>((size_t)P.Q * p.cmax);
-    const long long ldf = (P.Q + 3) / 4 * 4;       // fallback buffers, sized for all queries
+    const long long ldf = (P.Q + 3) / 4 * 4;       // second-chance buffers, sized for all queries
     float *qsub = cv.take<float>((size_t)P.d * ldf);
     float *sd = cv.take<float>((size_t)P.k * ldf);
     int *si = cv.take<int>((size_t)P.k * ldf);
     unsigned char *xs = cv.take<unsigned char>(0);
     const size_t xcap = P.scratch_bytes > cv.used ? P.scratch_bytes - cv.used : 0;
     if (cv.used > P.scratch_bytes) return kErrScratch;
+    PhaseTimer *tm = P.timer;
 
     // queries: norms + BF16 K-major copy
     tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, qn, nullptr);
     tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
         P.qry, P.Q, P.ldq, P.d, p.d_pad, qB, nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-    PhaseTimer *tm = P.timer;
     if (tm) tm->mark(st, kPhaseTcPrepQuery);
+    if (cudaFuncSetAttribute(knn_tc_scan_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TC_SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(knn_tc_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TC_SMEM) != cudaSuccess)
+        return kErrLaunch;
 
-    CUtensorMap tmA, tmB;
-    if (!encode_bf16_kmajor(&tmA, qB, P.Q, p.d_pad)) return kErrTensorMap;
-    if (!encode_bf16_kmajor(&tmB, R.refB, P.N, p.d_pad)) return kErrTensorMap;
-
-    TcArgs a;
-    a.N = P.N;
-    a.Q = P.Q;
-    a.kb_count = p.kb;
-    a.n_tiles = p.n_tiles;
-    a.n_splits = p.splits;
-    a.rn = R.rn;
-    a.thr = thr;
-    a.p1 = p1;
-    a.cand = cand;
-    a.count = count;
-    a.cmax = p.cmax;
-    a.status = P.status;
-    dim3 grid(p.qtiles, p.splits);
-    cudaError_t e;
-    e = cudaFuncSetAttribute(knn_tc_scan_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TC_SMEM);
-    if (e != cudaSuccess) return kErrLaunch;
-    e = cudaFuncSetAttribute(knn_tc_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TC_SMEM);
-    if (e != cudaSuccess) return kErrLaunch;
-
-    a.tile_stride = p.stride1;
-    knn_tc_scan_kernel<0><<<grid, TC_THREADS, TC_SMEM, st>>>(tmA, tmB, a);
-    if (tm) tm->mark(st, kPhaseTcPass1);
-    tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, p.splits, P.Q, thr, count);
-    if (tm) tm->mark(st, kPhaseTcThreshold);
-    a.tile_stride = 1;
-    knn_tc_scan_kernel<1><<<grid, TC_THREADS, TC_SMEM, st>>>(tmA, tmB, a);
-    if (tm) tm->mark(st, kPhaseTcPass2);
-    if (cudaMemsetAsync(nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
-    int cpow = 1;
-    while (cpow < p.cmax) cpow <<= 1;
-    const size_t rsmem = (((size_t)p.d_pad * 4 + 15) & ~size_t(15)) + (size_t)cpow * 8;
-    e = cudaFuncSetAttribute(tc_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)rsmem);
-    if (e != cudaSuccess) return kErrLaunch;
-    tc_rerank_kernel<<<P.Q, 256, rsmem, st>>>(R.refT, P.d, p.d_pad, P.qry, P.ldq, qn,
-                                              R.rmax_bits, thr, cand, count, p.cmax, P.k,
-                                              P.out_dist, P.out_idx, P.ld_out, fail, nfail);
-    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-    if (tm) tm->mark(st, kPhaseTcRerank);
-
-    // uncertified queries -> exact kernel
+    // pass 1: thresholds from a strided sample of the reference tiles
+    {
+        CUtensorMap tmA, tmB;
+        if (!encode_bf16_kmajor(&tmA, qB, P.Q, p.d_pad)) return kErrTensorMap;
+        if (!encode_bf16_kmajor(&tmB, R.refB, P.N, p.d_pad)) return kErrTensorMap;
+        TcArgs a;
+        a.N = P.N;
+        a.Q = P.Q;
+        a.kb_count = p.kb;
+        a.n_tiles = p.n_tiles;
+        a.n_splits = p.splits;
+        a.tile_stride = p.stride1;
+        a.rn = R.rn;
+        a.thr = thr;
+        a.p1 = p1;
+        a.cand = cand;
+        a.count = count;
+        a.cmax = p.cmax;
+        a.status = P.status;
+        knn_tc_scan_kernel<0><<<dim3(p.qtiles, p.splits), TC_THREADS, TC_SMEM, st>>>(tmA, tmB,
+                                                                                     a);
+        if (tm) tm->mark(st, kPhaseTcPass1);
+        tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, p.splits, P.Q, qn,
+                                                               R.rmax_bits, p.d_pad, thr, count);
+        if (tm) tm->mark(st, kPhaseTcThreshold);
+    }
+    // pass 2 + re-rank of every query
+    int rc = scan_and_rerank(P, R, p, st, qB, P.Q, P.qry, P.ldq, qn, thr, count, cand,
+                             P.out_dist, P.out_idx, P.ld_out, fail, nfail, retry);
+    if (rc != kOk) return rc;
     int nf = 0;
-    if (cudaMemcpyAsync(host_nfail, nfail, sizeof(int), cudaMemcpyDeviceToHost, st) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-        return kErrCuda;
-    nf = *host_nfail;
+    if ((rc = read_count(nfail, host_tmp, st, nf)) != kOk) return rc;
+    host_stats[0] = nf;
     if (nf == 0) return kOk;
-    // as many reference splits as the remaining scratch holds (one split needs none)
-    const long long per_split = (long long)nf * P.k * 8;
-    const int splits = (int)std::max<long long>(
-        1, std::min<long long>(exact_plan_splits(P.N, nf, P.d, P.k, P.num_sms),
-                               (long long)(xcap / per_split)));
+
+    // second chance: the uncertified queries, compacted, scanned again with
+    // thresholds that certify (list overflows excepted)
     gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, fail,
                                                                        nf, qsub, ldf);
-    ExactProblem x;
-    x.ref = P.ref;
-    x.N = P.N;
-    x.ldr = P.ldr;
-    x.qry = qsub;
-    x.Q = nf;
-    x.ldq = ldf;
-    x.d = P.d;
-    x.k = P.k;
-    x.out_dist = sd;
-    x.out_idx = si;
-    x.ld_out = ldf;
-    x.scratch = xs;
-    x.scratch_bytes = xcap;
-    x.status = P.status;
-    x.num_sms = P.num_sms;
-    x.force_splits = splits;
-    x.timer = nullptr;
-    int rc = launch_exact(x, st);
+    tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(qsub, nf, ldf, P.d, qn, nullptr);
+    tc_pack_kernel<<<dim3((nf + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
+        qsub, nf, ldf, P.d, p.d_pad, qB, nullptr);
+    tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(fail, nf, retry, thr, count);
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    rc = scan_and_rerank(P, R, p, st, qB, nf, qsub, ldf, qn, thr, count, cand, sd, si, ldf,
+                         fail2, nfail, retry);
     if (rc != kOk) return rc;
+    int nf2 = 0;
+    if ((rc = read_count(nfail, host_tmp, st, nf2)) != kOk) return rc;
+    host_stats[1] = nf2;
+    if (nf2 > 0) {
+        // still uncertified (list overflow): the exact kernel recomputes the
+        // compacted batch
+        const long long per_split = (long long)nf * P.k * 8;
+        const int splits = (int)std::max<long long>(
+            1, std::min<long long>(exact_plan_splits(P.N, nf, P.d, P.k, P.num_sms),
+                                   (long long)(xcap / per_split)));
+        ExactProblem x;
+        x.ref = P.ref;
+        x.N = P.N;
+        x.ldr = P.ldr;
+        x.qry = qsub;
+        x.Q = nf;
+        x.ldq = ldf;
+        x.d = P.d;
+        x.k = P.k;
+        x.out_dist = sd;
+        x.out_idx = si;
+        x.ld_out = ldf;
+        x.scratch = xs;
+        x.scratch_bytes = xcap;
+        x.status = P.status;
+        x.num_sms = P.num_sms;
+        x.force_splits = splits;
+        x.timer = nullptr;
+        if ((rc = launch_exact(x, st)) != kOk) return rc;
+    }
     scatter_results_kernel<<<dim3((nf + 127) / 128, P.k), 128, 0, st>>>(
         sd, si, ldf, fail, nf, P.out_dist, P.out_idx, P.ld_out);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
