@@ -233,7 +233,7 @@ def time_tier(knncuda, torch, D, stream, step, steps, clocks=None):
     if clocks:
         clocks.start()
     knncuda.set_phase_timing(True)
-    phase_sum, second, exact = {}, 0, 0
+    phase_sum, second, exact, cands = {}, 0, 0, 0
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -242,8 +242,9 @@ def time_tier(knncuda, torch, D, stream, step, steps, clocks=None):
         torch.cuda.synchronize()
         for k, v in knncuda.last_phase_times().items():
             phase_sum[k] = phase_sum.get(k, 0.0) + v
-        a, b = knncuda.last_fallback_counts()
-        second, exact = second + a, exact + b
+        st = knncuda.last_tc_stats()
+        second, exact = second + st["second_scan"], exact + st["exact"]
+        cands += st["candidates"]
     e1.record(stream)
     torch.cuda.synchronize()
     knncuda.set_phase_timing(False)
@@ -253,7 +254,8 @@ def time_tier(knncuda, torch, D, stream, step, steps, clocks=None):
         raise RuntimeError("device status error in timed region")
     ms = D.max(e0.elapsed_time(e1) / steps)
     return (ms, {k: v / steps for k, v in phase_sum.items()},
-            {"second_scan": second / steps, "exact": exact / steps}, clk)
+            {"second_scan": second / steps, "exact": exact / steps,
+             "candidates": cands / steps}, clk)
 
 
 def fp64_recall(torch, ref_d, qry_d, idx, dist, k, sample):

@@ -107,12 +107,13 @@ KNNB200_API const char *knnb200_status_string(int code);
  * the roofline denominator of the FP32 direct-form path. */
 KNNB200_API double knnb200_measure_fp32_peak(int iters, void *stream);
 
-/* For the last knn_cublas-method call on the current device: the number of
- * queries that failed the first tensor-core certification and were scanned a
+/* For the last knn_cublas-method call on the current device: the total
+ * number of candidates the first tensor-core scan emitted (*candidates), the
+ * number of queries that failed the first certification and were scanned a
  * second time (*second_scan), and of those the number recomputed by the
- * exact kernel (*exact).  Both 0 when the call ran the exact kernel only.
- * Either pointer may be NULL. */
-KNNB200_API void knnb200_last_fallback_counts(int *second_scan, int *exact);
+ * exact kernel (*exact).  All 0 when the call ran the exact kernel only.
+ * Any pointer may be NULL. */
+KNNB200_API void knnb200_last_tc_stats(long long *candidates, int *second_scan, int *exact);
 
 /* Per-phase device timing of the calls on the current device (CUDA events on
  * the launching stream between the kernels of a call).  Off by default. */

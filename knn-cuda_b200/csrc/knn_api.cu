@@ -109,7 +109,7 @@ struct Workspace {
         if (!status.ensure(sizeof(int))) return false;
         if (cudaMallocHost(reinterpret_cast<void **>(&status_host), sizeof(int)) != cudaSuccess)
             return false;
-        if (cudaMallocHost(reinterpret_cast<void **>(&tc_stats), 4 * sizeof(int)) != cudaSuccess)
+        if (cudaMallocHost(reinterpret_cast<void **>(&tc_stats), 8 * sizeof(int)) != cudaSuccess)
             return false;
         for (int i = 0; i < PhaseTimer::kMaxMarks; ++i)
             if (cudaEventCreate(&timer.ev[i]) != cudaSuccess) return false;
@@ -140,7 +140,7 @@ size_t scratch_for(int method, int N, int Q, int d, int k, int num_sms) {
 // (it synchronises the stream once, to recompute uncertified queries);
 // everything else runs the fused exact kernel.
 int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st) {
-    ws.tc_stats[0] = ws.tc_stats[1] = 0;
+    for (int i = 0; i < 8; ++i) ws.tc_stats[i] = 0;
     if (!exact_supported_k(p0.k)) return kErrUnsupported;
     ExactProblem p = p0;
     p.timer = &ws.timer;
@@ -477,12 +477,14 @@ int knnb200_last_phase_times(float *ms, int n) {
     return kNumPhases;
 }
 
-void knnb200_last_fallback_counts(int *second_scan, int *exact) {
+void knnb200_last_tc_stats(long long *candidates, int *second_scan, int *exact) {
+    if (candidates) *candidates = 0;
     if (second_scan) *second_scan = 0;
     if (exact) *exact = 0;
     Workspace *ws = nullptr;
     if (current_workspace(ws) != kOk || !ws->init) return;
     std::lock_guard<std::mutex> lock(ws->mu);
+    if (candidates) *candidates = *reinterpret_cast<const long long *>(ws->tc_stats + 4);
     if (second_scan) *second_scan = ws->tc_stats[0];
     if (exact) *exact = ws->tc_stats[1];
 }

@@ -36,14 +36,16 @@ namespace knnb200 {
 constexpr int EX_BR = 256;       // reference points per tile
 constexpr int EX_BD = 16;        // dimensions per pipeline stage
 constexpr int EX_CB = 128;       // candidate slots per query (one half tile)
-constexpr int EX_WARPS = 8;      // consumer warps
+constexpr int EX_WARPS = 16;     // consumer warps
 constexpr int EX_THREADS = (EX_WARPS + 1) * 32;
-constexpr int EX_STAGES = 4;
+constexpr int EX_STAGES = 3;
 
 template <int QPW, int KCAP>
 struct ExCfg {
     static constexpr int BQ = QPW * EX_WARPS;
-    static constexpr int Q_FLOATS = EX_BD * BQ;
+    // query slab of a stage: each query value stored twice, (q, q), so a
+    // 64-bit shared load yields a ready packed operand
+    static constexpr int Q_FLOATS = EX_BD * 2 * BQ;
     static constexpr int R_FLOATS = EX_BD * EX_BR;
     static constexpr int STAGE_FLOATS = Q_FLOATS + R_FLOATS;
     static constexpr int STAGE_BYTES = STAGE_FLOATS * 4;
@@ -203,7 +205,7 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
                 float *rs = qs + C::Q_FLOATS;
                 const int rt = t0 + it / a.n_dchunks, dc = it % a.n_dchunks;
                 mbar_arrive_expect_tx(&full[s], C::STAGE_BYTES);
-                tma_load_2d(qs, &tm_qry, &full[s], qtile * C::BQ, dc * EX_BD);
+                tma_load_2d(qs, &tm_qry, &full[s], qtile * 2 * C::BQ, dc * EX_BD);
                 tma_load_2d(rs, &tm_ref, &full[s], rt * EX_BR, dc * EX_BD);
                 issued = it + 1;
             }
@@ -245,26 +247,19 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
                 alive = false;
                 break;
             }
-            const float *qs = stages + (size_t)s * C::STAGE_FLOATS + warp * QPW;
+            const float *qs = stages + (size_t)s * C::STAGE_FLOATS + warp * 2 * QPW;
             const float *rs = stages + (size_t)s * C::STAGE_FLOATS + C::Q_FLOATS + lane * 4;
-#pragma unroll
+#pragma unroll 4
             for (int dd = 0; dd < EX_BD; ++dd) {
                 const float4 ra = *reinterpret_cast<const float4 *>(rs + dd * EX_BR);
                 const float4 rb = *reinterpret_cast<const float4 *>(rs + dd * EX_BR + 128);
-                float qv[QPW];
-#pragma unroll
-                for (int i = 0; i < QPW; i += 4) {
-                    const float4 q4 = *reinterpret_cast<const float4 *>(qs + dd * C::BQ + i);
-                    qv[i] = q4.x;
-                    qv[i + 1] = q4.y;
-                    qv[i + 2] = q4.z;
-                    qv[i + 3] = q4.w;
-                }
                 const f32x2_t r0 = f2_pack(ra.x, ra.y), r1 = f2_pack(ra.z, ra.w);
                 const f32x2_t r2 = f2_pack(rb.x, rb.y), r3 = f2_pack(rb.z, rb.w);
+                const f32x2_t *qp =
+                    reinterpret_cast<const f32x2_t *>(qs + dd * 2 * C::BQ);
 #pragma unroll
                 for (int i = 0; i < QPW; ++i) {
-                    const f32x2_t qq = f2_pack(qv[i], qv[i]);
+                    const f32x2_t qq = qp[i];   // (q_i, q_i)
                     f32x2_t t;
                     t = f2_sub(r0, qq); acc[i][0] = f2_fma(t, t, acc[i][0]);
                     t = f2_sub(r1, qq); acc[i][1] = f2_fma(t, t, acc[i][1]);
@@ -314,6 +309,18 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
             unsigned long long *dst = a.part + ((size_t)split * a.Q + q) * a.k;
             for (int j = lane; j < a.k; j += 32) dst[j] = wl[i * C::REGION + j];
         }
+    }
+}
+
+// Duplicate every query value into a (q, q) pair: dst[d][2i] = dst[d][2i+1]
+// = src[d][i].
+__global__ void dup_queries_kernel(const float *__restrict__ src, int Q, long long lds, int d,
+                                   float2 *__restrict__ dst, long long ldd2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int dd = blockIdx.y;
+    if (i < Q) {
+        const float v = src[(size_t)dd * lds + i];
+        dst[(size_t)dd * ldd2 + i] = make_float2(v, v);
     }
 }
 
@@ -377,10 +384,10 @@ void shape_of(ExactShape &s) {
 }
 
 bool choose_shape(int N, int Q, int d, int k, int num_sms, ExactShape &s) {
-    if (k <= 32) shape_of<8, 32>(s);
-    else if (k <= 64) shape_of<8, 64>(s);
-    else if (k <= 128) shape_of<8, 128>(s);
-    else if (k <= 256) shape_of<4, 256>(s);
+    if (k <= 32) shape_of<4, 32>(s);
+    else if (k <= 64) shape_of<4, 64>(s);
+    else if (k <= 128) shape_of<4, 128>(s);
+    else if (k <= 256) shape_of<2, 256>(s);
     else return false;
     s.n_rtiles = (N + EX_BR - 1) / EX_BR;
     s.n_dchunks = (d + EX_BD - 1) / EX_BD;
@@ -425,10 +432,15 @@ cudaError_t launch_t(const CUtensorMap &mr, const CUtensorMap &mq, const ExactAr
 
 }  // namespace
 
+// Row pitch (in float2) of the duplicated query copy.
+static long long qdup_pitch2(int Q) { return ((long long)Q + 31) / 32 * 32; }
+
 size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     ExactShape s;
     if (!choose_shape(N, Q, d, k, num_sms, s)) return 0;
-    return s.splits > 1 ? (size_t)s.splits * Q * k * sizeof(unsigned long long) : 0;
+    const size_t dup = (size_t)d * qdup_pitch2(Q) * sizeof(float2);
+    const size_t part = s.splits > 1 ? (size_t)s.splits * Q * k * sizeof(unsigned long long) : 0;
+    return dup + 256 + part;
 }
 
 bool exact_supported_k(int k) { return k >= 1 && k <= 256; }
@@ -436,14 +448,23 @@ bool exact_supported_k(int k) { return k >= 1 && k <= 256; }
 int launch_exact(const ExactProblem &p, cudaStream_t st) {
     ExactShape s;
     if (!choose_shape(p.N, p.Q, p.d, p.k, p.num_sms, s)) return kErrUnsupported;
-    if (p.force_splits > 0) s.splits = std::min(p.force_splits, std::min(s.n_rtiles, 64));
-    const size_t need = s.splits > 1 ? (size_t)s.splits * p.Q * p.k * 8 : 0;
+    if (p.force_splits > 0) s.splits = std::min(p.force_splits, std::min(s.n_rtiles, 256));
+    const long long ld2 = qdup_pitch2(p.Q);
+    const size_t dup = (size_t)p.d * ld2 * sizeof(float2);
+    const size_t need = dup + 256 + (s.splits > 1 ? (size_t)s.splits * p.Q * p.k * 8 : 0);
     if (need > p.scratch_bytes) return kErrScratch;
+    float2 *qdup = static_cast<float2 *>(p.scratch);
+    unsigned long long *part = reinterpret_cast<unsigned long long *>(
+        static_cast<unsigned char *>(p.scratch) + ((dup + 255) & ~size_t(255)));
+    dup_queries_kernel<<<dim3((p.Q + 255) / 256, p.d), 256, 0, st>>>(p.qry, p.Q, p.ldq, p.d, qdup,
+                                                                   ld2);
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
 
     CUtensorMap mr, mq;
     if (!encode_f32_2d(&mr, p.ref, (uint64_t)p.N, (uint64_t)p.d, (uint64_t)p.ldr, EX_BR, EX_BD))
         return kErrTensorMap;
-    if (!encode_f32_2d(&mq, p.qry, (uint64_t)p.Q, (uint64_t)p.d, (uint64_t)p.ldq, s.bq, EX_BD))
+    if (!encode_f32_2d(&mq, qdup, (uint64_t)(2 * p.Q), (uint64_t)p.d, (uint64_t)(2 * ld2),
+                       2 * s.bq, EX_BD))
         return kErrTensorMap;
 
     ExactArgs a;
@@ -457,16 +478,16 @@ int launch_exact(const ExactProblem &p, cudaStream_t st) {
     a.out_dist = p.out_dist;
     a.out_idx = p.out_idx;
     a.ld_out = p.ld_out;
-    a.part = static_cast<unsigned long long *>(p.scratch);
+    a.part = part;
     a.status = p.status;
     const int qtiles = (p.Q + s.bq - 1) / s.bq;
 
     cudaError_t e;
     switch (s.kcap) {
-        case 32: e = launch_t<8, 32>(mr, mq, a, qtiles, st); break;
-        case 64: e = launch_t<8, 64>(mr, mq, a, qtiles, st); break;
-        case 128: e = launch_t<8, 128>(mr, mq, a, qtiles, st); break;
-        default: e = launch_t<4, 256>(mr, mq, a, qtiles, st); break;
+        case 32: e = launch_t<4, 32>(mr, mq, a, qtiles, st); break;
+        case 64: e = launch_t<4, 64>(mr, mq, a, qtiles, st); break;
+        case 128: e = launch_t<4, 128>(mr, mq, a, qtiles, st); break;
+        default: e = launch_t<2, 256>(mr, mq, a, qtiles, st); break;
     }
     if (e != cudaSuccess) return kErrLaunch;
     if (p.timer) p.timer->mark(st, kPhaseExactMain);

@@ -139,8 +139,9 @@ int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, i
 // Queues the tensor-core k-NN.  Synchronises once to learn how many queries
 // failed certification; those get a second scan with thresholds that
 // certify, and queries whose candidate list overflowed are recomputed by the
-// exact kernel.  host_stats (pinned, 3 ints): [0] queries given the second
-// scan, [1] queries recomputed by the exact kernel, [2] scratch.
+// exact kernel.  host_stats (pinned, 8 ints, 8-byte aligned): [0] queries
+// given the second scan, [1] queries recomputed by the exact kernel, [2]
+// scratch, [4..5] total first-scan candidates (64-bit).
 int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_stats);
 
 }  // namespace knnb200

@@ -152,6 +152,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 mbar_arrive_expect_tx(&b_full[s], TC_TILE_BYTES);
                 tma_load_2d(sB + (size_t)s * TC_TILE_BYTES, &tmB, &b_full[s], kb * TC_BK,
                             (first + j * G) * TC_BN);
+                // pull the block two tiles ahead into L2 so the ring's loads
+                // see L2 rather than DRAM latency
+                if (j + 2 < n_my)
+                    tma_prefetch_l2_2d(&tmB, kb * TC_BK, (first + (j + 2) * G) * TC_BN);
                 issued = it + 1;
             }
             for (int it = max(0, issued - TC_STAGES); it < issued; ++it)
@@ -426,7 +430,7 @@ __global__ void __launch_bounds__(256)
                      const int *__restrict__ cand, const int *__restrict__ count, int cmax,
                      int k, float *__restrict__ out_dist, int *__restrict__ out_idx,
                      long long ld_out, int *__restrict__ fail_list, int *__restrict__ n_fail,
-                     float *__restrict__ retry) {
+                     float *__restrict__ retry, unsigned long long *__restrict__ cand_total) {
     extern __shared__ unsigned char rsm[];
     float *qv = reinterpret_cast<float *>(rsm);
     unsigned long long *keys =
@@ -434,6 +438,7 @@ __global__ void __launch_bounds__(256)
     __shared__ int failed;
     const int q = blockIdx.x, tid = threadIdx.x;
     const int c = count[q];
+    if (tid == 0) atomicAdd(cand_total, (unsigned long long)c);
     if (c > cmax || c < k) {
         if (tid == 0) {
             fail_list[atomicAdd(n_fail, 1)] = q;
@@ -457,16 +462,24 @@ __global__ void __launch_bounds__(256)
             const int r = cand[(size_t)q * cmax + t];
             const float4 *row = reinterpret_cast<const float4 *>(refT + (size_t)r * d_pad);
             float acc = 0.f;
-            for (int dd4 = 0; dd4 < d_pad / 4; ++dd4) {
-                const float4 v = __ldg(row + dd4);
-                float t0 = __fsub_rn(v.x, qv[4 * dd4 + 0]);
-                acc = __fmaf_rn(t0, t0, acc);
-                t0 = __fsub_rn(v.y, qv[4 * dd4 + 1]);
-                acc = __fmaf_rn(t0, t0, acc);
-                t0 = __fsub_rn(v.z, qv[4 * dd4 + 2]);
-                acc = __fmaf_rn(t0, t0, acc);
-                t0 = __fsub_rn(v.w, qv[4 * dd4 + 3]);
-                acc = __fmaf_rn(t0, t0, acc);
+            // 16 row segments in flight per thread, then the FMA chain in
+            // increasing d (the exact kernel's order)
+            for (int c0 = 0; c0 < d_pad / 4; c0 += 16) {
+                float4 buf[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) buf[i] = __ldg(row + c0 + i);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const float *qq4 = qv + 4 * (c0 + i);
+                    float t0 = __fsub_rn(buf[i].x, qq4[0]);
+                    acc = __fmaf_rn(t0, t0, acc);
+                    t0 = __fsub_rn(buf[i].y, qq4[1]);
+                    acc = __fmaf_rn(t0, t0, acc);
+                    t0 = __fsub_rn(buf[i].z, qq4[2]);
+                    acc = __fmaf_rn(t0, t0, acc);
+                    t0 = __fsub_rn(buf[i].w, qq4[3]);
+                    acc = __fmaf_rn(t0, t0, acc);
+                }
             }
             key = make_key(acc, (uint32_t)r);
         }
@@ -650,7 +663,8 @@ namespace {
 int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cudaStream_t st,
                     const __nv_bfloat16 *qB, int Q, const float *qry, long long ldq,
                     const float *qn, const float *thr, int *count, int *cand, float *out_dist,
-                    int *out_idx, long long ld_out, int *fail, int *nfail, float *retry) {
+                    int *out_idx, long long ld_out, int *fail, int *nfail, float *retry,
+                    unsigned long long *cand_total) {
     const TcPlan pb = plan_tc(P.N, Q, P.d, P.k, P.num_sms);
     CUtensorMap tmA, tmB;
     if (!encode_bf16_kmajor(&tmA, qB, Q, p.d_pad)) return kErrTensorMap;
@@ -680,7 +694,7 @@ int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cud
         return kErrLaunch;
     tc_rerank_kernel<<<Q, 256, rsmem, st>>>(R.refT, P.d, p.d_pad, qry, ldq, qn, R.rmax_bits,
                                             thr, cand, count, p.cmax, P.k, out_dist, out_idx,
-                                            ld_out, fail, nfail, retry);
+                                            ld_out, fail, nfail, retry, cand_total);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (P.timer) P.timer->mark(st, kPhaseTcRerank);
     return kOk;
@@ -700,6 +714,7 @@ int read_count(const int *dev, int *host_pinned, cudaStream_t st, int &out) {
 int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_stats) {
     int *host_tmp = host_stats + 2;
     host_stats[0] = host_stats[1] = 0;
+    host_stats[4] = host_stats[5] = 0;
     const TcPlan p = plan_tc(P.N, P.Q, P.d, P.k, P.num_sms);
     if (!tc_supported(P.N, P.Q, P.d, P.k)) return kErrUnsupported;
     Carve cv{static_cast<unsigned char *>(P.scratch), 0, P.scratch_bytes};
@@ -711,6 +726,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     int *fail = cv.take<int>(P.Q);
     int *fail2 = cv.take<int>(P.Q);
     int *nfail = cv.take<int>(4);
+    unsigned long long *cand_total = cv.take<unsigned long long>(1);
     float *p1 = cv.take<float>((size_t)p.splits * P.Q * TC_KS);
     int *cand = cv.take<int>((size_t)P.Q * p.cmax);
     const long long ldf = (P.Q + 3) / 4 * 4;       // second-chance buffers, sized for all queries
@@ -761,10 +777,15 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
         if (tm) tm->mark(st, kPhaseTcThreshold);
     }
     // pass 2 + re-rank of every query
+    if (cudaMemsetAsync(cand_total, 0, sizeof(unsigned long long), st) != cudaSuccess)
+        return kErrCuda;
     int rc = scan_and_rerank(P, R, p, st, qB, P.Q, P.qry, P.ldq, qn, thr, count, cand,
-                             P.out_dist, P.out_idx, P.ld_out, fail, nfail, retry);
+                             P.out_dist, P.out_idx, P.ld_out, fail, nfail, retry, cand_total);
     if (rc != kOk) return rc;
     int nf = 0;
+    if (cudaMemcpyAsync(host_stats + 4, cand_total, sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return kErrCuda;
     if ((rc = read_count(nfail, host_tmp, st, nf)) != kOk) return rc;
     host_stats[0] = nf;
     if (nf == 0) return kOk;
@@ -779,7 +800,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(fail, nf, retry, thr, count);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     rc = scan_and_rerank(P, R, p, st, qB, nf, qsub, ldf, qn, thr, count, cand, sd, si, ldf,
-                         fail2, nfail, retry);
+                         fail2, nfail, retry, cand_total);
     if (rc != kOk) return rc;
     int nf2 = 0;
     if ((rc = read_count(nfail, host_tmp, st, nf2)) != kOk) return rc;

@@ -43,7 +43,7 @@ C_SYMBOLS = (
     "knnb200_cuda_global", "knnb200_cuda_texture", "knnb200_cublas", "knnb200_knn_device",
     "knnb200_sync_status", "knnb200_scratch_bytes", "knnb200_plan_splits",
     "knnb200_release_workspace", "knnb200_status_string", "knnb200_version",
-    "knnb200_measure_fp32_peak", "knnb200_last_fallback_counts",
+    "knnb200_measure_fp32_peak", "knnb200_last_tc_stats",
     "knnb200_knn_device_noalloc", "knnb200_set_phase_timing", "knnb200_last_phase_times",
 )
 PHASES = ("tc_prep_ref", "tc_prep_query", "tc_pass1", "tc_threshold", "tc_pass2", "tc_rerank",
@@ -93,8 +93,8 @@ def lib():
         L.knnb200_set_phase_timing.argtypes = [ctypes.c_int]
         L.knnb200_last_phase_times.restype = ctypes.c_int
         L.knnb200_last_phase_times.argtypes = [_FP, ctypes.c_int]
-        L.knnb200_last_fallback_counts.restype = None
-        L.knnb200_last_fallback_counts.argtypes = [_IP, _IP]
+        L.knnb200_last_tc_stats.restype = None
+        L.knnb200_last_tc_stats.argtypes = [ctypes.POINTER(ctypes.c_longlong), _IP, _IP]
         L.knnb200_version.restype = ctypes.c_char_p
         L.knnb200_version.argtypes = []
         _lib = L
@@ -228,12 +228,18 @@ def last_phase_times() -> dict:
     return {name: float(v) for name, v in zip(PHASES, buf) if v >= 0}
 
 
+def last_tc_stats() -> dict:
+    """Statistics of the last knn_cublas-method call: first-scan candidates,
+    queries given a second tensor scan, queries recomputed by the exact kernel."""
+    c, a, b = ctypes.c_longlong(0), ctypes.c_int(0), ctypes.c_int(0)
+    lib().knnb200_last_tc_stats(ctypes.byref(c), ctypes.byref(a), ctypes.byref(b))
+    return {"candidates": c.value, "second_scan": a.value, "exact": b.value}
+
+
 def last_fallback_counts() -> tuple:
-    """(second_scan, exact): queries of the last knn_cublas-method call that
-    needed a second tensor scan, and those recomputed by the exact kernel."""
-    a, b = ctypes.c_int(0), ctypes.c_int(0)
-    lib().knnb200_last_fallback_counts(ctypes.byref(a), ctypes.byref(b))
-    return a.value, b.value
+    """(second_scan, exact) of the last knn_cublas-method call."""
+    s = last_tc_stats()
+    return s["second_scan"], s["exact"]
 
 
 def version() -> str:
