@@ -49,14 +49,15 @@ constexpr int TC_KBMAX = 4;           // d_pad <= 256
 constexpr int TC_STAGES = 5;
 constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;   // 16 KB (A or B K-block tile)
 constexpr int TC_KS = 16;             // pass-1 per-row list length
-constexpr int TC_THREADS = 192;       // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
+constexpr int TC_EPI_WARPS = 8;       // two per TMEM lane quadrant (one per query tile)
+constexpr int TC_THREADS = 32 * (2 + TC_EPI_WARPS);   // warp 0 TMA, warp 1 MMA, 2..9 epilogue
 constexpr uint32_t TC_TMEM_COLS = 512;   // 2 accumulator buffers x 2 A tiles x 128
 constexpr uint32_t TC_IDESC = umma_idesc_bf16(TC_BM, TC_BN);
 
 constexpr size_t TC_OFF_A = 0;
 constexpr size_t TC_OFF_B = (size_t)2 * TC_KBMAX * TC_TILE_BYTES;             // 128 KB
 constexpr size_t TC_OFF_RN = TC_OFF_B + (size_t)TC_STAGES * TC_TILE_BYTES;    // +64 KB
-constexpr size_t TC_OFF_BAR = TC_OFF_RN + 4 * TC_BN * sizeof(float);   // one rn slab per epilogue warp
+constexpr size_t TC_OFF_BAR = TC_OFF_RN + TC_EPI_WARPS * TC_BN * sizeof(float);   // rn slab per epilogue warp
 constexpr int TC_NBARS = 1 + 2 * TC_STAGES + 2 + 2 + 1;
 constexpr size_t TC_SMEM = 1024 + TC_OFF_BAR + TC_NBARS * 8 + 16;
 
@@ -109,7 +110,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], 4);
+            mbar_init(&acc_empty[b], TC_EPI_WARPS);
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -214,19 +215,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         __syncwarp();
     } else {
-        // ------------------------- epilogue (4 warps) --------------------
-        const int qd = warp & 3;                  // TMEM lane quadrant of this warp
-        int qrow[2];
-        float thr[2];
-        float L[2][TC_KS];
+        // ------------------------- epilogue (8 warps) --------------------
+        // Warp w reads TMEM lane quadrant w % 4 of query tile h = (w - 2) / 4:
+        // one query row per thread, 128 reference columns per tile.
+        const int qd = warp & 3;
+        const int h = (warp - 2) >> 2;
+        const int qrow = qtile * TC_QT + h * TC_BM + qd * 32 + lane;
+        float thr = -INFINITY;
+        if (MODE == 1 && qrow < a.Q) thr = a.thr[qrow];
+        float L[TC_KS];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            qrow[h] = qtile * TC_QT + h * TC_BM + qd * 32 + lane;
-            thr[h] = -INFINITY;
-            if (MODE == 1 && qrow[h] < a.Q) thr[h] = a.thr[qrow[h]];
-#pragma unroll
-            for (int i = 0; i < TC_KS; ++i) L[h][i] = INFINITY;
-        }
+        for (int i = 0; i < TC_KS; ++i) L[i] = INFINITY;
         // Norms of the next tile are fetched into registers before waiting on
         // its accumulator, so the global-load latency overlaps the wait.
         float rn_next[TC_BN / 32];
@@ -256,55 +255,56 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             for (int i = 0; i < TC_BN / 32; ++i) rnb[i * 32 + lane] = rn_next[i];
             __syncwarp();
             fetch_rn(j + 1);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
 #pragma unroll 1
-                for (int c = 0; c < TC_BN / 32; c += 2) {
-                    // two TMEM loads in flight per wait
-                    uint32_t v0[32], v1[32];
-                    const uint32_t tbase = tmem + ((uint32_t)(qd * 32) << 16) +
-                                           (uint32_t)((b * 2 + h) * TC_BM + c * 32);
-                    tmem_ld32(tbase, v0);
-                    tmem_ld32(tbase + 32, v1);
-                    tmem_ld_wait(v0);
-                    tmem_ld_wait(v1);
+            for (int c = 0; c < TC_BN / 32; c += 2) {
+                // two TMEM loads in flight per wait
+                uint32_t v0[32], v1[32];
+                const uint32_t tbase = tmem + ((uint32_t)(qd * 32) << 16) +
+                                       (uint32_t)((b * 2 + h) * TC_BM + c * 32);
+                tmem_ld32(tbase, v0);
+                tmem_ld32(tbase + 32, v1);
+                tmem_ld_wait(v0);
+                tmem_ld_wait(v1);
 #pragma unroll
-                    for (int half = 0; half < 2; ++half) {
-                        const uint32_t *v = half ? v1 : v0;
-                        const float *rc = rnb + (c + half) * 32;
-                        float av[32];
+                for (int half = 0; half < 2; ++half) {
+                    const uint32_t *v = half ? v1 : v0;
+                    const float *rc = rnb + (c + half) * 32;
+                    // a = ||r||^2 - 2 r.q for the chunk's 32 columns
+                    float av[32];
 #pragma unroll
-                        for (int e = 0; e < 32; e += 2) {
-                            const float2 r2 = *reinterpret_cast<const float2 *>(rc + e);
-                            const f32x2_t t = f2_fma(f2_pack(-2.0f, -2.0f),
-                                                     f2_pack(__uint_as_float(v[e]),
-                                                             __uint_as_float(v[e + 1])),
-                                                     f2_pack(r2.x, r2.y));
-                            av[e] = f2_lo(t);
-                            av[e + 1] = f2_hi(t);
-                        }
-                        const float lim = MODE == 1 ? thr[h] : L[h][TC_KS - 1];
-                        uint32_t m = 0;
+                    for (int e = 0; e < 32; e += 2) {
+                        const float2 r2 = *reinterpret_cast<const float2 *>(rc + e);
+                        const f32x2_t t = f2_fma(f2_pack(-2.0f, -2.0f),
+                                                 f2_pack(__uint_as_float(v[e]),
+                                                         __uint_as_float(v[e + 1])),
+                                                 f2_pack(r2.x, r2.y));
+                        av[e] = f2_lo(t);
+                        av[e + 1] = f2_hi(t);
+                    }
+                    // one comparison per chunk in the common case
+                    float mn = av[0];
 #pragma unroll
-                        for (int e = 0; e < 32; ++e) m |= (av[e] < lim ? 1u : 0u) << e;
-                        const int cbase = tile * TC_BN + (c + half) * 32;
-                        while (m) {   // rare after the first tiles
-                            const int e = __ffs(m) - 1;
-                            m &= m - 1;
-                            float x = av[0];
+                    for (int e = 1; e < 32; ++e) mn = fminf(mn, av[e]);
+                    const float lim = MODE == 1 ? thr : L[TC_KS - 1];
+                    if (!(mn < lim)) continue;
+                    uint32_t m = 0;
 #pragma unroll
-                            for (int t = 1; t < 32; ++t) x = (t == e) ? av[t] : x;
-                            if (MODE == 1) {
-                                const int pos = atomicAdd(&a.count[qrow[h]], 1);
-                                if (pos < a.cmax)
-                                    a.cand[(size_t)qrow[h] * a.cmax + pos] = cbase + e;
-                            } else if (x < L[h][TC_KS - 1]) {
+                    for (int e = 0; e < 32; ++e) m |= (av[e] < lim ? 1u : 0u) << e;
+                    const int cbase = tile * TC_BN + (c + half) * 32;
+                    while (m) {
+                        const int e = __ffs(m) - 1;
+                        m &= m - 1;
+                        float x = av[0];
 #pragma unroll
-                                for (int i = TC_KS - 1; i > 0; --i)
-                                    L[h][i] = x < L[h][i - 1] ? L[h][i - 1]
-                                                              : (x < L[h][i] ? x : L[h][i]);
-                                L[h][0] = fminf(L[h][0], x);
-                            }
+                        for (int t = 1; t < 32; ++t) x = (t == e) ? av[t] : x;
+                        if (MODE == 1) {
+                            const int pos = atomicAdd(&a.count[qrow], 1);
+                            if (pos < a.cmax) a.cand[(size_t)qrow * a.cmax + pos] = cbase + e;
+                        } else if (x < L[TC_KS - 1]) {
+#pragma unroll
+                            for (int i = TC_KS - 1; i > 0; --i)
+                                L[i] = x < L[i - 1] ? L[i - 1] : (x < L[i] ? x : L[i]);
+                            L[0] = fminf(L[0], x);
                         }
                     }
                 }
@@ -313,14 +313,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[b]);
         }
-        if (MODE == 0 && !*abort_flag) {
+        if (MODE == 0 && !*abort_flag && qrow < a.Q) {
+            float *dst = a.p1 + ((size_t)split * a.Q + qrow) * TC_KS;
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
-                if (qrow[h] < a.Q) {
-                    float *dst = a.p1 + ((size_t)split * a.Q + qrow[h]) * TC_KS;
-#pragma unroll
-                    for (int i = 0; i < TC_KS; ++i) dst[i] = L[h][i];
-                }
+            for (int i = 0; i < TC_KS; ++i) dst[i] = L[i];
         }
     }
 
@@ -569,8 +565,26 @@ bool encode_bf16_kmajor(CUtensorMap *m, const void *base, int rows, int d_pad) {
 }
 
 struct TcPlan {
-    int d_pad, kb, qtiles, n_tiles, splits, stride1, cmax;
+    int d_pad, kb, qtiles, n_tiles, splits, splits1, stride1, cmax;
 };
+
+// Splits that fill whole waves of one CTA per SM for `tiles` tiles per
+// query tile, with at least min_tiles per CTA; modelled per-CTA cost =
+// tiles per split + a fixed set-up cost of `fixed` tiles.
+static int choose_splits(int qtiles, int tiles, int min_tiles, double fixed, int num_sms) {
+    int best = 1;
+    double best_t = 1e300;
+    const int max_s = std::max(1, std::min(256, tiles / std::max(1, min_tiles)));
+    for (int S = 1; S <= max_s; ++S) {
+        const long long ctas = (long long)qtiles * S;
+        const double t = (double)((ctas + num_sms - 1) / num_sms) * ((double)tiles / S + fixed);
+        if (t < best_t * 0.999) {
+            best_t = t;
+            best = S;
+        }
+    }
+    return best;
+}
 
 TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
     TcPlan p;
@@ -578,21 +592,13 @@ TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
     p.kb = p.d_pad / 64;
     p.qtiles = (Q + TC_QT - 1) / TC_QT;
     p.n_tiles = (N + TC_BN - 1) / TC_BN;
-    // splits: fill whole waves of one CTA per SM, at least 16 tiles per CTA
-    int best = 1;
-    double best_t = 1e300;
-    const int max_s = std::max(1, std::min(256, p.n_tiles / 16));
-    for (int S = 1; S <= max_s; ++S) {
-        const long long ctas = (long long)p.qtiles * S;
-        const double t = (double)((ctas + num_sms - 1) / num_sms) * ((double)p.n_tiles / S + 2.0);
-        if (t < best_t * 0.999) {
-            best_t = t;
-            best = S;
-        }
-    }
-    p.splits = best;
+    p.splits = choose_splits(p.qtiles, p.n_tiles, 16, 2.0, num_sms);
     // the sample must hold about 2.5k points below T_q: KS * stride >= 2.5k
     p.stride1 = std::max(16, (5 * k + 2 * TC_KS - 1) / (2 * TC_KS));
+    // pass 1 scans 1/stride1 of the tiles: coarser splits amortise each
+    // CTA's set-up (query tile load, TMEM allocation, pipeline fill)
+    p.splits1 = choose_splits(p.qtiles, (p.n_tiles + p.stride1 - 1) / p.stride1, 32, 8.0,
+                              num_sms);
     p.cmax = 4 * TC_KS * p.stride1;
     return p;
 }
@@ -629,7 +635,7 @@ static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
 size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     const TcPlan p = plan_tc(N, Q, d, k, num_sms);
     size_t b = (size_t)p.qtiles * TC_QT * p.d_pad * 2 + (size_t)Q * 4 * 6 + 16;
-    b += (size_t)p.splits * Q * TC_KS * 4;
+    b += (size_t)std::max(p.splits, p.splits1) * Q * TC_KS * 4;
     b += (size_t)Q * p.cmax * 4;
     b += fallback_bytes(N, Q, d, k, num_sms);   // worst case: every query uncertified
     return b + 16 * 256;
@@ -727,7 +733,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     int *fail2 = cv.take<int>(P.Q);
     int *nfail = cv.take<int>(4);
     unsigned long long *cand_total = cv.take<unsigned long long>(1);
-    float *p1 = cv.take<float>((size_t)p.splits * P.Q * TC_KS);
+    float *p1 = cv.take<float>((size_t)p.splits1 * P.Q * TC_KS);
     int *cand = cv.take<int>((size_t)P.Q * p.cmax);
     const long long ldf = (P.Q + 3) / 4 * 4;       // second-chance buffers, sized for all queries
     float *qsub = cv.take<float>((size_t)P.d * ldf);
@@ -760,7 +766,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
         a.Q = P.Q;
         a.kb_count = p.kb;
         a.n_tiles = p.n_tiles;
-        a.n_splits = p.splits;
+        a.n_splits = p.splits1;
         a.tile_stride = p.stride1;
         a.rn = R.rn;
         a.thr = thr;
@@ -769,10 +775,10 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
         a.count = count;
         a.cmax = p.cmax;
         a.status = P.status;
-        knn_tc_scan_kernel<0><<<dim3(p.qtiles, p.splits), TC_THREADS, TC_SMEM, st>>>(tmA, tmB,
-                                                                                     a);
+        knn_tc_scan_kernel<0><<<dim3(p.qtiles, p.splits1), TC_THREADS, TC_SMEM, st>>>(tmA, tmB,
+                                                                                      a);
         if (tm) tm->mark(st, kPhaseTcPass1);
-        tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, p.splits, P.Q, qn,
+        tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, p.splits1, P.Q, qn,
                                                                R.rmax_bits, p.d_pad, thr, count);
         if (tm) tm->mark(st, kPhaseTcThreshold);
     }
