@@ -412,31 +412,52 @@ __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
 }
 
 // Exact FP32 re-rank of each query's candidates + certification.
-// One block (256 threads) per query.  An uncertified query is appended to
-// fail_list and retry[q] receives a threshold for a second scan: when it had
-// at least k candidates, their k-th exact distance D_k bounds the true k-th
-// from above, so every point of the true top-k has a < D_k (1+g) + E -
-// ||q||^2 and a second scan emitting below D_k (1+g) + 2.5 E - ||q||^2 passes
-// the check; with fewer than k candidates the threshold is widened by 8 E;
-// an overflowing list gets NaN (no second scan: exact kernel).
-__global__ void __launch_bounds__(256)
+// One warp per query (TC_RR_WARPS queries per block, no block-wide syncs).
+// Candidates are handled 32 at a time, one per lane: the warp loads the 32
+// candidate rows of the FP32 point-major copy with coalesced 16-byte loads
+// (two rows per instruction) into a padded shared tile, 64 dimensions at a
+// time, and each lane then runs its candidate's FMA chain in increasing d --
+// the fused exact kernel's arithmetic and order, so distances are identical.
+// The keys are bitonic-sorted by the warp.
+//
+// An uncertified query is appended to fail_list and retry[q] receives a
+// threshold for a second scan: when it had at least k candidates, their k-th
+// exact distance D_k bounds the true k-th from above, so every point of the
+// true top-k has a < D_k (1+g) + E - ||q||^2 and a second scan emitting below
+// D_k (1+g) + 2.5 E - ||q||^2 passes the check; with fewer than k candidates
+// the threshold is widened by 8 E; an overflowing list gets NaN (no second
+// scan: exact kernel).
+constexpr int TC_RR_WARPS = 4;
+constexpr int TC_RR_DCH = 64;                 // dimensions per staged chunk
+constexpr int TC_RR_STRIDE = TC_RR_DCH + 1;   // padded row: conflict-free column reads
+
+__host__ __device__ inline size_t tc_rr_warp_bytes(int d_pad, int cpow) {
+    return (((size_t)d_pad * 4 + 32 * TC_RR_STRIDE * 4 + 15) & ~size_t(15)) + (size_t)cpow * 8;
+}
+
+__global__ void __launch_bounds__(TC_RR_WARPS * 32)
     tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
                      const float *__restrict__ qry, long long ldq, const float *__restrict__ qn,
                      const unsigned *__restrict__ rmax_bits, const float *__restrict__ thr,
                      const int *__restrict__ cand, const int *__restrict__ count, int cmax,
-                     int k, float *__restrict__ out_dist, int *__restrict__ out_idx,
-                     long long ld_out, int *__restrict__ fail_list, int *__restrict__ n_fail,
-                     float *__restrict__ retry, unsigned long long *__restrict__ cand_total) {
+                     int cpow, int Q, int k, float *__restrict__ out_dist,
+                     int *__restrict__ out_idx, long long ld_out, int *__restrict__ fail_list,
+                     int *__restrict__ n_fail, float *__restrict__ retry,
+                     unsigned long long *__restrict__ cand_total) {
     extern __shared__ unsigned char rsm[];
-    float *qv = reinterpret_cast<float *>(rsm);
-    unsigned long long *keys =
-        reinterpret_cast<unsigned long long *>(rsm + (((size_t)d_pad * 4 + 15) & ~size_t(15)));
-    __shared__ int failed;
-    const int q = blockIdx.x, tid = threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * TC_RR_WARPS + warp;
+    if (q >= Q) return;
+    unsigned char *mine = rsm + (size_t)warp * tc_rr_warp_bytes(d_pad, cpow);
+    float *qv = reinterpret_cast<float *>(mine);
+    float *rows = qv + d_pad;
+    unsigned long long *keys = reinterpret_cast<unsigned long long *>(
+        mine + (((size_t)d_pad * 4 + 32 * TC_RR_STRIDE * 4 + 15) & ~size_t(15)));
+
     const int c = count[q];
-    if (tid == 0) atomicAdd(cand_total, (unsigned long long)c);
+    if (lane == 0) atomicAdd(cand_total, (unsigned long long)c);
     if (c > cmax || c < k) {
-        if (tid == 0) {
+        if (lane == 0) {
             fail_list[atomicAdd(n_fail, 1)] = q;
             // too few candidates: the threshold was low; widen it by 8 E.
             // An overflowing list goes to the exact kernel (NaN).
@@ -447,45 +468,50 @@ __global__ void __launch_bounds__(256)
         }
         return;
     }
-    for (int dd = tid; dd < d_pad; dd += blockDim.x)
-        qv[dd] = dd < d ? qry[(size_t)dd * ldq + q] : 0.f;
+    for (int dd = lane; dd < d_pad; dd += 32) qv[dd] = dd < d ? qry[(size_t)dd * ldq + q] : 0.f;
+    __syncwarp();
+    const int *cq = cand + (size_t)q * cmax;
+    for (int g = 0; g * 32 < c; ++g) {
+        const int t = g * 32 + lane;
+        const int my_r = t < c ? cq[t] : -1;
+        float acc = 0.f;
+        for (int ch = 0; ch < d_pad; ch += TC_RR_DCH) {
+            float4 v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int r = __shfl_sync(0xffffffffu, my_r, 2 * i + (lane >> 4));
+                v[i] = r >= 0 ? __ldg(reinterpret_cast<const float4 *>(
+                                          refT + (size_t)r * d_pad + ch) +
+                                      (lane & 15))
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                float *dst = rows + (2 * i + (lane >> 4)) * TC_RR_STRIDE + (lane & 15) * 4;
+                dst[0] = v[i].x;
+                dst[1] = v[i].y;
+                dst[2] = v[i].z;
+                dst[3] = v[i].w;
+            }
+            __syncwarp();
+            const float *myrow = rows + lane * TC_RR_STRIDE;
+#pragma unroll 16
+            for (int dd = 0; dd < TC_RR_DCH; ++dd) {
+                const float t0 = __fsub_rn(myrow[dd], qv[ch + dd]);
+                acc = __fmaf_rn(t0, t0, acc);
+            }
+            __syncwarp();
+        }
+        if (t < c) keys[t] = make_key(acc, (uint32_t)my_r);
+    }
     int P = 1;
     while (P < c) P <<= 1;
-    __syncthreads();
-    for (int t = tid; t < P; t += blockDim.x) {
-        unsigned long long key = kKeyInf;
-        if (t < c) {
-            const int r = cand[(size_t)q * cmax + t];
-            const float4 *row = reinterpret_cast<const float4 *>(refT + (size_t)r * d_pad);
-            float acc = 0.f;
-            // 16 row segments in flight per thread, then the FMA chain in
-            // increasing d (the exact kernel's order)
-            for (int c0 = 0; c0 < d_pad / 4; c0 += 16) {
-                float4 buf[16];
-#pragma unroll
-                for (int i = 0; i < 16; ++i) buf[i] = __ldg(row + c0 + i);
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const float *qq4 = qv + 4 * (c0 + i);
-                    float t0 = __fsub_rn(buf[i].x, qq4[0]);
-                    acc = __fmaf_rn(t0, t0, acc);
-                    t0 = __fsub_rn(buf[i].y, qq4[1]);
-                    acc = __fmaf_rn(t0, t0, acc);
-                    t0 = __fsub_rn(buf[i].z, qq4[2]);
-                    acc = __fmaf_rn(t0, t0, acc);
-                    t0 = __fsub_rn(buf[i].w, qq4[3]);
-                    acc = __fmaf_rn(t0, t0, acc);
-                }
-            }
-            key = make_key(acc, (uint32_t)r);
-        }
-        keys[t] = key;
-    }
-    __syncthreads();
+    for (int t = c + lane; t < P; t += 32) keys[t] = kKeyInf;
+    __syncwarp();
     // bitonic sort of keys[0..P), ascending
     for (int size = 2; size <= P; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int t = tid; t < P / 2; t += blockDim.x) {
+            for (int t = lane; t < P / 2; t += 32) {
                 const int lo = 2 * t - (t & (stride - 1));
                 const int hi = lo + stride;
                 const bool up = (lo & size) == 0;
@@ -495,10 +521,11 @@ __global__ void __launch_bounds__(256)
                     keys[hi] = x;
                 }
             }
-            __syncthreads();
+            __syncwarp();
         }
     }
-    if (tid == 0) {
+    int failed = 0;
+    if (lane == 0) {
         const float dk = key_dist2(keys[k - 1]);
         const float qq = qn[q];
         const float r2 = __uint_as_float(*rmax_bits);
@@ -512,9 +539,8 @@ __global__ void __launch_bounds__(256)
             retry[q] = T2 + 2.5f * tc_error_bound(qq, r2, T2, d_pad);
         }
     }
-    __syncthreads();
-    if (failed) return;
-    for (int j = tid; j < k; j += blockDim.x) {
+    if (__shfl_sync(0xffffffffu, failed, 0)) return;
+    for (int j = lane; j < k; j += 32) {
         const unsigned long long key = keys[j];
         out_dist[(size_t)j * ld_out + q] = sqrtf(key_dist2(key));
         out_idx[(size_t)j * ld_out + q] = key_index(key);
@@ -694,13 +720,13 @@ int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cud
     if (cudaMemsetAsync(nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
     int cpow = 1;
     while (cpow < p.cmax) cpow <<= 1;
-    const size_t rsmem = (((size_t)p.d_pad * 4 + 15) & ~size_t(15)) + (size_t)cpow * 8;
+    const size_t rsmem = TC_RR_WARPS * tc_rr_warp_bytes(p.d_pad, cpow);
     if (cudaFuncSetAttribute(tc_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)rsmem) != cudaSuccess)
         return kErrLaunch;
-    tc_rerank_kernel<<<Q, 256, rsmem, st>>>(R.refT, P.d, p.d_pad, qry, ldq, qn, R.rmax_bits,
-                                            thr, cand, count, p.cmax, P.k, out_dist, out_idx,
-                                            ld_out, fail, nfail, retry, cand_total);
+    tc_rerank_kernel<<<(Q + TC_RR_WARPS - 1) / TC_RR_WARPS, TC_RR_WARPS * 32, rsmem, st>>>(
+        R.refT, P.d, p.d_pad, qry, ldq, qn, R.rmax_bits, thr, cand, count, p.cmax, cpow, Q, P.k,
+        out_dist, out_idx, ld_out, fail, nfail, retry, cand_total);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (P.timer) P.timer->mark(st, kPhaseTcRerank);
     return kOk;
