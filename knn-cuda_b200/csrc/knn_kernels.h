@@ -36,7 +36,9 @@ enum Phase : int {
     kPhaseTcFallback = 6,
     kPhaseExactMain = 7,
     kPhaseExactMerge = 8,
-    kNumPhases = 9,
+    kPhaseTcRetryScan = 9,     // second-chance scan of uncertified queries
+    kPhaseTcRetryRerank = 10,
+    kNumPhases = 11,
 };
 
 struct PhaseTimer {

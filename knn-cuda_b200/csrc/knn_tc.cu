@@ -696,7 +696,7 @@ int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cud
                     const __nv_bfloat16 *qB, int Q, const float *qry, long long ldq,
                     const float *qn, const float *thr, int *count, int *cand, float *out_dist,
                     int *out_idx, long long ld_out, int *fail, int *nfail, float *retry,
-                    unsigned long long *cand_total) {
+                    unsigned long long *cand_total, bool second) {
     const TcPlan pb = plan_tc(P.N, Q, P.d, P.k, P.num_sms);
     CUtensorMap tmA, tmB;
     if (!encode_bf16_kmajor(&tmA, qB, Q, p.d_pad)) return kErrTensorMap;
@@ -716,7 +716,7 @@ int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cud
     a.cmax = p.cmax;
     a.status = P.status;
     knn_tc_scan_kernel<1><<<dim3(pb.qtiles, pb.splits), TC_THREADS, TC_SMEM, st>>>(tmA, tmB, a);
-    if (P.timer) P.timer->mark(st, kPhaseTcPass2);
+    if (P.timer) P.timer->mark(st, second ? kPhaseTcRetryScan : kPhaseTcPass2);
     if (cudaMemsetAsync(nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
     int cpow = 1;
     while (cpow < p.cmax) cpow <<= 1;
@@ -728,7 +728,7 @@ int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cud
         R.refT, P.d, p.d_pad, qry, ldq, qn, R.rmax_bits, thr, cand, count, p.cmax, cpow, Q, P.k,
         out_dist, out_idx, ld_out, fail, nfail, retry, cand_total);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-    if (P.timer) P.timer->mark(st, kPhaseTcRerank);
+    if (P.timer) P.timer->mark(st, second ? kPhaseTcRetryRerank : kPhaseTcRerank);
     return kOk;
 }
 
@@ -812,7 +812,8 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     if (cudaMemsetAsync(cand_total, 0, sizeof(unsigned long long), st) != cudaSuccess)
         return kErrCuda;
     int rc = scan_and_rerank(P, R, p, st, qB, P.Q, P.qry, P.ldq, qn, thr, count, cand,
-                             P.out_dist, P.out_idx, P.ld_out, fail, nfail, retry, cand_total);
+                             P.out_dist, P.out_idx, P.ld_out, fail, nfail, retry, cand_total,
+                             false);
     if (rc != kOk) return rc;
     int nf = 0;
     if (cudaMemcpyAsync(host_stats + 4, cand_total, sizeof(unsigned long long),
@@ -832,7 +833,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(fail, nf, retry, thr, count);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     rc = scan_and_rerank(P, R, p, st, qB, nf, qsub, ldf, qn, thr, count, cand, sd, si, ldf,
-                         fail2, nfail, retry, cand_total);
+                         fail2, nfail, retry, cand_total, true);
     if (rc != kOk) return rc;
     int nf2 = 0;
     if ((rc = read_count(nfail, host_tmp, st, nf2)) != kOk) return rc;

@@ -47,7 +47,7 @@ C_SYMBOLS = (
     "knnb200_knn_device_noalloc", "knnb200_set_phase_timing", "knnb200_last_phase_times",
 )
 PHASES = ("tc_prep_ref", "tc_prep_query", "tc_pass1", "tc_threshold", "tc_pass2", "tc_rerank",
-          "tc_fallback", "exact_main", "exact_merge")
+          "tc_fallback", "exact_main", "exact_merge", "tc_retry_scan", "tc_retry_rerank")
 CXX_SYMBOLS = (
     "_Z15knn_cuda_globalPKfiS0_iiiPfPi",
     "_Z16knn_cuda_texturePKfiS0_iiiPfPi",

@@ -113,9 +113,12 @@ def test_no_device_reports_error(knncuda, capfd):
 
 
 def test_scratch_and_split_plan_are_consistent(knncuda):
-    # splits > 1 needs splits * Q * k * 8 bytes of scratch; one split needs none
+    # the exact path's scratch: the (q, q)-duplicated query copy (d rows of
+    # Q rounded up to 32 pairs) + 256 B, plus splits * Q * k 8-byte keys when
+    # the reference set is split
     for n, q, d, k in [(16384, 4096, 128, 16), (1 << 20, 16384, 256, 100), (1000, 5000, 8, 4)]:
         s = knncuda.plan_splits(n, q, d, k)
         assert s >= 1
         b = knncuda.scratch_bytes(n, q, d, k)
-        assert b == (s * q * k * 8 if s > 1 else 0)
+        dup = d * ((q + 31) // 32 * 32) * 8
+        assert b == dup + 256 + (s * q * k * 8 if s > 1 else 0)
