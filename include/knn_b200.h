@@ -85,6 +85,52 @@ KNNB200_API int knnb200_knn_device_noalloc(const float *ref, int ref_nb, long lo
                                            long long query_ld, int dim, int k, float *knn_dist,
                                            int *knn_index, long long out_ld, void *stream);
 
+/* ---- Resident reference sets (no counterpart in the reference, which
+ * re-uploads the reference set on every call, code/knncuda.cu:341, :695). */
+typedef struct knnb200_refset knnb200_refset;
+
+/* Copy a dim x ref_nb reference set (row pitch ref_ld elements; host memory,
+ * or device memory when on_device != 0) into a resident set on the current
+ * device, with the tensor-core view prepared when the shape qualifies. */
+KNNB200_API int knnb200_refset_create(const float *ref, int ref_nb, long long ref_ld, int dim,
+                                      int on_device, knnb200_refset **out);
+KNNB200_API void knnb200_refset_destroy(knnb200_refset *rs);
+/* Device bytes held by the resident set. */
+KNNB200_API size_t knnb200_refset_device_bytes(const knnb200_refset *rs);
+/* k-NN of device-resident queries (dim x query_nb, pitch query_ld, a multiple
+ * of 4) against the resident set; results k x query_nb (pitch out_ld) in
+ * device memory.  Synchronises `stream` before returning.  Same methods and
+ * results as knnb200_knn_device. */
+KNNB200_API int knnb200_refset_knn(knnb200_refset *rs, const float *query, int query_nb,
+                                   long long query_ld, int k, int method, float *knn_dist,
+                                   int *knn_index, long long out_ld, void *stream);
+
+/* ---- Continuous-batching server over a resident set.  `slots` worker
+ * threads, each with its own stream and scratch, form batches of up to
+ * max_batch_queries queries from the head of the request queue; a batch is
+ * admitted only while the working memory of all batches in flight stays
+ * within memory_budget_bytes (one batch is always admitted).  Requests of
+ * different k share a batch (top-k_max, each takes its first k rows), and a
+ * request's result does not depend on its batch. */
+typedef struct knnb200_server knnb200_server;
+KNNB200_API int knnb200_server_create(knnb200_refset *rs, int slots, size_t memory_budget_bytes,
+                                      int max_batch_queries, int method, knnb200_server **out);
+/* Queue a request: host queries dim x query_nb (contiguous), host outputs
+ * k x query_nb filled on completion.  Buffers must stay valid until
+ * knnb200_server_wait returns.  Returns a ticket > 0, or -KNNB200_E*. */
+KNNB200_API long long knnb200_server_submit(knnb200_server *s, const float *query, int query_nb,
+                                            int k, float *knn_dist, int *knn_index);
+/* Block until the request is done; returns its status and (optionally) its
+ * latency from submit to completion. */
+KNNB200_API int knnb200_server_wait(knnb200_server *s, long long ticket, double *latency_ms);
+/* Latency percentiles of completed requests, totals, and wall time from the
+ * first submit to the last completion. */
+KNNB200_API int knnb200_server_stats(knnb200_server *s, double *p50_ms, double *p99_ms,
+                                     long long *queries_done, long long *batches_done,
+                                     double *wall_seconds);
+/* Drain the queue, stop the workers and free the server (not the refset). */
+KNNB200_API void knnb200_server_destroy(knnb200_server *s);
+
 /* Synchronise `stream` and return the status of the last device-resident
  * call on the current device (KNNB200_OK or KNNB200_ETIMEOUT / ECUDA). */
 KNNB200_API int knnb200_sync_status(void *stream);

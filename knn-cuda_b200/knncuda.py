@@ -45,6 +45,9 @@ C_SYMBOLS = (
     "knnb200_release_workspace", "knnb200_status_string", "knnb200_version",
     "knnb200_measure_fp32_peak", "knnb200_last_tc_stats",
     "knnb200_knn_device_noalloc", "knnb200_set_phase_timing", "knnb200_last_phase_times",
+    "knnb200_refset_create", "knnb200_refset_destroy", "knnb200_refset_device_bytes",
+    "knnb200_refset_knn", "knnb200_server_create", "knnb200_server_submit",
+    "knnb200_server_wait", "knnb200_server_stats", "knnb200_server_destroy",
 )
 PHASES = ("tc_prep_ref", "tc_prep_query", "tc_pass1", "tc_threshold", "tc_pass2", "tc_rerank",
           "tc_fallback", "exact_main", "exact_merge", "tc_retry_scan", "tc_retry_rerank")
@@ -95,6 +98,29 @@ def lib():
         L.knnb200_last_phase_times.argtypes = [_FP, ctypes.c_int]
         L.knnb200_last_tc_stats.restype = None
         L.knnb200_last_tc_stats.argtypes = [ctypes.POINTER(ctypes.c_longlong), _IP, _IP]
+        vp, ll, sz = ctypes.c_void_p, ctypes.c_longlong, ctypes.c_size_t
+        L.knnb200_refset_create.restype = ctypes.c_int
+        L.knnb200_refset_create.argtypes = [vp, ctypes.c_int, ll, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(vp)]
+        L.knnb200_refset_destroy.restype = None
+        L.knnb200_refset_destroy.argtypes = [vp]
+        L.knnb200_refset_device_bytes.restype = sz
+        L.knnb200_refset_device_bytes.argtypes = [vp]
+        L.knnb200_refset_knn.restype = ctypes.c_int
+        L.knnb200_refset_knn.argtypes = [vp, vp, ctypes.c_int, ll, ctypes.c_int, ctypes.c_int,
+                                         vp, vp, ll, vp]
+        L.knnb200_server_create.restype = ctypes.c_int
+        L.knnb200_server_create.argtypes = [vp, ctypes.c_int, sz, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(vp)]
+        L.knnb200_server_submit.restype = ll
+        L.knnb200_server_submit.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
+        L.knnb200_server_wait.restype = ctypes.c_int
+        L.knnb200_server_wait.argtypes = [vp, ll, ctypes.POINTER(ctypes.c_double)]
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.knnb200_server_stats.restype = ctypes.c_int
+        L.knnb200_server_stats.argtypes = [vp, dp, dp, ctypes.POINTER(ll), ctypes.POINTER(ll), dp]
+        L.knnb200_server_destroy.restype = None
+        L.knnb200_server_destroy.argtypes = [vp]
         L.knnb200_version.restype = ctypes.c_char_p
         L.knnb200_version.argtypes = []
         _lib = L
@@ -186,6 +212,119 @@ def knn_device(ref, query, k: int, method: str = "global", dist=None, index=None
     if rc != 0:
         raise RuntimeError(f"knnb200_knn_device failed: {status_string(rc)}")
     return dist, index
+
+
+class RefSet:
+    """A reference set kept resident on the current device (dim x ref_nb)."""
+
+    def __init__(self, ref):
+        import torch
+
+        self._h = ctypes.c_void_p()
+        if isinstance(ref, np.ndarray):
+            ref = np.ascontiguousarray(ref, dtype=np.float32)
+            self.dim, self.ref_nb = ref.shape
+            rc = lib().knnb200_refset_create(ref.ctypes.data, self.ref_nb, self.ref_nb, self.dim,
+                                             0, ctypes.byref(self._h))
+        else:
+            if ref.dtype != torch.float32 or ref.stride(1) != 1:
+                raise TypeError("ref must be a float32 tensor with contiguous rows")
+            self.dim, self.ref_nb = ref.shape
+            rc = lib().knnb200_refset_create(ref.data_ptr(), self.ref_nb, ref.stride(0), self.dim,
+                                             1, ctypes.byref(self._h))
+        if rc != 0:
+            raise RuntimeError(f"knnb200_refset_create failed: {status_string(rc)}")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_bytes(self) -> int:
+        return lib().knnb200_refset_device_bytes(self._h)
+
+    def knn(self, query, k: int, method: str = "global", dist=None, index=None, stream=None):
+        """k-NN of a device tensor of queries (dim x query_nb); synchronises."""
+        import torch
+
+        query_nb = query.shape[1]
+        if dist is None:
+            dist = torch.empty((k, query_nb), dtype=torch.float32, device=query.device)
+        if index is None:
+            index = torch.empty((k, query_nb), dtype=torch.int32, device=query.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(query.device)
+        rc = lib().knnb200_refset_knn(self._h, query.data_ptr(), query_nb, query.stride(0), k,
+                                      METHODS[method], dist.data_ptr(), index.data_ptr(),
+                                      dist.stride(0), ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"knnb200_refset_knn failed: {status_string(rc)}")
+        return dist, index
+
+    def close(self):
+        if self._h:
+            lib().knnb200_refset_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching k-NN server over a RefSet (host queries in, host
+    results out)."""
+
+    def __init__(self, refset: RefSet, slots: int = 2, memory_budget: int = 8 << 30,
+                 max_batch_queries: int = 4096, method: str = "cublas"):
+        self.refset = refset
+        self._h = ctypes.c_void_p()
+        rc = lib().knnb200_server_create(refset.handle, slots, memory_budget, max_batch_queries,
+                                         METHODS[method], ctypes.byref(self._h))
+        if rc != 0:
+            raise RuntimeError(f"knnb200_server_create failed: {status_string(rc)}")
+        self._bufs = {}
+
+    def submit(self, query: np.ndarray, k: int) -> int:
+        query = np.ascontiguousarray(query, dtype=np.float32)
+        qn = query.shape[1]
+        dist = np.empty((k, qn), np.float32)
+        idx = np.empty((k, qn), np.int32)
+        t = lib().knnb200_server_submit(self._h, query.ctypes.data, qn, k, dist.ctypes.data,
+                                        idx.ctypes.data)
+        if t < 0:
+            raise RuntimeError(f"knnb200_server_submit failed: {status_string(-t)}")
+        self._bufs[t] = (query, dist, idx)
+        return t
+
+    def wait(self, ticket: int):
+        """(dist, index, latency_ms) of a submitted request."""
+        lat = ctypes.c_double(0)
+        rc = lib().knnb200_server_wait(self._h, ticket, ctypes.byref(lat))
+        _, dist, idx = self._bufs.pop(ticket)
+        if rc != 0:
+            raise RuntimeError(f"request {ticket} failed: {status_string(rc)}")
+        return dist, idx, lat.value
+
+    def stats(self) -> dict:
+        p50, p99, w = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+        q, b = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        lib().knnb200_server_stats(self._h, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(q),
+                                   ctypes.byref(b), ctypes.byref(w))
+        return {"p50_ms": p50.value, "p99_ms": p99.value, "queries": q.value,
+                "batches": b.value, "wall_s": w.value}
+
+    def close(self):
+        if self._h:
+            lib().knnb200_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def sync_status(stream=None) -> int:
