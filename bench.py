@@ -72,6 +72,9 @@ def parse_args(argv=None):
     p.add_argument("--cpu-seconds", type=float, default=15.0,
                    help="target CPU time of the bounded knn_c sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--mode", choices=["batch", "serving"], default="batch",
+                   help="serving: resident serving128 set, Poisson request stream")
+    p.add_argument("--serve-seconds", type=float, default=20.0)
     return p.parse_args(argv)
 
 
@@ -447,11 +450,88 @@ def run_reference(args, D: Dist):
     }), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# serving: resident reference set, Poisson request stream, continuous batching
+# ---------------------------------------------------------------------------
+def run_serving(args, D: Dist):
+    import random
+    import threading
+
+    import torch
+
+    import knncuda
+
+    D.init("nccl")
+    w = workloads.WORKLOADS["serving128"]
+    ref, _ = workloads.generate(w, query_nb=1)
+    rs = knncuda.RefSet(ref)
+    reqs = workloads.serving_requests(w, 4000)
+
+    def drive(rate_hz, seconds, method, window=0):
+        """window > 0: closed loop with `window` requests outstanding;
+        otherwise open loop with Poisson arrivals at rate_hz."""
+        import collections
+
+        srv = knncuda.Server(rs, slots=3, memory_budget=16 << 30, max_batch_queries=8192,
+                             method=method)
+        pending = collections.deque()
+        rnd = random.Random(7)
+        i = 0
+        t_end = time.perf_counter() + seconds
+        t_next = time.perf_counter()
+        while time.perf_counter() < t_end:
+            if window:
+                while len(pending) >= window:
+                    srv.wait(pending.popleft())
+            else:
+                delay = t_next - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                t_next += rnd.expovariate(rate_hz)
+                while len(pending) >= 4096:          # bound host memory if overloaded
+                    srv.wait(pending.popleft())
+            pending.append(srv.submit(*reqs[i % len(reqs)]))
+            i += 1
+        while pending:
+            srv.wait(pending.popleft())
+        st = srv.stats()
+        srv.close()
+        st["requests"] = i
+        st["qps"] = st["queries"] / st["wall_s"] if st["wall_s"] > 0 else 0.0
+        return st
+
+    out = {}
+    for method in ("cublas", "global"):
+        drive(0, 1.0, method, window=8)            # warm the slots
+        sat = drive(0, min(5.0, args.serve_seconds / 4), method, window=24)  # capacity
+        mean_q = float(np.mean([q.shape[1] for q, _ in reqs]))
+        rate = 0.7 * sat["qps"] / mean_q            # offered load: 70 % of capacity
+        open_loop = drive(rate, args.serve_seconds, method)
+        out[method] = {"saturation_qps": sat["qps"], "offered_requests_per_s": rate,
+                       "qps": open_loop["qps"], "p50_ms": open_loop["p50_ms"],
+                       "p99_ms": open_loop["p99_ms"], "requests": open_loop["requests"],
+                       "batches": open_loop["batches"]}
+    line = {"metric": "serving queries/s and p50/p99 latency (resident 2M x 128, k in {10,50,100})",
+            "value": out["cublas"]["qps"], "unit": "queries/s", "n_gpus": D.world,
+            "higher_is_better": True, "impl": "ours", "mode": "serving",
+            "config": dict(w.describe(), refset_bytes=rs.device_bytes(),
+                           arrivals="Poisson at 70 % of the capacity measured with 24 "
+                                    "requests outstanding",
+                           request_queries="log-uniform 1..1024"),
+            "methods": out}
+    if D.rank == 0:
+        print(json.dumps(line), flush=True)
+    rs.close()
+    D.close()
+
+
 def main(argv=None):
     args = parse_args(argv)
     D = Dist()
     if args.impl == "reference":
         run_reference(args, D)
+    elif args.mode == "serving":
+        run_serving(args, D)
     else:
         run_ours(args, D)
 

@@ -369,6 +369,8 @@ __global__ void knn_merge_splits_kernel(const unsigned long long *__restrict__ p
 // ---------------------------------------------------------------------------
 namespace {
 
+constexpr size_t kMergeSmemMax = 200u * 1024u;   // dynamic smem limit of the merge kernel
+
 struct ExactShape {
     int qpw, kcap, bq, splits, n_rtiles, n_dchunks;
     size_t smem;
@@ -495,9 +497,11 @@ int launch_exact(const ExactProblem &p, cudaStream_t st) {
         const size_t per_warp = (size_t)s.splits * p.k * 8;
         int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (160u * 1024u) / per_warp));
         const size_t smem = per_warp * wpb;
-        if (smem > 200u * 1024u) return kErrUnsupported;
+        if (smem > kMergeSmemMax) return kErrUnsupported;
+        // one fixed limit for every launch: calls from several host threads
+        // must not lower it between another call's set and launch
         e = cudaFuncSetAttribute(knn_merge_splits_kernel,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMergeSmemMax);
         if (e != cudaSuccess) return kErrLaunch;
         knn_merge_splits_kernel<<<(p.Q + wpb - 1) / wpb, wpb * 32, smem, st>>>(
             a.part, s.splits, p.Q, p.k, p.out_dist, p.out_idx, p.ld_out);

@@ -590,6 +590,10 @@ bool encode_bf16_kmajor(CUtensorMap *m, const void *base, int rows, int d_pad) {
                      (uint64_t)rows, (uint64_t)d_pad, TC_BK, TC_BM, CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
+// Largest candidate-list capacity (rounded to a power of two) of any shape:
+// k <= 128 gives stride1 <= 20 and cmax = 4 * KS * stride1 <= 1280.
+constexpr int kTcCmaxPow2Max = 2048;
+
 struct TcPlan {
     int d_pad, kb, qtiles, n_tiles, splits, splits1, stride1, cmax;
 };
@@ -721,8 +725,12 @@ int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cud
     int cpow = 1;
     while (cpow < p.cmax) cpow <<= 1;
     const size_t rsmem = TC_RR_WARPS * tc_rr_warp_bytes(p.d_pad, cpow);
-    if (cudaFuncSetAttribute(tc_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)rsmem) != cudaSuccess)
+    // one fixed limit (the largest any shape uses) for every launch, so that
+    // calls from several host threads never lower it under each other
+    const size_t rsmem_max = TC_RR_WARPS * tc_rr_warp_bytes(TC_KBMAX * TC_BK, kTcCmaxPow2Max);
+    if (rsmem > rsmem_max ||
+        cudaFuncSetAttribute(tc_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)rsmem_max) != cudaSuccess)
         return kErrLaunch;
     tc_rerank_kernel<<<(Q + TC_RR_WARPS - 1) / TC_RR_WARPS, TC_RR_WARPS * 32, rsmem, st>>>(
         R.refT, P.d, p.d_pad, qry, ldq, qn, R.rmax_bits, thr, cand, count, p.cmax, cpow, Q, P.k,

@@ -15,6 +15,10 @@ Workloads (name: ref_nb, query_nb, dim, k, distribution, seed):
 * ``cloud3``   1048576, 65536, 3, 8 -- U[0,1)^3 point cloud.
 * ``mixture256`` 1048576, 16384, 256, 100 -- mixture of 1024 unit-norm centres
   (normalised Gaussian), sigma 0.1.
+* ``serving128`` 2097152 resident points, dim 128 -- mixture of 2048
+  unit-norm centres, sigma 0.1; requests of 1..1024 queries (log-uniform)
+  with k in {10, 50, 100}, Poisson arrivals (query_nb / k below are the
+  request maxima).
 """
 from __future__ import annotations
 
@@ -51,7 +55,25 @@ WORKLOADS = {
     "cloud3": Workload("cloud3", 1048576, 65536, 3, 8, "uniform", 3),
     "mixture256": Workload("mixture256", 1048576, 16384, 256, 100, "mixture", 4,
                            centres=1024, sigma=0.1, centre_kind="unitnorm"),
+    "serving128": Workload("serving128", 2097152, 1024, 128, 100, "mixture", 6,
+                           centres=2048, sigma=0.1, centre_kind="unitnorm"),
 }
+
+
+def serving_requests(w: Workload, count: int, seed: int = 66):
+    """Request stream for the serving workload: (queries dim x q, k) with q
+    log-uniform in [1, w.query_nb] and k drawn from {10, 50, 100}; the queries
+    come from the same mixture as the reference set."""
+    rng = np.random.default_rng(w.seed)
+    centres = make_centres(rng, w.centres, w.dim, w.centre_kind)
+    rq = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        q = int(np.exp(rq.uniform(0.0, np.log(w.query_nb + 1))))
+        q = max(1, min(w.query_nb, q))
+        k = int(rq.choice([10, 50, 100]))
+        out.append((np.ascontiguousarray(mixture_points(rq, centres, q, w.sigma)), k))
+    return out
 
 
 def uniform_points(rng: np.random.Generator, dim: int, n: int) -> np.ndarray:
