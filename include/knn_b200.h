@@ -131,6 +131,49 @@ KNNB200_API int knnb200_server_stats(knnb200_server *s, double *p50_ms, double *
 /* Drain the queue, stop the workers and free the server (not the refset). */
 KNNB200_API void knnb200_server_destroy(knnb200_server *s);
 
+/* ---- Many independent problems in one persistent launch (no counterpart
+ * in the reference, which solves one problem per call,
+ * code/knncuda.cu:271-278).  All pointers are device memory; the reference
+ * set of each problem must have a row pitch that is a multiple of 4 and a
+ * 16-byte-aligned base.  k <= 256 for every problem. */
+typedef struct knnb200_problem {
+    const float *ref;       /* dim x ref_nb, pitch ref_ld */
+    int ref_nb;
+    long long ref_ld;
+    const float *query;     /* dim x query_nb, pitch query_ld */
+    int query_nb;
+    long long query_ld;
+    int dim;
+    int k;
+    float *knn_dist;        /* k x query_nb, pitch out_ld */
+    int *knn_index;
+    long long out_ld;
+} knnb200_problem;
+typedef struct knnb200_batched_plan knnb200_batched_plan;
+/* Build a plan: problem table, TMA descriptors and scratch on the current
+ * device (this call allocates and synchronises).  item_stages sets the work-
+ * item granularity in pipeline stages (<= 0: 256); see the autotuner. */
+KNNB200_API int knnb200_batched_plan_create(const knnb200_problem *problems, int count,
+                                            int item_stages, knnb200_batched_plan **out);
+/* Queue the plan's work on `stream`: one persistent exact kernel over a
+ * device work queue plus a batched split merge.  Allocates nothing and does
+ * not synchronise. */
+KNNB200_API int knnb200_batched_run(knnb200_batched_plan *plan, void *stream);
+/* Synchronise `stream` and report the device status of the last run. */
+KNNB200_API int knnb200_batched_status(knnb200_batched_plan *plan, void *stream);
+/* Number of work items of the plan. */
+KNNB200_API long long knnb200_batched_items(const knnb200_batched_plan *plan);
+KNNB200_API void knnb200_batched_plan_destroy(knnb200_batched_plan *plan);
+/* Capture knnb200_batched_run(plan) into an instantiated CUDA graph
+ * (cudaGraphExec_t returned as void*); launch with knnb200_graph_launch. */
+KNNB200_API int knnb200_batched_graph_create(knnb200_batched_plan *plan, void **graph_exec);
+KNNB200_API int knnb200_graph_launch(void *graph_exec, void *stream);
+KNNB200_API void knnb200_graph_destroy(void *graph_exec);
+/* Time plans of several work-item granularities on `stream` and return the
+ * fastest (and its time per run in ms). */
+KNNB200_API int knnb200_batched_autotune(const knnb200_problem *problems, int count,
+                                         void *stream, int *best_item_stages, float *best_ms);
+
 /* Synchronise `stream` and return the status of the last device-resident
  * call on the current device (KNNB200_OK or KNNB200_ETIMEOUT / ECUDA). */
 KNNB200_API int knnb200_sync_status(void *stream);

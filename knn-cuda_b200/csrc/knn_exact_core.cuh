@@ -1,0 +1,214 @@
+// knn_exact_core.cuh -- device building blocks of the fused exact FP32 k-NN
+// kernels (single problem: knn_exact.cu; many problems in one persistent
+// launch: knn_batched.cu).  See knn_exact.cu for the algorithm.
+#pragma once
+
+#include "knn_common.cuh"
+
+namespace knnb200 {
+
+constexpr int EX_BR = 256;       // reference points per tile
+constexpr int EX_BD = 16;        // dimensions per pipeline stage
+constexpr int EX_CB = 128;       // candidate slots per query (one half tile)
+constexpr int EX_WARPS = 16;     // consumer warps
+constexpr int EX_THREADS = (EX_WARPS + 1) * 32;
+constexpr int EX_STAGES = 3;
+
+template <int QPW, int KCAP>
+struct ExCfg {
+    static constexpr int BQ = QPW * EX_WARPS;
+    // query slab of a stage: each query value stored twice, (q, q), so a
+    // 64-bit shared load yields a ready packed operand
+    static constexpr int Q_FLOATS = EX_BD * 2 * BQ;
+    static constexpr int R_FLOATS = EX_BD * EX_BR;
+    static constexpr int STAGE_FLOATS = Q_FLOATS + R_FLOATS;
+    static constexpr int STAGE_BYTES = STAGE_FLOATS * 4;
+    static constexpr int REGION = KCAP + EX_CB;   // keys per query: list + candidates
+    static constexpr size_t LIST_BYTES = (size_t)BQ * REGION * 8;
+    static constexpr size_t BAR_OFFSET = (size_t)EX_STAGES * STAGE_BYTES + LIST_BYTES;
+    static constexpr size_t SMEM = 1024 + BAR_OFFSET + 2 * EX_STAGES * 8 + 16;
+    static_assert(STAGE_BYTES % 1024 == 0, "stage alignment");
+    static_assert(KCAP % 32 == 0 && (KCAP & (KCAP - 1)) == 0, "KCAP power of two >= 32");
+};
+
+KNN_DI void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(EX_WARPS * 32) : "memory"); }
+
+// Number of elements of the sorted array L[0..n) (n a power of two) below x.
+template <int n>
+KNN_DI int rank_pow2(const unsigned long long *L, unsigned long long x) {
+    int pos = 0;
+#pragma unroll
+    for (int step = n / 2; step >= 1; step >>= 1)
+        if (L[pos + step - 1] < x) pos += step;
+    return pos + (L[pos] < x ? 1 : 0);
+}
+
+// Merge c unsorted candidate keys (L[KCAP .. KCAP+c)) into the sorted list
+// L[0..k) held by one warp.  Every key's final position is its rank in the
+// union: list element at p -> p + #(candidates below it); candidate x ->
+// #(list below x) + #(candidates below x).  Keys are unique (distinct
+// indices), so the positions form a permutation; positions >= k are dropped.
+template <int KCAP>
+KNN_DI void warp_merge(unsigned long long *L, int c, int k, int lane) {
+    constexpr int LPL = KCAP / 32;
+    constexpr int CPL = EX_CB / 32;
+    const unsigned long long *C = L + KCAP;
+    unsigned long long lv[LPL], cv[CPL];
+    int lp[LPL], cp[CPL];
+#pragma unroll
+    for (int a = 0; a < LPL; ++a) {
+        lv[a] = L[a * 32 + lane];
+        lp[a] = a * 32 + lane;
+    }
+#pragma unroll
+    for (int b = 0; b < CPL; ++b) {
+        const int t = b * 32 + lane;
+        cv[b] = t < c ? C[t] : kKeyInf;
+        cp[b] = rank_pow2<KCAP>(L, cv[b]);
+    }
+    for (int t = 0; t < c; ++t) {
+        const unsigned long long x = C[t];
+#pragma unroll
+        for (int a = 0; a < LPL; ++a) lp[a] += x < lv[a] ? 1 : 0;
+#pragma unroll
+        for (int b = 0; b < CPL; ++b) cp[b] += x < cv[b] ? 1 : 0;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int a = 0; a < LPL; ++a)
+        if (lp[a] < k) L[lp[a]] = lv[a];
+#pragma unroll
+    for (int b = 0; b < CPL; ++b)
+        if (b * 32 + lane < c && cp[b] < k) L[cp[b]] = cv[b];
+    __syncwarp();
+}
+
+// Filter one half tile (4 reference points per lane) against each query's
+// threshold, append survivors to the candidate buffers and merge.
+// d2(i, j) gives the squared distance of query i to the lane's j-th point.
+template <int QPW, int KCAP, typename D2>
+KNN_DI void select_half(unsigned long long *wl, unsigned long long (&tau)[QPW], D2 d2,
+                        uint32_t rbase, int N, int k, int lane) {
+    constexpr int REGION = KCAP + EX_CB;
+    uint32_t pm[QPW];
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) {
+        pm[i] = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t idx = rbase + j;
+            const bool p = (idx < (uint32_t)N) && make_key(d2(i, j), idx) < tau[i];
+            pm[i] |= (p ? 1u : 0u) << j;
+            any |= p;
+        }
+    }
+    if (!__any_sync(0xffffffffu, any)) return;
+    const unsigned lt = (1u << lane) - 1u;
+    int cnt[QPW];
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) {
+        unsigned long long *cb = wl + i * REGION + KCAP;
+        int c = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const bool p = (pm[i] >> j) & 1u;
+            const unsigned m = __ballot_sync(0xffffffffu, p);
+            if (p) cb[c + __popc(m & lt)] = make_key(d2(i, j), rbase + j);
+            c += __popc(m);
+        }
+        cnt[i] = c;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) {
+        if (cnt[i] > 0) {
+            unsigned long long *L = wl + i * REGION;
+            warp_merge<KCAP>(L, cnt[i], k, lane);
+            tau[i] = L[k - 1];
+        }
+    }
+}
+
+
+// Consume the n_dchunks pipeline stages of one reference tile: the lane's
+// QPW x 8 block of squared distances accumulates sum_d (r_d - q_d)^2 with a
+// rounded sub and a fused multiply-add per dimension, in increasing d (the
+// order of the reference's compute_distances loop, code/knncuda.cu:77-80).
+// `it` is the running stage counter of the CTA's ring.  Returns false (warp-
+// uniformly) if a wait timed out or another warp aborted.
+template <int QPW, int KCAP>
+KNN_DI bool consume_ref_tile(f32x2_t (&acc)[QPW][4], const float *stages, uint64_t *full,
+                             uint64_t *empty, volatile int *abort_flag, int &it, int n_dchunks,
+                             int warp, int lane, int *status) {
+    using C = ExCfg<QPW, KCAP>;
+#pragma unroll
+    for (int i = 0; i < QPW; ++i)
+#pragma unroll
+        for (int p = 0; p < 4; ++p) acc[i][p] = 0ull;
+    for (int dc = 0; dc < n_dchunks; ++dc, ++it) {
+        const int s = it % EX_STAGES;
+        const bool got = mbar_wait(&full[s], (it / EX_STAGES) & 1);
+        // warp-uniform decision: every lane leaves together or none does
+        const bool timed_out = __any_sync(0xffffffffu, !got);
+        if (timed_out || __any_sync(0xffffffffu, *abort_flag != 0)) {
+            if (lane == 0) {
+                if (timed_out) atomicMax(status, (int)kDevTimeoutFull);
+                *abort_flag = 1;
+            }
+            return false;
+        }
+        const float *qs = stages + (size_t)s * C::STAGE_FLOATS + warp * 2 * QPW;
+        const float *rs = stages + (size_t)s * C::STAGE_FLOATS + C::Q_FLOATS + lane * 4;
+#pragma unroll 4
+        for (int dd = 0; dd < EX_BD; ++dd) {
+            const float4 ra = *reinterpret_cast<const float4 *>(rs + dd * EX_BR);
+            const float4 rb = *reinterpret_cast<const float4 *>(rs + dd * EX_BR + 128);
+            const f32x2_t r0 = f2_pack(ra.x, ra.y), r1 = f2_pack(ra.z, ra.w);
+            const f32x2_t r2 = f2_pack(rb.x, rb.y), r3 = f2_pack(rb.z, rb.w);
+            const f32x2_t *qp = reinterpret_cast<const f32x2_t *>(qs + dd * 2 * C::BQ);
+#pragma unroll
+            for (int i = 0; i < QPW; ++i) {
+                const f32x2_t qq = qp[i];   // (q_i, q_i)
+                f32x2_t t;
+                t = f2_sub(r0, qq); acc[i][0] = f2_fma(t, t, acc[i][0]);
+                t = f2_sub(r1, qq); acc[i][1] = f2_fma(t, t, acc[i][1]);
+                t = f2_sub(r2, qq); acc[i][2] = f2_fma(t, t, acc[i][2]);
+                t = f2_sub(r3, qq); acc[i][3] = f2_fma(t, t, acc[i][3]);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    return true;
+}
+
+// Select both halves of a consumed tile (reference points rt*256 + ...).
+template <int QPW, int KCAP>
+KNN_DI void select_tile(unsigned long long *wl, unsigned long long (&tau)[QPW],
+                        f32x2_t (&acc)[QPW][4], int rt, int N, int k, int lane) {
+    const uint32_t rb0 = (uint32_t)rt * EX_BR + lane * 4;
+    select_half<QPW, KCAP>(
+        wl, tau,
+        [&](int i, int j) { return (j & 1) ? f2_hi(acc[i][j >> 1]) : f2_lo(acc[i][j >> 1]); },
+        rb0, N, k, lane);
+    select_half<QPW, KCAP>(
+        wl, tau,
+        [&](int i, int j) {
+            return (j & 1) ? f2_hi(acc[i][2 + (j >> 1)]) : f2_lo(acc[i][2 + (j >> 1)]);
+        },
+        rb0 + 128, N, k, lane);
+}
+
+// Number of elements of sorted A[0..n) below x.
+KNN_DI int rank_sorted(const unsigned long long *A, int n, unsigned long long x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (A[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+}  // namespace knnb200

@@ -48,7 +48,19 @@ C_SYMBOLS = (
     "knnb200_refset_create", "knnb200_refset_destroy", "knnb200_refset_device_bytes",
     "knnb200_refset_knn", "knnb200_server_create", "knnb200_server_submit",
     "knnb200_server_wait", "knnb200_server_stats", "knnb200_server_destroy",
+    "knnb200_batched_plan_create", "knnb200_batched_run", "knnb200_batched_status",
+    "knnb200_batched_items", "knnb200_batched_plan_destroy", "knnb200_batched_graph_create",
+    "knnb200_graph_launch", "knnb200_graph_destroy", "knnb200_batched_autotune",
 )
+
+
+class Problem(ctypes.Structure):
+    """Mirror of knnb200_problem (include/knn_b200.h)."""
+    _fields_ = [("ref", ctypes.c_void_p), ("ref_nb", ctypes.c_int), ("ref_ld", ctypes.c_longlong),
+                ("query", ctypes.c_void_p), ("query_nb", ctypes.c_int),
+                ("query_ld", ctypes.c_longlong), ("dim", ctypes.c_int), ("k", ctypes.c_int),
+                ("knn_dist", ctypes.c_void_p), ("knn_index", ctypes.c_void_p),
+                ("out_ld", ctypes.c_longlong)]
 PHASES = ("tc_prep_ref", "tc_prep_query", "tc_pass1", "tc_threshold", "tc_pass2", "tc_rerank",
           "tc_fallback", "exact_main", "exact_merge", "tc_retry_scan", "tc_retry_rerank")
 CXX_SYMBOLS = (
@@ -121,6 +133,27 @@ def lib():
         L.knnb200_server_stats.argtypes = [vp, dp, dp, ctypes.POINTER(ll), ctypes.POINTER(ll), dp]
         L.knnb200_server_destroy.restype = None
         L.knnb200_server_destroy.argtypes = [vp]
+        PP = ctypes.POINTER(Problem)
+        L.knnb200_batched_plan_create.restype = ctypes.c_int
+        L.knnb200_batched_plan_create.argtypes = [PP, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.POINTER(vp)]
+        L.knnb200_batched_run.restype = ctypes.c_int
+        L.knnb200_batched_run.argtypes = [vp, vp]
+        L.knnb200_batched_status.restype = ctypes.c_int
+        L.knnb200_batched_status.argtypes = [vp, vp]
+        L.knnb200_batched_items.restype = ll
+        L.knnb200_batched_items.argtypes = [vp]
+        L.knnb200_batched_plan_destroy.restype = None
+        L.knnb200_batched_plan_destroy.argtypes = [vp]
+        L.knnb200_batched_graph_create.restype = ctypes.c_int
+        L.knnb200_batched_graph_create.argtypes = [vp, ctypes.POINTER(vp)]
+        L.knnb200_graph_launch.restype = ctypes.c_int
+        L.knnb200_graph_launch.argtypes = [vp, vp]
+        L.knnb200_graph_destroy.restype = None
+        L.knnb200_graph_destroy.argtypes = [vp]
+        L.knnb200_batched_autotune.restype = ctypes.c_int
+        L.knnb200_batched_autotune.argtypes = [PP, ctypes.c_int, vp, ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_float)]
         L.knnb200_version.restype = ctypes.c_char_p
         L.knnb200_version.argtypes = []
         _lib = L
@@ -325,6 +358,88 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def problems_from(tensors):
+    """ctypes array of Problem from [(ref, query, k, dist, index)] torch tensors,
+    each (dim, n) with contiguous rows."""
+    arr = (Problem * len(tensors))()
+    for i, (ref, query, k, dist, index) in enumerate(tensors):
+        arr[i] = Problem(ref.data_ptr(), ref.shape[1], ref.stride(0), query.data_ptr(),
+                         query.shape[1], query.stride(0), ref.shape[0], k, dist.data_ptr(),
+                         index.data_ptr(), dist.stride(0))
+    return arr
+
+
+class BatchedPlan:
+    """Many independent exact k-NN problems in one persistent launch."""
+
+    def __init__(self, problems, item_stages: int = 0):
+        self._arr = problems
+        self._h = ctypes.c_void_p()
+        rc = lib().knnb200_batched_plan_create(problems, len(problems), item_stages,
+                                               ctypes.byref(self._h))
+        if rc != 0:
+            raise RuntimeError(f"knnb200_batched_plan_create failed: {status_string(rc)}")
+        self._graph = ctypes.c_void_p()
+
+    def items(self) -> int:
+        return lib().knnb200_batched_items(self._h)
+
+    def run(self, stream=None):
+        import torch
+
+        stream = stream or torch.cuda.current_stream()
+        rc = lib().knnb200_batched_run(self._h, ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"knnb200_batched_run failed: {status_string(rc)}")
+
+    def status(self, stream=None) -> int:
+        import torch
+
+        stream = stream or torch.cuda.current_stream()
+        return lib().knnb200_batched_status(self._h, ctypes.c_void_p(stream.cuda_stream))
+
+    def capture_graph(self):
+        rc = lib().knnb200_batched_graph_create(self._h, ctypes.byref(self._graph))
+        if rc != 0:
+            raise RuntimeError(f"knnb200_batched_graph_create failed: {status_string(rc)}")
+
+    def replay(self, stream=None):
+        import torch
+
+        stream = stream or torch.cuda.current_stream()
+        rc = lib().knnb200_graph_launch(self._graph, ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"knnb200_graph_launch failed: {status_string(rc)}")
+
+    def close(self):
+        if self._graph:
+            lib().knnb200_graph_destroy(self._graph)
+            self._graph = ctypes.c_void_p()
+        if self._h:
+            lib().knnb200_batched_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batched_autotune(problems, stream=None):
+    """(best item_stages, ms per run) among the tuner's candidates."""
+    import torch
+
+    stream = stream or torch.cuda.current_stream()
+    best, ms = ctypes.c_int(0), ctypes.c_float(0)
+    rc = lib().knnb200_batched_autotune(problems, len(problems),
+                                        ctypes.c_void_p(stream.cuda_stream), ctypes.byref(best),
+                                        ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"knnb200_batched_autotune failed: {status_string(rc)}")
+    return best.value, ms.value
 
 
 def sync_status(stream=None) -> int:
