@@ -72,8 +72,9 @@ def parse_args(argv=None):
     p.add_argument("--cpu-seconds", type=float, default=15.0,
                    help="target CPU time of the bounded knn_c sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--mode", choices=["batch", "serving"], default="batch",
-                   help="serving: resident serving128 set, Poisson request stream")
+    p.add_argument("--mode", choices=["batch", "serving", "batched"], default="batch",
+                   help="serving: resident serving128 set, Poisson request stream; "
+                        "batched: 512 uneven problems, one persistent launch vs per-problem")
     p.add_argument("--serve-seconds", type=float, default=20.0)
     return p.parse_args(argv)
 
@@ -525,6 +526,71 @@ def run_serving(args, D: Dist):
     D.close()
 
 
+# ---------------------------------------------------------------------------
+# batched: 512 uneven problems, per-problem launches vs one persistent launch
+# ---------------------------------------------------------------------------
+def run_batched(args, D: Dist):
+    import torch
+
+    import knncuda
+
+    D.init("nccl")
+    dev = torch.device(f"cuda:{D.local_rank}")
+    shapes = workloads.batched_problems()
+    probs, outs = [], []
+    for n, q, d, k, seed in shapes:
+        g = torch.Generator(device=dev).manual_seed(seed)
+        ldr, ldq = (n + 3) // 4 * 4, (q + 3) // 4 * 4
+        ref = torch.rand((d, ldr), generator=g, device=dev)[:, :n]
+        qry = torch.rand((d, ldq), generator=g, device=dev)[:, :q]
+        probs.append((ref, qry, k))
+        outs.append((torch.empty((k, q), device=dev), torch.empty((k, q), dtype=torch.int32,
+                                                                   device=dev)))
+    stream = torch.cuda.current_stream(dev)
+    pairs = sum(q * n for n, q, d, k, _ in shapes)
+
+    def per_problem():
+        for (ref, qry, k), (dd, ii) in zip(probs, outs):
+            knncuda.knn_device(ref, qry, k, "global", dd, ii, stream)
+
+    def timed(fn, reps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    ms_single = timed(per_problem, args.steps)
+    ref_out = [(d.clone(), i.clone()) for d, i in outs]
+    arr = knncuda.problems_from([(r, q, k, d, i) for (r, q, k), (d, i) in zip(probs, outs)])
+    best, tuned_ms = knncuda.batched_autotune(arr)
+    plan = knncuda.BatchedPlan(arr, item_stages=best)
+    ms_batched = timed(plan.run, args.steps)
+    plan.capture_graph()
+    ms_graph = timed(plan.replay, args.steps)
+    same = all(torch.equal(d, a) and torch.equal(i, b) for (d, i), (a, b) in zip(outs, ref_out))
+    if plan.status() != 0:
+        raise RuntimeError("device status error")
+    line = {"metric": "batched k-NN: 512 uneven problems per step",
+            "value": 1e3 / ms_graph, "unit": "steps/s (512 problems each)", "n_gpus": D.world,
+            "higher_is_better": True, "impl": "ours", "mode": "batched",
+            "config": {"workload": "batched512", "problems": len(shapes),
+                       "pairs_per_step": pairs, "autotuned_item_stages": best,
+                       "work_items": plan.items()},
+            "ms_per_problem_launches": ms_single, "ms_persistent_launch": ms_batched,
+            "ms_graph_replay": ms_graph, "speedup_vs_per_problem": ms_single / ms_graph,
+            "identical_to_per_problem": same}
+    plan.close()
+    if D.rank == 0:
+        print(json.dumps(line), flush=True)
+    D.close()
+
+
 def main(argv=None):
     args = parse_args(argv)
     D = Dist()
@@ -532,6 +598,8 @@ def main(argv=None):
         run_reference(args, D)
     elif args.mode == "serving":
         run_serving(args, D)
+    elif args.mode == "batched":
+        run_batched(args, D)
     else:
         run_ours(args, D)
 

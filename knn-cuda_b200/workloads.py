@@ -15,6 +15,9 @@ Workloads (name: ref_nb, query_nb, dim, k, distribution, seed):
 * ``cloud3``   1048576, 65536, 3, 8 -- U[0,1)^3 point cloud.
 * ``mixture256`` 1048576, 16384, 256, 100 -- mixture of 1024 unit-norm centres
   (normalised Gaussian), sigma 0.1.
+* ``batched512`` 512 independent problems (seed 5): ref_nb log-uniform
+  1k-64k, query_nb log-uniform 16-2048, dim in {3, 32, 64, 128, 256}, k
+  uniform 1-64, i.i.d. U[0,1) -- ``batched_problems``.
 * ``serving128`` 2097152 resident points, dim 128 -- mixture of 2048
   unit-norm centres, sigma 0.1; requests of 1..1024 queries (log-uniform)
   with k in {10, 50, 100}, Poisson arrivals (query_nb / k below are the
@@ -58,6 +61,20 @@ WORKLOADS = {
     "serving128": Workload("serving128", 2097152, 1024, 128, 100, "mixture", 6,
                            centres=2048, sigma=0.1, centre_kind="unitnorm"),
 }
+
+
+def batched_problems(count: int = 512, seed: int = 5):
+    """Shapes (ref_nb, query_nb, dim, k) and a data seed per problem of the
+    batched workload."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(np.exp(rng.uniform(np.log(1000), np.log(65536))))
+        q = int(np.exp(rng.uniform(np.log(16), np.log(2048))))
+        d = int(rng.choice([3, 32, 64, 128, 256]))
+        k = int(rng.integers(1, 65))
+        out.append((n, q, d, k, int(rng.integers(1 << 31))))
+    return out
 
 
 def serving_requests(w: Workload, count: int, seed: int = 66):
