@@ -251,7 +251,24 @@ cudaError_t launch_t(const CUtensorMap &mr, const CUtensorMap &mq, const ExactAr
 // Row pitch (in float2) of the duplicated query copy.
 static long long qdup_pitch2(int Q) { return ((long long)Q + 31) / 32 * 32; }
 
+int launch_split_merge(const unsigned long long *part, int S, int Q, int k, float *out_dist,
+                       int *out_idx, long long ld_out, cudaStream_t st) {
+    const size_t per_warp = (size_t)S * k * 8;
+    const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (160u * 1024u) / per_warp));
+    const size_t smem = per_warp * wpb;
+    if (smem > kMergeSmemMax) return kErrUnsupported;
+    // one fixed limit for every launch: calls from several host threads must
+    // not lower it between another call's set and launch
+    if (cudaFuncSetAttribute(knn_merge_splits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kMergeSmemMax) != cudaSuccess)
+        return kErrLaunch;
+    knn_merge_splits_kernel<<<(Q + wpb - 1) / wpb, wpb * 32, smem, st>>>(part, S, Q, k, out_dist,
+                                                                       out_idx, ld_out);
+    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
+}
+
 size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
+    if (lowdim_applies(N, Q, d, k)) return lowdim_scratch_bytes(N, Q, d, k, num_sms);
     ExactShape s;
     if (!choose_shape(N, Q, d, k, num_sms, s)) return 0;
     const size_t dup = (size_t)d * qdup_pitch2(Q) * sizeof(float2);
@@ -262,6 +279,7 @@ size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
 bool exact_supported_k(int k) { return k >= 1 && k <= 256; }
 
 int launch_exact(const ExactProblem &p, cudaStream_t st) {
+    if (lowdim_applies(p.N, p.Q, p.d, p.k)) return launch_lowdim(p, st);
     ExactShape s;
     if (!choose_shape(p.N, p.Q, p.d, p.k, p.num_sms, s)) return kErrUnsupported;
     if (p.force_splits > 0) s.splits = std::min(p.force_splits, std::min(s.n_rtiles, 256));
@@ -308,24 +326,16 @@ int launch_exact(const ExactProblem &p, cudaStream_t st) {
     if (e != cudaSuccess) return kErrLaunch;
     if (p.timer) p.timer->mark(st, kPhaseExactMain);
     if (s.splits > 1) {
-        const size_t per_warp = (size_t)s.splits * p.k * 8;
-        int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (160u * 1024u) / per_warp));
-        const size_t smem = per_warp * wpb;
-        if (smem > kMergeSmemMax) return kErrUnsupported;
-        // one fixed limit for every launch: calls from several host threads
-        // must not lower it between another call's set and launch
-        e = cudaFuncSetAttribute(knn_merge_splits_kernel,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMergeSmemMax);
-        if (e != cudaSuccess) return kErrLaunch;
-        knn_merge_splits_kernel<<<(p.Q + wpb - 1) / wpb, wpb * 32, smem, st>>>(
-            a.part, s.splits, p.Q, p.k, p.out_dist, p.out_idx, p.ld_out);
-        if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+        const int rc = launch_split_merge(a.part, s.splits, p.Q, p.k, p.out_dist, p.out_idx,
+                                          p.ld_out, st);
+        if (rc != kOk) return rc;
         if (p.timer) p.timer->mark(st, kPhaseExactMerge);
     }
     return kOk;
 }
 
 int exact_plan_splits(int N, int Q, int d, int k, int num_sms) {
+    if (lowdim_applies(N, Q, d, k)) return lowdim_plan_splits(N, Q, d, k, num_sms);
     ExactShape s;
     return choose_shape(N, Q, d, k, num_sms, s) ? s.splits : 0;
 }

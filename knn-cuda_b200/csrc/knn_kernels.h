@@ -102,6 +102,14 @@ inline bool encode_f32_2d(CUtensorMap *map, const void *base, uint64_t cols, uin
 }
 
 bool exact_supported_k(int k);
+// Low-dimension path (d <= 4, k <= 16): chosen by launch_exact itself.
+bool lowdim_applies(int N, int Q, int d, int k);
+size_t lowdim_scratch_bytes(int N, int Q, int d, int k, int num_sms);
+int lowdim_plan_splits(int N, int Q, int d, int k, int num_sms);
+int launch_lowdim(const ExactProblem &p, cudaStream_t st);
+// Merge per-split sorted key lists [S][Q][k] into the k x Q output.
+int launch_split_merge(const unsigned long long *part, int S, int Q, int k, float *out_dist,
+                       int *out_idx, long long ld_out, cudaStream_t st);
 size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms);
 int exact_plan_splits(int N, int Q, int d, int k, int num_sms);
 int launch_exact(const ExactProblem &p, cudaStream_t st);
