@@ -76,6 +76,11 @@ def parse_args(argv=None):
                    help="serving: resident serving128 set, Poisson request stream; "
                         "batched: 512 uneven problems, one persistent launch vs per-problem")
     p.add_argument("--serve-seconds", type=float, default=20.0)
+    p.add_argument("--ref-gpu", choices=["", "cublas", "global"], default="",
+                   help="with --impl reference: time the reference's own GPU function "
+                        "(built from its sources) instead of its CPU knn_c")
+    p.add_argument("--ref-chunks", type=int, default=2,
+                   help="query chunks of 1024 timed for --ref-gpu")
     return p.parse_args(argv)
 
 
@@ -408,9 +413,61 @@ def run_ours(args, D: Dist):
 # ---------------------------------------------------------------------------
 # reference arm: the reference's own CPU implementation on all host threads
 # ---------------------------------------------------------------------------
+def run_reference_gpu(args, D: Dist):
+    """The reference's own GPU knn_cublas / knn_cuda_global (code/knncuda.cu,
+    built unmodified into oracle/_ref/libknnref_gpu.so), called through its
+    host API, inside its limits: ref_nb <= 1,048,560 (grid-y) and a multiple
+    of 128 (knn_cublas needs ref_pitch == ref_nb), queries in chunks of 1024
+    so ref_nb * query_pitch < 2^31 (32-bit index math)."""
+    import ctypes
+
+    from oracle import oracle
+
+    w = workloads.WORKLOADS[args.workload]
+    ref, query = workloads.generate(w)
+    dim, N = ref.shape
+    n_ref = min(N, 1048560) // 128 * 128
+    ref = np.ascontiguousarray(ref[:, :n_ref])
+    chunk = min(1024, query.shape[1])
+    lib = ctypes.CDLL(oracle.REF_GPU_SO)
+    names = {"cublas": "_Z10knn_cublasPKfiS0_iiiPfPi",
+             "global": "_Z15knn_cuda_globalPKfiS0_iiiPfPi"}
+    fn = getattr(lib, names[args.ref_gpu])
+    fp, ip = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)
+    fn.restype = ctypes.c_bool
+    fn.argtypes = [fp, ctypes.c_int, fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp, ip]
+    k = w.k
+    dist = np.empty((k, chunk), np.float32)
+    idx = np.empty((k, chunk), np.int32)
+    qs = [np.ascontiguousarray(query[:, i * chunk:(i + 1) * chunk]) for i in range(args.ref_chunks + 1)]
+    call = lambda q: fn(ref.ctypes.data_as(fp), n_ref, q.ctypes.data_as(fp), chunk, dim, k,
+                        dist.ctypes.data_as(fp), idx.ctypes.data_as(ip))
+    if not call(qs[0]):
+        raise RuntimeError("reference GPU function failed")
+    t0 = time.perf_counter()
+    for q in qs[1:args.ref_chunks + 1]:
+        if not call(q):
+            raise RuntimeError("reference GPU function failed")
+    s = (time.perf_counter() - t0) / args.ref_chunks
+    value = chunk / s
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.ref_chunks,
+        "warmup": 1, "ms_per_step": s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "reference_path": f"knn_{'cublas' if args.ref_gpu == 'cublas' else 'cuda_global'} "
+                          "(reference GPU code, host API, per-call alloc + H2D + D2H)",
+        "config": dict(w.describe(), ref_nb_used=n_ref, query_chunk=chunk,
+                       note="ref_nb trimmed to the reference's limits; per-query cost "
+                            "scales ~linearly with ref_nb"),
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(ref.nbytes + qs[0].nbytes),
+                "d2h_bytes_per_step": int(dist.nbytes + idx.nbytes)}}), flush=True)
+
+
 def run_reference(args, D: Dist):
     if D.rank != 0:
         return
+    if args.ref_gpu:
+        return run_reference_gpu(args, D)
     from oracle import oracle
 
     w = workloads.WORKLOADS[args.workload]
