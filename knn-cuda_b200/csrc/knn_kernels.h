@@ -118,7 +118,7 @@ int launch_exact(const ExactProblem &p, cudaStream_t st);
 struct TcRefView {
     __nv_bfloat16 *refB;    // [N][d_pad] BF16, K-major
     float *refT;            // [N][d_pad] FP32 point-major (re-rank gathers)
-    float *rn;              // [N] squared norms
+    __nv_bfloat16 *refN;    // [N][16] squared norm as three BF16 parts, then zeros
     unsigned *rmax_bits;    // largest squared norm (float bits)
 };
 

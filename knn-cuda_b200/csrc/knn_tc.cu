@@ -4,16 +4,23 @@
 // The reference computes D = ||r||^2 - 2 Q^T R + ||q||^2 with cublasSgemm
 // plus norm kernels, sorts the full matrix and adds ||q||^2 to the survivors
 // (code/knncuda.cu:709-794).  Here the contraction runs in BF16 on the 5th-gen
-// tensor cores with FP32 accumulation in TMEM, and the norm add and selection
-// live in the GEMM epilogue; nothing of size ref_nb x query_nb is stored.
+// tensor cores with FP32 accumulation in TMEM, and the selection lives in the
+// GEMM epilogue; nothing of size ref_nb x query_nb is stored.
+//
+// The norm term is part of the contraction: the query operand is
+// bf16(-2 q) (exact scaling of bf16(q)), and one extra K=16 step multiplies
+// a tile of ones by the reference's squared norm split into three BF16 parts
+// (h + m + l = ||r||^2 to 2^-27 relative), so the accumulator holds
+// a = ||r||^2 - 2 r.q directly and the epilogue reads nothing but TMEM.
 //
 //   prep      reference / query sets -> BF16 point-major (K-major) copies,
 //             FP32 point-major copy of the reference set (for re-ranking),
-//             FP32 squared norms and the largest reference norm.
+//             the reference norm parts, FP32 query norms and the largest
+//             reference norm.
 //   pass 1    tensor scan of a strided 1/G sample of the reference tiles; each
-//             epilogue thread keeps the KS smallest a = ||r||^2 - 2 r.q of its
-//             query row in registers -> threshold T_q (KS-th smallest over the
-//             sample; over the full set about KS*G points lie below it).
+//             epilogue thread keeps the KS smallest a of its query row in
+//             registers -> threshold T_q (KS-th smallest over the sample;
+//             over the full set about KS*G points lie below it).
 //   pass 2    tensor scan of all reference tiles; the epilogue emits every
 //             reference with a < T_q into the query's candidate list.
 //   rerank    exact FP32 direct-form distances of the candidates, in the same
@@ -24,13 +31,16 @@
 //             every reference: then every point that could belong to the
 //             exact top-k was emitted, and the output is bit-identical to
 //             the exact kernel's.  Uncertified queries (sample too small, list
-//             overflow) are recomputed by the exact kernel.
+//             overflow) are scanned again or recomputed by the exact kernel.
 //
-// Error bound (u = 2^-8, BF16 unit roundoff): |bf16(r).bf16(q) - r.q| <=
-// (2u + u^2) sum|r_i q_i| + FP32 accumulation error <= eps_d ||r|| ||q|| with
-// eps_d = 2^-7 + 2^-16 + d_pad 2^-22 (twice the usual gamma_d margin for the
-// accumulation), so E_q = 2 eps_d ||q|| max||r|| + d_pad 2^-22 (max||r||^2 +
-// ||q||^2) + 2^-20 (|T_q| + ||q||^2) also covers norm and epilogue roundings.
+// Error bound (u = 2^-8, BF16 unit roundoff; K = d_pad + 16 accumulated
+// terms): |bf16(r).bf16(q) - r.q| <= (2u + u^2) sum|r_i q_i|, and the FP32
+// accumulation of the K products adds at most K 2^-23 of the sum of their
+// magnitudes (2 ||r|| ||q|| (1 + u)^2 + ||r||^2 (1 + 2^-8)); the norm itself
+// carries the FP32 rounding of its d-term FMA chain and the 2^-27 of the
+// split.  With g = K 2^-22 (twice the accumulation term) and eps = 2^-7 +
+// 2^-16 + g, E_q = 2 eps ||q|| max||r|| + g (max||r||^2 + ||q||^2) + 2^-20
+// (|T_q| + ||q||^2) covers all of them and the roundings of ||q||^2 and T_q.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -48,6 +58,9 @@ constexpr int TC_BK = 64;             // K block: 64 bf16 = 128 B (one swizzle r
 constexpr int TC_KBMAX = 4;           // d_pad <= 256
 constexpr int TC_STAGES = 5;
 constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;   // 16 KB (A or B K-block tile)
+constexpr int TC_NK = 16;             // norm step: K = 16 (h, m, l, 13 zeros)
+constexpr int TC_NORM_BYTES = TC_BN * TC_NK * 2;   // 4 KB norm tile (32-byte swizzle)
+constexpr int TC_NSLOTS = 3;          // norm tiles in flight
 constexpr int TC_KS = 16;             // pass-1 per-row list length
 constexpr int TC_EPI_WARPS = 8;       // two per TMEM lane quadrant (one per query tile)
 constexpr int TC_THREADS = 32 * (2 + TC_EPI_WARPS);   // warp 0 TMA, warp 1 MMA, 2..9 epilogue
@@ -55,15 +68,16 @@ constexpr uint32_t TC_TMEM_COLS = 512;   // 2 accumulator buffers x 2 A tiles x 
 constexpr uint32_t TC_IDESC = umma_idesc_bf16(TC_BM, TC_BN);
 
 constexpr size_t TC_OFF_A = 0;
-constexpr size_t TC_OFF_B = (size_t)2 * TC_KBMAX * TC_TILE_BYTES;             // 128 KB
-constexpr size_t TC_OFF_RN = TC_OFF_B + (size_t)TC_STAGES * TC_TILE_BYTES;    // +64 KB
-constexpr size_t TC_OFF_BAR = TC_OFF_RN + TC_EPI_WARPS * TC_BN * sizeof(float);   // rn slab per epilogue warp
-constexpr int TC_NBARS = 1 + 2 * TC_STAGES + 2 + 2 + 1;
+constexpr size_t TC_OFF_ONES = (size_t)2 * TC_KBMAX * TC_TILE_BYTES;           // 128 KB
+constexpr size_t TC_OFF_B = TC_OFF_ONES + (size_t)TC_BM * TC_NK * 2;           // +4 KB
+constexpr size_t TC_OFF_N = TC_OFF_B + (size_t)TC_STAGES * TC_TILE_BYTES;       // +80 KB
+constexpr size_t TC_OFF_BAR = TC_OFF_N + (size_t)TC_NSLOTS * TC_NORM_BYTES;     // +12 KB
+constexpr int TC_NBARS = 1 + 2 * TC_STAGES + 2 * TC_NSLOTS + 2 + 2 + 1;
 constexpr size_t TC_SMEM = 1024 + TC_OFF_BAR + TC_NBARS * 8 + 16;
+static_assert(TC_SMEM <= 232448, "scan kernel shared memory");
 
 struct TcArgs {
     int N, Q, kb_count, n_tiles, n_splits, tile_stride;
-    const float *rn;        // [N] reference squared norms
     const float *thr;       // pass 2: [Q] thresholds (a units)
     float *p1;              // pass 1: [n_splits][Q][TC_KS]
     int *cand;              // pass 2: [Q][cmax]
@@ -75,18 +89,22 @@ struct TcArgs {
 template <int MODE>   // 0: threshold sample pass, 1: emit pass
 __global__ void __launch_bounds__(TC_THREADS, 1)
     knn_tc_scan_kernel(const __grid_constant__ CUtensorMap tmA,
-                       const __grid_constant__ CUtensorMap tmB, TcArgs a) {
+                       const __grid_constant__ CUtensorMap tmB,
+                       const __grid_constant__ CUtensorMap tmN, TcArgs a) {
     extern __shared__ unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char *sA = base + TC_OFF_A;
+    unsigned char *sOnes = base + TC_OFF_ONES;
     unsigned char *sB = base + TC_OFF_B;
-    float *rn_s = reinterpret_cast<float *>(base + TC_OFF_RN);
+    unsigned char *sN = base + TC_OFF_N;
     uint64_t *bars = reinterpret_cast<uint64_t *>(base + TC_OFF_BAR);
     uint64_t *a_full = bars;
     uint64_t *b_full = bars + 1;
     uint64_t *b_empty = b_full + TC_STAGES;
-    uint64_t *acc_full = b_empty + TC_STAGES;
+    uint64_t *n_full = b_empty + TC_STAGES;
+    uint64_t *n_empty = n_full + TC_NSLOTS;
+    uint64_t *acc_full = n_empty + TC_NSLOTS;
     uint64_t *acc_empty = acc_full + 2;
     uint64_t *drain = acc_empty + 2;
     uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + TC_NBARS);
@@ -102,11 +120,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int first = ((t0 + G - 1) / G) * G;
     const int n_my = first < t1 ? (t1 - first + G - 1) / G : 0;
 
+    // the ones tile of the norm step (every element 1.0 bf16, so the
+    // swizzle does not move anything)
+    for (int i = threadIdx.x; i < TC_BM * TC_NK / 2; i += TC_THREADS)
+        reinterpret_cast<uint32_t *>(sOnes)[i] = 0x3F803F80u;
+    fence_proxy_async_smem();
     if (warp == 0 && lane == 0) {
         mbar_init(a_full, 1);
         for (int s = 0; s < TC_STAGES; ++s) {
             mbar_init(&b_full[s], 1);
             mbar_init(&b_empty[s], 1);
+        }
+        for (int s = 0; s < TC_NSLOTS; ++s) {
+            mbar_init(&n_full[s], 1);
+            mbar_init(&n_empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
@@ -117,6 +144,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         fence_mbar_init();
         prefetch_tensormap(&tmA);
         prefetch_tensormap(&tmB);
+        prefetch_tensormap(&tmN);
     }
     if (warp == 1) {
         tmem_alloc(tmem_holder, TC_TMEM_COLS);
@@ -130,8 +158,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 0) {
         // ------------------------- TMA producer --------------------------
         if (lane == 0) {
-            int issued = 0;
-            bool a_issued = false;
+            int issued = 0, n_issued = 0;
+            bool a_issued = false, ok = true;
             if (n_my > 0) {
                 mbar_arrive_expect_tx(a_full, (uint32_t)(2 * KB * TC_TILE_BYTES));
                 for (int h = 0; h < 2; ++h)
@@ -140,27 +168,45 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                                     kb * TC_BK, qtile * TC_QT + h * TC_BM);
                 a_issued = true;
             }
-            const int total = n_my * KB;
-            for (int it = 0; it < total; ++it) {
-                const int s = it % TC_STAGES;
-                if (it >= TC_STAGES && !mbar_wait(&b_empty[s], ((it / TC_STAGES) - 1) & 1)) {
-                    atomicMax(a.status, (int)kDevTimeoutEmpty);
-                    *abort_flag = 1;
+            for (int j = 0; j < n_my && ok; ++j) {
+                const int row0 = (first + j * G) * TC_BN;
+                const int ns = j % TC_NSLOTS;
+                if (j >= TC_NSLOTS && !mbar_wait(&n_empty[ns], ((j / TC_NSLOTS) - 1) & 1)) {
+                    ok = false;
                     break;
                 }
                 if (*abort_flag) break;
-                const int j = it / KB, kb = it - j * KB;
-                mbar_arrive_expect_tx(&b_full[s], TC_TILE_BYTES);
-                tma_load_2d(sB + (size_t)s * TC_TILE_BYTES, &tmB, &b_full[s], kb * TC_BK,
-                            (first + j * G) * TC_BN);
-                // pull the block two tiles ahead into L2 so the ring's loads
-                // see L2 rather than DRAM latency
-                if (j + 2 < n_my)
-                    tma_prefetch_l2_2d(&tmB, kb * TC_BK, (first + (j + 2) * G) * TC_BN);
-                issued = it + 1;
+                mbar_arrive_expect_tx(&n_full[ns], TC_NORM_BYTES);
+                tma_load_2d(sN + (size_t)ns * TC_NORM_BYTES, &tmN, &n_full[ns], 0, row0);
+                n_issued = j + 1;
+                for (int kb = 0; kb < KB; ++kb) {
+                    const int it = j * KB + kb, s = it % TC_STAGES;
+                    if (it >= TC_STAGES && !mbar_wait(&b_empty[s], ((it / TC_STAGES) - 1) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    if (*abort_flag) break;
+                    mbar_arrive_expect_tx(&b_full[s], TC_TILE_BYTES);
+                    tma_load_2d(sB + (size_t)s * TC_TILE_BYTES, &tmB, &b_full[s], kb * TC_BK,
+                                row0);
+                    // pull the block two tiles ahead into L2 so the ring's
+                    // loads see L2 rather than DRAM latency
+                    if (j + 2 < n_my)
+                        tma_prefetch_l2_2d(&tmB, kb * TC_BK, (first + (j + 2) * G) * TC_BN);
+                    issued = it + 1;
+                }
+                if (*abort_flag) break;
             }
+            if (!ok) {
+                atomicMax(a.status, (int)kDevTimeoutEmpty);
+                *abort_flag = 1;
+            }
+            // every TMA write into this CTA's shared memory has landed
             for (int it = max(0, issued - TC_STAGES); it < issued; ++it)
                 if (!mbar_wait(&b_full[it % TC_STAGES], (it / TC_STAGES) & 1))
+                    atomicMax(a.status, (int)kDevTimeoutDrain);
+            for (int j = max(0, n_issued - TC_NSLOTS); j < n_issued; ++j)
+                if (!mbar_wait(&n_full[j % TC_NSLOTS], (j / TC_NSLOTS) & 1))
                     atomicMax(a.status, (int)kDevTimeoutDrain);
             if (a_issued && !mbar_wait(a_full, 0)) atomicMax(a.status, (int)kDevTimeoutDrain);
         }
@@ -171,13 +217,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             bool ok = n_my == 0 || mbar_wait(a_full, 0);
             bool issued_mma = false;
             tc_fence_after();
+            const uint64_t odesc = umma_desc_sw32(sOnes);
             for (int j = 0; j < n_my && ok; ++j) {
                 const int b = j & 1;
                 if (j >= 2 && !mbar_wait(&acc_empty[b], ((j >> 1) - 1) & 1)) {
                     ok = false;
                     break;
                 }
+                // norm step first: D = ones x (h, m, l) = ||r||^2 per column
+                const int ns = j % TC_NSLOTS;
+                if (!mbar_wait(&n_full[ns], (j / TC_NSLOTS) & 1) || *abort_flag) {
+                    ok = false;
+                    break;
+                }
                 tc_fence_after();
+                const uint64_t ndesc = umma_desc_sw32(sN + (size_t)ns * TC_NORM_BYTES);
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    umma_bf16(tmem + (uint32_t)((b * 2 + h) * TC_BM), odesc, ndesc, TC_IDESC, 0u);
+                umma_commit(&n_empty[ns]);
+                issued_mma = true;
                 for (int kb = 0; kb < KB; ++kb) {
                     const int it = j * KB + kb, s = it % TC_STAGES;
                     if (!mbar_wait(&b_full[s], (it / TC_STAGES) & 1) || *abort_flag) {
@@ -194,11 +253,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                                 sA + (size_t)(h * TC_KBMAX + kb) * TC_TILE_BYTES);
                             umma_bf16(tmem + (uint32_t)((b * 2 + h) * TC_BM),
                                       adesc + (uint64_t)(2 * k), bdesc + (uint64_t)(2 * k),
-                                      TC_IDESC, (kb > 0 || k > 0) ? 1u : 0u);
+                                      TC_IDESC, 1u);
                         }
                     }
                     umma_commit(&b_empty[s]);
-                    issued_mma = true;
                 }
                 if (!ok) break;
                 umma_commit(&acc_full[b]);
@@ -217,7 +275,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else {
         // ------------------------- epilogue (8 warps) --------------------
         // Warp w reads TMEM lane quadrant w % 4 of query tile h = (w - 2) / 4:
-        // one query row per thread, 128 reference columns per tile.
+        // one query row per thread, 128 reference columns per tile; the
+        // accumulator already is a = ||r||^2 - 2 r.q.
         const int qd = warp & 3;
         const int h = (warp - 2) >> 2;
         const int qrow = qtile * TC_QT + h * TC_BM + qd * 32 + lane;
@@ -226,18 +285,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         float L[TC_KS];
 #pragma unroll
         for (int i = 0; i < TC_KS; ++i) L[i] = INFINITY;
-        // Norms of the next tile are fetched into registers before waiting on
-        // its accumulator, so the global-load latency overlaps the wait.
-        float rn_next[TC_BN / 32];
-        auto fetch_rn = [&](int jj) {
-#pragma unroll
-            for (int i = 0; i < TC_BN / 32; ++i) {
-                const int ridx = (first + jj * G) * TC_BN + i * 32 + lane;
-                rn_next[i] = (jj < n_my && ridx < a.N) ? __ldg(a.rn + ridx) : INFINITY;
-            }
-        };
-        fetch_rn(0);
-        float *rnb = rn_s + (warp - 2) * TC_BN;   // this warp's copy of the tile norms
         for (int j = 0; j < n_my; ++j) {
             const int b = j & 1;
             const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
@@ -250,11 +297,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             tc_fence_after();
             const int tile = first + j * G;
-            __syncwarp();
-#pragma unroll
-            for (int i = 0; i < TC_BN / 32; ++i) rnb[i * 32 + lane] = rn_next[i];
-            __syncwarp();
-            fetch_rn(j + 1);
+            // columns past the end of the set (zero rows from the TMA fill)
+            const int valid = a.N - tile * TC_BN;
 #pragma unroll 1
             for (int c = 0; c < TC_BN / 32; c += 2) {
                 // two TMEM loads in flight per wait
@@ -267,44 +311,40 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 tmem_ld_wait(v1);
 #pragma unroll
                 for (int half = 0; half < 2; ++half) {
-                    const uint32_t *v = half ? v1 : v0;
-                    const float *rc = rnb + (c + half) * 32;
-                    // a = ||r||^2 - 2 r.q for the chunk's 32 columns
-                    float av[32];
+                    uint32_t *v = half ? v1 : v0;
+                    const int cvalid = valid - (c + half) * 32;
+                    if (cvalid < 32) {
 #pragma unroll
-                    for (int e = 0; e < 32; e += 2) {
-                        const float2 r2 = *reinterpret_cast<const float2 *>(rc + e);
-                        const f32x2_t t = f2_fma(f2_pack(-2.0f, -2.0f),
-                                                 f2_pack(__uint_as_float(v[e]),
-                                                         __uint_as_float(v[e + 1])),
-                                                 f2_pack(r2.x, r2.y));
-                        av[e] = f2_lo(t);
-                        av[e + 1] = f2_hi(t);
+                        for (int e = 0; e < 32; ++e)
+                            if (e >= cvalid) v[e] = 0x7f800000u;   // +inf
                     }
                     // one comparison per chunk in the common case
-                    float mn = av[0];
+                    float mn = __uint_as_float(v[0]);
 #pragma unroll
-                    for (int e = 1; e < 32; ++e) mn = fminf(mn, av[e]);
+                    for (int e = 1; e < 32; ++e) mn = fminf(mn, __uint_as_float(v[e]));
                     const float lim = MODE == 1 ? thr : L[TC_KS - 1];
                     if (!(mn < lim)) continue;
                     uint32_t m = 0;
 #pragma unroll
-                    for (int e = 0; e < 32; ++e) m |= (av[e] < lim ? 1u : 0u) << e;
+                    for (int e = 0; e < 32; ++e) m |= (__uint_as_float(v[e]) < lim ? 1u : 0u) << e;
                     const int cbase = tile * TC_BN + (c + half) * 32;
                     while (m) {
                         const int e = __ffs(m) - 1;
                         m &= m - 1;
-                        float x = av[0];
-#pragma unroll
-                        for (int t = 1; t < 32; ++t) x = (t == e) ? av[t] : x;
                         if (MODE == 1) {
                             const int pos = atomicAdd(&a.count[qrow], 1);
                             if (pos < a.cmax) a.cand[(size_t)qrow * a.cmax + pos] = cbase + e;
-                        } else if (x < L[TC_KS - 1]) {
+                        } else {
+                            uint32_t xb = v[0];
 #pragma unroll
-                            for (int i = TC_KS - 1; i > 0; --i)
-                                L[i] = x < L[i - 1] ? L[i - 1] : (x < L[i] ? x : L[i]);
-                            L[0] = fminf(L[0], x);
+                            for (int t = 1; t < 32; ++t) xb = (t == e) ? v[t] : xb;
+                            const float x = __uint_as_float(xb);
+                            if (x < L[TC_KS - 1]) {
+#pragma unroll
+                                for (int i = TC_KS - 1; i > 0; --i)
+                                    L[i] = x < L[i - 1] ? L[i - 1] : (x < L[i] ? x : L[i]);
+                                L[0] = fminf(L[0], x);
+                            }
                         }
                     }
                 }
@@ -327,11 +367,302 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Pass-2 scan on CTA pairs (cta_group::2).  A cluster of two CTAs owns 256
+// queries (128 per CTA, resident) and walks its reference range in tiles of
+// 256 points, each CTA loading its 128-point half of every K block.  The
+// even CTA issues M = 256, N = 256 MMAs whose operands come from both CTAs'
+// shared memory, so each SM's tensor core reads 8 KB of operands per 1 MFLOP
+// instead of 16 KB (two 128 x 128 MMAs sharing one B tile): the scan is
+// tensor-bound rather than shared-memory-bound.  Each CTA's epilogue reads
+// its own 128 accumulator rows x 256 columns from TMEM.
+//
+// Synchronisation: the full barriers live in the even CTA and count the TMA
+// bytes of both CTAs (the even CTA's producer expects both shares); the
+// MMA commits arrive on the empty / accumulator-full barriers of both CTAs;
+// both CTAs' epilogue warps arrive on the even CTA's accumulator-empty
+// barriers.  Every wait is bounded; both CTAs reach the closing cluster
+// barrier on every path.
+// ---------------------------------------------------------------------------
+constexpr int TP_BN = 256;            // reference points per pair tile
+constexpr int TP_STAGES = 8;
+constexpr int TP_NSLOTS = 4;
+constexpr uint32_t TP_IDESC = umma_idesc_bf16(2 * TC_BM, TP_BN);
+
+constexpr size_t TP_OFF_A = 0;
+constexpr size_t TP_OFF_ONES = (size_t)TC_KBMAX * TC_TILE_BYTES;                // 64 KB
+constexpr size_t TP_OFF_B = TP_OFF_ONES + (size_t)TC_BM * TC_NK * 2;            // +4 KB
+constexpr size_t TP_OFF_N = TP_OFF_B + (size_t)TP_STAGES * TC_TILE_BYTES;        // +128 KB
+constexpr size_t TP_OFF_BAR = TP_OFF_N + (size_t)TP_NSLOTS * TC_NORM_BYTES;      // +16 KB
+constexpr int TP_NBARS = 1 + 2 * TP_STAGES + 2 * TP_NSLOTS + 2 + 2 + 1;
+constexpr size_t TP_SMEM = 1024 + TP_OFF_BAR + TP_NBARS * 8 + 16;
+static_assert(TP_SMEM <= 232448, "pair scan kernel shared memory");
+
+struct TpArgs {
+    int N, Q, kb_count, n_tiles, n_splits;   // n_tiles: 256-point tiles
+    const float *thr;       // [Q] thresholds (a units)
+    int *cand;              // [Q][cmax]
+    int *count;             // [Q]
+    int cmax;
+    int *status;
+};
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
+    knn_tc_pair_scan_kernel(const __grid_constant__ CUtensorMap tmA,
+                            const __grid_constant__ CUtensorMap tmB,
+                            const __grid_constant__ CUtensorMap tmN, TpArgs a) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char *sA = base + TP_OFF_A;
+    unsigned char *sOnes = base + TP_OFF_ONES;
+    unsigned char *sB = base + TP_OFF_B;
+    unsigned char *sN = base + TP_OFF_N;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(base + TP_OFF_BAR);
+    uint64_t *a_full = bars;
+    uint64_t *b_full = bars + 1;
+    uint64_t *b_empty = b_full + TP_STAGES;
+    uint64_t *n_full = b_empty + TP_STAGES;
+    uint64_t *n_empty = n_full + TP_NSLOTS;
+    uint64_t *acc_full = n_empty + TP_NSLOTS;
+    uint64_t *acc_empty = acc_full + 2;
+    uint64_t *drain = acc_empty + 2;
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + TP_NBARS);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const bool lead = rank == 0;
+    const int qpair = blockIdx.x >> 1, split = blockIdx.y;
+    const int KB = a.kb_count;
+    const int t0 = (int)((long long)a.n_tiles * split / a.n_splits);
+    const int t1 = (int)((long long)a.n_tiles * (split + 1) / a.n_splits);
+    const int n_my = t1 - t0;
+
+    for (int i = threadIdx.x; i < TC_BM * TC_NK / 2; i += TC_THREADS)
+        reinterpret_cast<uint32_t *>(sOnes)[i] = 0x3F803F80u;
+    fence_proxy_async_smem();
+    if (warp == 0 && lane == 0) {
+        mbar_init(a_full, 1);
+        for (int s = 0; s < TP_STAGES; ++s) {
+            mbar_init(&b_full[s], 1);
+            mbar_init(&b_empty[s], 1);
+        }
+        for (int s = 0; s < TP_NSLOTS; ++s) {
+            mbar_init(&n_full[s], 1);
+            mbar_init(&n_empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 2 * TC_EPI_WARPS);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+        prefetch_tensormap(&tmA);
+        prefetch_tensormap(&tmB);
+        prefetch_tensormap(&tmN);
+    }
+    if (warp == 1) {
+        tmem_alloc_pair(tmem_holder, TC_TMEM_COLS);
+        tmem_relinquish_pair();
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();   // both CTAs' barriers are initialised before any use
+    tc_fence_after();
+    const uint32_t tmem = *tmem_holder;
+
+    if (warp == 0) {
+        // ---------------- TMA producer (both CTAs) ----------------
+        if (lane == 0) {
+            int issued = 0, n_issued = 0;
+            bool a_issued = false, ok = true;
+            const int half_row = (int)rank * TC_BM;
+            if (n_my > 0) {
+                if (lead) mbar_arrive_expect_tx(a_full, (uint32_t)(2 * KB * TC_TILE_BYTES));
+                const uint32_t bar = mapa_shared(smem_u32(a_full), 0);
+                for (int kb = 0; kb < KB; ++kb)
+                    tma_load_2d_pair(sA + (size_t)kb * TC_TILE_BYTES, &tmA, bar, kb * TC_BK,
+                                     qpair * TC_QT + half_row);
+                a_issued = true;
+            }
+            for (int j = 0; j < n_my && ok; ++j) {
+                const int row0 = (t0 + j) * TP_BN + half_row;
+                const int ns = j % TP_NSLOTS;
+                if (j >= TP_NSLOTS && !mbar_wait(&n_empty[ns], ((j / TP_NSLOTS) - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                if (*abort_flag) break;
+                if (lead) mbar_arrive_expect_tx(&n_full[ns], 2 * TC_NORM_BYTES);
+                tma_load_2d_pair(sN + (size_t)ns * TC_NORM_BYTES, &tmN,
+                                 mapa_shared(smem_u32(&n_full[ns]), 0), 0, row0);
+                n_issued = j + 1;
+                for (int kb = 0; kb < KB; ++kb) {
+                    const int it = j * KB + kb, s = it % TP_STAGES;
+                    if (it >= TP_STAGES && !mbar_wait(&b_empty[s], ((it / TP_STAGES) - 1) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    if (*abort_flag) break;
+                    if (lead) mbar_arrive_expect_tx(&b_full[s], 2 * TC_TILE_BYTES);
+                    tma_load_2d_pair(sB + (size_t)s * TC_TILE_BYTES, &tmB,
+                                     mapa_shared(smem_u32(&b_full[s]), 0), kb * TC_BK, row0);
+                    if (j + 2 < n_my && row0 + 2 * TP_BN < a.N)
+                        tma_prefetch_l2_2d(&tmB, kb * TC_BK, row0 + 2 * TP_BN);
+                    issued = it + 1;
+                }
+                if (*abort_flag) break;
+            }
+            if (!ok) {
+                atomicMax(a.status, (int)kDevTimeoutEmpty);
+                *abort_flag = 1;
+            }
+            // The even CTA's full barriers count both CTAs' bytes: once its
+            // last phases completed, no TMA write into either CTA is in
+            // flight (the closing cluster barrier orders the odd CTA's exit
+            // after this).
+            if (lead) {
+                for (int it = max(0, issued - TP_STAGES); it < issued; ++it)
+                    if (!mbar_wait(&b_full[it % TP_STAGES], (it / TP_STAGES) & 1))
+                        atomicMax(a.status, (int)kDevTimeoutDrain);
+                for (int j = max(0, n_issued - TP_NSLOTS); j < n_issued; ++j)
+                    if (!mbar_wait(&n_full[j % TP_NSLOTS], (j / TP_NSLOTS) & 1))
+                        atomicMax(a.status, (int)kDevTimeoutDrain);
+                if (a_issued && !mbar_wait(a_full, 0)) atomicMax(a.status, (int)kDevTimeoutDrain);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---------------- MMA issuer (even CTA) ----------------
+        if (lead && lane == 0) {
+            bool ok = n_my == 0 || mbar_wait(a_full, 0);
+            bool issued_mma = false;
+            tc_fence_after();
+            const uint64_t odesc = umma_desc_sw32(sOnes);
+            for (int j = 0; j < n_my && ok; ++j) {
+                const int b = j & 1;
+                if (j >= 2 && !mbar_wait_cluster(&acc_empty[b], ((j >> 1) - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                const int ns = j % TP_NSLOTS;
+                if (!mbar_wait(&n_full[ns], (j / TP_NSLOTS) & 1) || *abort_flag) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                umma_bf16_pair(tmem + (uint32_t)(b * TP_BN), odesc,
+                               umma_desc_sw32(sN + (size_t)ns * TC_NORM_BYTES), TP_IDESC, 0u);
+                umma_commit_pair_mc(&n_empty[ns], 0x3);
+                issued_mma = true;
+                for (int kb = 0; kb < KB; ++kb) {
+                    const int it = j * KB + kb, s = it % TP_STAGES;
+                    if (!mbar_wait(&b_full[s], (it / TP_STAGES) & 1) || *abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t adesc = umma_desc_sw128(sA + (size_t)kb * TC_TILE_BYTES);
+                    const uint64_t bdesc = umma_desc_sw128(sB + (size_t)s * TC_TILE_BYTES);
+#pragma unroll
+                    for (int k = 0; k < TC_BK / 16; ++k)
+                        umma_bf16_pair(tmem + (uint32_t)(b * TP_BN), adesc + (uint64_t)(2 * k),
+                                       bdesc + (uint64_t)(2 * k), TP_IDESC, 1u);
+                    umma_commit_pair_mc(&b_empty[s], 0x3);
+                }
+                if (!ok) break;
+                umma_commit_pair_mc(&acc_full[b], 0x3);
+            }
+            if (!ok) {
+                atomicMax(a.status, (int)kDevTimeoutFull);
+                *abort_flag = 1;
+            }
+            if (issued_mma) {
+                umma_commit_pair(drain);
+                if (!mbar_wait(drain, 0)) atomicMax(a.status, (int)kDevTimeoutDrain);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue (8 warps per CTA) ----------------
+        // Warp w: TMEM lane quadrant w % 4 (32 query rows), column half
+        // (w - 2) / 4 (128 of the tile's 256 reference points).
+        const int qd = warp & 3;
+        const int hc = (warp - 2) >> 2;
+        const int qrow = qpair * TC_QT + (int)rank * TC_BM + qd * 32 + lane;
+        const float thr = qrow < a.Q ? a.thr[qrow] : -INFINITY;
+        for (int j = 0; j < n_my; ++j) {
+            const int b = j & 1;
+            const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
+            if (__any_sync(0xffffffffu, !got || *abort_flag != 0)) {
+                if (lane == 0) {
+                    if (!got) atomicMax(a.status, (int)kDevTimeoutFull);
+                    *abort_flag = 1;
+                }
+                break;
+            }
+            tc_fence_after();
+            const int col0 = (t0 + j) * TP_BN + hc * 128;   // first reference of this warp
+            const int valid = a.N - col0;
+#pragma unroll 1
+            for (int c = 0; c < 4; c += 2) {
+                uint32_t v0[32], v1[32];
+                const uint32_t tbase = tmem + ((uint32_t)(qd * 32) << 16) +
+                                       (uint32_t)(b * TP_BN + hc * 128 + c * 32);
+                tmem_ld32(tbase, v0);
+                tmem_ld32(tbase + 32, v1);
+                tmem_ld_wait(v0);
+                tmem_ld_wait(v1);
+#pragma unroll
+                for (int half = 0; half < 2; ++half) {
+                    uint32_t *v = half ? v1 : v0;
+                    const int cvalid = valid - (c + half) * 32;
+                    if (cvalid < 32) {
+#pragma unroll
+                        for (int e = 0; e < 32; ++e)
+                            if (e >= cvalid) v[e] = 0x7f800000u;   // +inf
+                    }
+                    float mn = __uint_as_float(v[0]);
+#pragma unroll
+                    for (int e = 1; e < 32; ++e) mn = fminf(mn, __uint_as_float(v[e]));
+                    if (!(mn < thr)) continue;
+                    uint32_t m = 0;
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) m |= (__uint_as_float(v[e]) < thr ? 1u : 0u) << e;
+                    const int cbase = col0 + (c + half) * 32;
+                    while (m) {
+                        const int e = __ffs(m) - 1;
+                        m &= m - 1;
+                        const int pos = atomicAdd(&a.count[qrow], 1);
+                        if (pos < a.cmax) a.cand[(size_t)qrow * a.cmax + pos] = cbase + e;
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                if (lead)
+                    mbar_arrive(&acc_empty[b]);
+                else
+                    mbar_arrive_cluster(mapa_shared(smem_u32(&acc_empty[b]), 0));
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();   // no MMA / TMA of the pair touches either CTA after this
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc_pair(tmem, TC_TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
 // error bound of the BF16 expansion (see the file comment)
 // ---------------------------------------------------------------------------
 KNN_DI float tc_error_bound(float qq, float r2, float T, int d_pad) {
-    const float g = (float)d_pad * 2.384185791015625e-07f;   // d_pad * 2^-22
-    const float eps = 0.0078125f + 1.52587890625e-05f + g;    // 2^-7 + 2^-16 + d_pad 2^-22
+    const float g = (float)(d_pad + TC_NK) * 2.384185791015625e-07f;   // K * 2^-22
+    const float eps = 0.0078125f + 1.52587890625e-05f + g;              // 2^-7 + 2^-16 + g
     return 2.f * eps * sqrtf(qq * r2) + g * (r2 + qq) + 9.5367431640625e-07f * (fabsf(T) + qq);
 }
 
@@ -339,10 +670,15 @@ KNN_DI float tc_error_bound(float qq, float r2, float T, int d_pad) {
 // prep kernels
 // ---------------------------------------------------------------------------
 
-// Squared norm of each point of a dim x n set (sequential FP32 fma over d)
-// and the largest squared norm (non-negative float bits compare as unsigned).
+// Squared norm of each point of a dim x n set (sequential FP32 fma over d):
+// as FP32 (nrm) and/or as the norm-step row of the tensor scan (parts: h, m,
+// l = successive BF16 roundings of the remainder, so h + m + l equals the
+// norm to 2^-27 relative; each subtraction is exact by Sterbenz' lemma;
+// 13 zeros), and the largest squared norm (non-negative float bits compare
+// as unsigned).
 __global__ void tc_norms_kernel(const float *__restrict__ x, int n, long long ld, int d,
-                                float *__restrict__ nrm, unsigned *__restrict__ max_bits) {
+                                float *__restrict__ nrm, __nv_bfloat16 *__restrict__ parts,
+                                unsigned *__restrict__ max_bits) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     float s = 0.f;
     if (p < n) {
@@ -350,7 +686,29 @@ __global__ void tc_norms_kernel(const float *__restrict__ x, int n, long long ld
             const float v = x[(size_t)dd * ld + p];
             s = fmaf(v, v, s);
         }
-        nrm[p] = s;
+        if (nrm) nrm[p] = s;
+        if (parts) {
+            __nv_bfloat16 hml[3];
+            if (isfinite(s)) {
+                float rem = s;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    hml[i] = __float2bfloat16_rn(rem);
+                    rem = rem - __bfloat162float(hml[i]);
+                }
+            } else {
+                hml[0] = __float2bfloat16_rn(INFINITY);
+                hml[1] = hml[2] = __float2bfloat16_rn(0.f);
+            }
+            uint4 row[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+            __nv_bfloat16 *e = reinterpret_cast<__nv_bfloat16 *>(row);
+            e[0] = hml[0];
+            e[1] = hml[1];
+            e[2] = hml[2];
+            uint4 *dst = reinterpret_cast<uint4 *>(parts + (size_t)p * TC_NK);
+            dst[0] = row[0];
+            dst[1] = row[1];
+        }
     }
     unsigned m = __float_as_uint(s);
 #pragma unroll
@@ -358,10 +716,11 @@ __global__ void tc_norms_kernel(const float *__restrict__ x, int n, long long ld
     if ((threadIdx.x & 31) == 0 && max_bits) atomicMax(max_bits, m);
 }
 
-// dim x n (row pitch ld) FP32 -> n x d_pad BF16 (and optionally FP32),
+// dim x n (row pitch ld) FP32 -> n x d_pad BF16 of scale * x (scale a power
+// of two, so bf16(scale x) = scale bf16(x)) and optionally FP32 x,
 // zero-padded in [d, d_pad).  32 x 32 tiles through shared memory.
 __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld, int d,
-                               int d_pad, __nv_bfloat16 *__restrict__ xb,
+                               int d_pad, float scale, __nv_bfloat16 *__restrict__ xb,
                                float *__restrict__ xt) {
     __shared__ float tile[32][33];
     const int p0 = blockIdx.x * 32, d0 = blockIdx.y * 32;
@@ -377,7 +736,7 @@ __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld,
         const int p = p0 + ty + 8 * i, dd = d0 + tx;
         if (p < n && dd < d_pad) {
             const float v = tile[tx][ty + 8 * i];
-            xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(v);
+            xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(v * scale);
             if (xt) xt[(size_t)p * d_pad + dd] = v;
         }
     }
@@ -590,12 +949,19 @@ bool encode_bf16_kmajor(CUtensorMap *m, const void *base, int rows, int d_pad) {
                      (uint64_t)rows, (uint64_t)d_pad, TC_BK, TC_BM, CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
+// Norm-step rows [rows][16] BF16, 128-row boxes with the 32-byte swizzle.
+bool encode_norm_rows(CUtensorMap *m, const void *base, int rows) {
+    return encode_2d(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, (uint64_t)TC_NK, (uint64_t)rows,
+                     (uint64_t)TC_NK, TC_NK, TC_BN, CU_TENSOR_MAP_SWIZZLE_32B);
+}
+
 // Largest candidate-list capacity (rounded to a power of two) of any shape:
 // k <= 128 gives stride1 <= 20 and cmax = 4 * KS * stride1 <= 1280.
 constexpr int kTcCmaxPow2Max = 2048;
 
 struct TcPlan {
     int d_pad, kb, qtiles, n_tiles, splits, splits1, stride1, cmax;
+    int n_tiles2, splits2;   // pair scan: 256-point tiles, splits over CTA pairs
 };
 
 // Splits that fill whole waves of one CTA per SM for `tiles` tiles per
@@ -630,6 +996,8 @@ TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
     p.splits1 = choose_splits(p.qtiles, (p.n_tiles + p.stride1 - 1) / p.stride1, 32, 8.0,
                               num_sms);
     p.cmax = 4 * TC_KS * p.stride1;
+    p.n_tiles2 = (N + TP_BN - 1) / TP_BN;
+    p.splits2 = choose_splits(p.qtiles, p.n_tiles2, 8, 2.0, std::max(1, num_sms / 2));
     return p;
 }
 
@@ -653,7 +1021,7 @@ bool tc_supported(int N, int Q, int d, int k) {
 
 size_t tc_ref_bytes(int N, int d) {
     const int d_pad = (d + 63) / 64 * 64;
-    return (size_t)N * d_pad * 2 + (size_t)N * d_pad * 4 + (size_t)N * 4 + 4 * 256;
+    return (size_t)N * d_pad * 2 + (size_t)N * d_pad * 4 + (size_t)N * TC_NK * 2 + 4 * 256;
 }
 
 static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
@@ -675,9 +1043,10 @@ int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, i
                    cudaStream_t st) {
     const int d_pad = (d + 63) / 64 * 64;
     if (cudaMemsetAsync(v.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess) return kErrCuda;
-    tc_norms_kernel<<<(N + 255) / 256, 256, 0, st>>>(ref, N, ldr, d, v.rn, v.rmax_bits);
+    tc_norms_kernel<<<(N + 255) / 256, 256, 0, st>>>(ref, N, ldr, d, nullptr, v.refN,
+                                                     v.rmax_bits);
     dim3 g((N + 31) / 32, d_pad / 32);
-    tc_pack_kernel<<<g, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, v.refB, v.refT);
+    tc_pack_kernel<<<g, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, 1.0f, v.refB, v.refT);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
@@ -687,7 +1056,7 @@ TcRefView tc_carve_ref(void *mem, int N, int d) {
     TcRefView v;
     v.refB = cv.take<__nv_bfloat16>((size_t)N * d_pad);
     v.refT = cv.take<float>((size_t)N * d_pad);
-    v.rn = cv.take<float>(N);
+    v.refN = cv.take<__nv_bfloat16>((size_t)N * TC_NK);
     v.rmax_bits = cv.take<unsigned>(1);
     return v;
 }
@@ -702,24 +1071,43 @@ int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cud
                     int *out_idx, long long ld_out, int *fail, int *nfail, float *retry,
                     unsigned long long *cand_total, bool second) {
     const TcPlan pb = plan_tc(P.N, Q, P.d, P.k, P.num_sms);
-    CUtensorMap tmA, tmB;
+    const bool pair = !second;   // the full scan runs on CTA pairs
+    CUtensorMap tmA, tmB, tmN;
     if (!encode_bf16_kmajor(&tmA, qB, Q, p.d_pad)) return kErrTensorMap;
     if (!encode_bf16_kmajor(&tmB, R.refB, P.N, p.d_pad)) return kErrTensorMap;
-    TcArgs a;
-    a.N = P.N;
-    a.Q = Q;
-    a.kb_count = p.kb;
-    a.n_tiles = p.n_tiles;
-    a.n_splits = pb.splits;
-    a.tile_stride = 1;
-    a.rn = R.rn;
-    a.thr = thr;
-    a.p1 = nullptr;
-    a.cand = cand;
-    a.count = count;
-    a.cmax = p.cmax;
-    a.status = P.status;
-    knn_tc_scan_kernel<1><<<dim3(pb.qtiles, pb.splits), TC_THREADS, TC_SMEM, st>>>(tmA, tmB, a);
+    if (!encode_norm_rows(&tmN, R.refN, P.N)) return kErrTensorMap;
+    if (pair) {
+        TpArgs a;
+        a.N = P.N;
+        a.Q = Q;
+        a.kb_count = p.kb;
+        a.n_tiles = pb.n_tiles2;
+        a.n_splits = pb.splits2;
+        a.thr = thr;
+        a.cand = cand;
+        a.count = count;
+        a.cmax = p.cmax;
+        a.status = P.status;
+        knn_tc_pair_scan_kernel<<<dim3(2 * pb.qtiles, pb.splits2), TC_THREADS, TP_SMEM, st>>>(
+            tmA, tmB, tmN, a);
+    } else {
+        TcArgs a;
+        a.N = P.N;
+        a.Q = Q;
+        a.kb_count = p.kb;
+        a.n_tiles = p.n_tiles;
+        a.n_splits = pb.splits;
+        a.tile_stride = 1;
+        a.thr = thr;
+        a.p1 = nullptr;
+        a.cand = cand;
+        a.count = count;
+        a.cmax = p.cmax;
+        a.status = P.status;
+        knn_tc_scan_kernel<1><<<dim3(pb.qtiles, pb.splits), TC_THREADS, TC_SMEM, st>>>(
+            tmA, tmB, tmN, a);
+    }
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (P.timer) P.timer->mark(st, second ? kPhaseTcRetryScan : kPhaseTcPass2);
     if (cudaMemsetAsync(nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
     int cpow = 1;
@@ -778,23 +1166,28 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     if (cv.used > P.scratch_bytes) return kErrScratch;
     PhaseTimer *tm = P.timer;
 
-    // queries: norms + BF16 K-major copy
-    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, qn, nullptr);
+    // queries: norms + BF16 K-major copy of -2 q
+    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, qn, nullptr,
+                                                       nullptr);
     tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
-        P.qry, P.Q, P.ldq, P.d, p.d_pad, qB, nullptr);
+        P.qry, P.Q, P.ldq, P.d, p.d_pad, -2.0f, qB, nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (tm) tm->mark(st, kPhaseTcPrepQuery);
     if (cudaFuncSetAttribute(knn_tc_scan_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TC_SMEM) != cudaSuccess ||
         cudaFuncSetAttribute(knn_tc_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TC_SMEM) != cudaSuccess)
+                             (int)TC_SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(knn_tc_pair_scan_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TP_SMEM) != cudaSuccess)
         return kErrLaunch;
 
     // pass 1: thresholds from a strided sample of the reference tiles
     {
-        CUtensorMap tmA, tmB;
+        CUtensorMap tmA, tmB, tmN;
         if (!encode_bf16_kmajor(&tmA, qB, P.Q, p.d_pad)) return kErrTensorMap;
         if (!encode_bf16_kmajor(&tmB, R.refB, P.N, p.d_pad)) return kErrTensorMap;
+        if (!encode_norm_rows(&tmN, R.refN, P.N)) return kErrTensorMap;
         TcArgs a;
         a.N = P.N;
         a.Q = P.Q;
@@ -802,7 +1195,6 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
         a.n_tiles = p.n_tiles;
         a.n_splits = p.splits1;
         a.tile_stride = p.stride1;
-        a.rn = R.rn;
         a.thr = thr;
         a.p1 = p1;
         a.cand = cand;
@@ -810,7 +1202,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
         a.cmax = p.cmax;
         a.status = P.status;
         knn_tc_scan_kernel<0><<<dim3(p.qtiles, p.splits1), TC_THREADS, TC_SMEM, st>>>(tmA, tmB,
-                                                                                      a);
+                                                                                      tmN, a);
         if (tm) tm->mark(st, kPhaseTcPass1);
         tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, p.splits1, P.Q, qn,
                                                                R.rmax_bits, p.d_pad, thr, count);
@@ -835,9 +1227,9 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     // thresholds that certify (list overflows excepted)
     gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, fail,
                                                                        nf, qsub, ldf);
-    tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(qsub, nf, ldf, P.d, qn, nullptr);
+    tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(qsub, nf, ldf, P.d, qn, nullptr, nullptr);
     tc_pack_kernel<<<dim3((nf + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
-        qsub, nf, ldf, P.d, p.d_pad, qB, nullptr);
+        qsub, nf, ldf, P.d, p.d_pad, -2.0f, qB, nullptr);
     tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(fail, nf, retry, thr, count);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     rc = scan_and_rerank(P, R, p, st, qB, nf, qsub, ldf, qn, thr, count, cand, sd, si, ldf,

@@ -38,6 +38,25 @@ KNN_DI uint64_t umma_desc_sw128(const void *smem_ptr) {
     return d;
 }
 
+// Same for the 32-byte swizzle (a TMA SWIZZLE_32B box of 16 bf16 x rows):
+// rows of 32 B (one K=16 step), 8-row atoms 256 B apart, layout type
+// SWIZZLE_32B (6).  The buffer is 256-B aligned.
+KNN_DI uint64_t umma_desc_sw32(const void *smem_ptr) {
+    const uint64_t addr = smem_u32(smem_ptr);
+    uint64_t d = (addr >> 4) & 0x3FFFull;
+    d |= 1ull << 16;
+    d |= (uint64_t)(256 >> 4) << 32;
+    d |= 1ull << 46;
+    d |= 6ull << 61;
+    return d;
+}
+
+// Make this thread's generic-proxy shared-memory writes visible to the
+// async proxy (tensor-core operand reads) after the next barrier.
+KNN_DI void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // Instruction descriptor, kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
 // (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 in
 // [17,23), M >> 4 in [24,29).
@@ -62,6 +81,87 @@ KNN_DI void umma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_
 KNN_DI void umma_commit(uint64_t *bar) {
     asm volatile(
         "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_u32(bar))
+        : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// CTA pairs (cluster of 2, cta_group::2): one MMA spans both CTAs' tensor
+// cores.  A (M = 256) is split by rows between the two CTAs' shared memory,
+// B (N) by rows (reference points) likewise, at the same shared-memory
+// offsets; CTA r's TMEM receives accumulator rows r * 128 .. + 127, all N
+// columns.  The even CTA of the pair (rank 0) issues the MMAs.
+// ---------------------------------------------------------------------------
+KNN_DI uint32_t cluster_ctarank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// Address of the same shared-memory offset in CTA `rank` of the cluster.
+KNN_DI uint32_t mapa_shared(uint32_t local_addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local_addr), "r"(rank));
+    return r;
+}
+// All threads of both CTAs; orders shared-memory (and barrier-init) writes
+// before the barrier against reads after it, cluster-wide.
+KNN_DI void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                     : "memory");
+}
+// Arrive on an mbarrier of another CTA of the cluster (shared::cluster
+// address), releasing this thread's prior writes / TMEM reads at cluster
+// scope.
+KNN_DI void mbar_arrive_cluster(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+                 : "memory");
+}
+// TMA 2-D load into this CTA's shared memory whose completion is counted on
+// an mbarrier of either CTA of the pair (shared::cluster address).
+KNN_DI void tma_load_2d_pair(void *smem_dst, const CUtensorMap *map, uint32_t bar_cluster_addr,
+                             int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(smem_dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster_addr), "r"(x), "r"(y)
+        : "memory");
+}
+// Both CTAs of the pair execute these (same warp), with the same holder
+// offset.
+KNN_DI void tmem_alloc_pair(uint32_t *smem_holder, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(smem_holder)),
+                 "r"(ncols)
+                 : "memory");
+}
+KNN_DI void tmem_relinquish_pair() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+KNN_DI void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+                 : "memory");
+}
+KNN_DI void umma_bf16_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                           uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+// Arrive on the mbarrier at this shared-memory offset in every CTA of
+// cta_mask once the pair MMAs issued so far have completed.
+KNN_DI void umma_commit_pair_mc(uint64_t *bar, uint16_t cta_mask) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+        " [%0], %1;" ::"r"(smem_u32(bar)),
+        "h"(cta_mask)
+        : "memory");
+}
+KNN_DI void umma_commit_pair(uint64_t *bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
             smem_u32(bar))
         : "memory");
 }

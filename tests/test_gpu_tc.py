@@ -30,6 +30,7 @@ CASES = [
     (4, 32768, 1, 32, 1),            # Q = 1, k = 1
     (5, 70001, 1000, 200, 50),       # d not a multiple of 64
     (6, 131072, 96, 16, 10),         # smallest tensor-path dim
+    (7, 33000, 300, 96, 20),         # last 256-point tile: second half partly valid
 ]
 
 
