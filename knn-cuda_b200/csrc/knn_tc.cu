@@ -76,11 +76,18 @@ constexpr int TC_NBARS = 1 + 2 * TC_STAGES + 2 * TC_NSLOTS + 2 + 2 + 1;
 constexpr size_t TC_SMEM = 1024 + TC_OFF_BAR + TC_NBARS * 8 + 16;
 static_assert(TC_SMEM <= 232448, "scan kernel shared memory");
 
+// Candidate entries: (order-preserving bits of a) << 32 | reference index,
+// so that unsigned order is (a, index) order for every non-NaN a.
+KNN_DI uint32_t ord_bits(uint32_t f) { return (f & 0x80000000u) ? ~f : (f | 0x80000000u); }
+KNN_DI float ord_float(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
 struct TcArgs {
     int N, Q, kb_count, n_tiles, n_splits, tile_stride;
     const float *thr;       // pass 2: [Q] thresholds (a units)
     float *p1;              // pass 1: [n_splits][Q][TC_KS]
-    int *cand;              // pass 2: [Q][cmax]
+    unsigned long long *cand;   // pass 2: [Q][cmax] (a, index) entries
     int *count;             // pass 2: [Q]
     int cmax;
     int *status;
@@ -331,13 +338,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     while (m) {
                         const int e = __ffs(m) - 1;
                         m &= m - 1;
+                        uint32_t xb = v[0];
+#pragma unroll
+                        for (int t = 1; t < 32; ++t) xb = (t == e) ? v[t] : xb;
                         if (MODE == 1) {
                             const int pos = atomicAdd(&a.count[qrow], 1);
-                            if (pos < a.cmax) a.cand[(size_t)qrow * a.cmax + pos] = cbase + e;
+                            if (pos < a.cmax)
+                                a.cand[(size_t)qrow * a.cmax + pos] =
+                                    ((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e);
                         } else {
-                            uint32_t xb = v[0];
-#pragma unroll
-                            for (int t = 1; t < 32; ++t) xb = (t == e) ? v[t] : xb;
                             const float x = __uint_as_float(xb);
                             if (x < L[TC_KS - 1]) {
 #pragma unroll
@@ -400,7 +409,7 @@ static_assert(TP_SMEM <= 232448, "pair scan kernel shared memory");
 struct TpArgs {
     int N, Q, kb_count, n_tiles, n_splits;   // n_tiles: 256-point tiles
     const float *thr;       // [Q] thresholds (a units)
-    int *cand;              // [Q][cmax]
+    unsigned long long *cand;   // [Q][cmax] (a, index) entries
     int *count;             // [Q]
     int cmax;
     int *status;
@@ -634,8 +643,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
                     while (m) {
                         const int e = __ffs(m) - 1;
                         m &= m - 1;
+                        uint32_t xb = v[0];
+#pragma unroll
+                        for (int t = 1; t < 32; ++t) xb = (t == e) ? v[t] : xb;
                         const int pos = atomicAdd(&a.count[qrow], 1);
-                        if (pos < a.cmax) a.cand[(size_t)qrow * a.cmax + pos] = cbase + e;
+                        if (pos < a.cmax)
+                            a.cand[(size_t)qrow * a.cmax + pos] =
+                                ((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e);
                     }
                 }
             }
@@ -770,104 +784,8 @@ __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
     count[q] = 0;
 }
 
-// Exact FP32 re-rank of each query's candidates + certification.
-// One warp per query (TC_RR_WARPS queries per block, no block-wide syncs).
-// Candidates are handled 32 at a time, one per lane: the warp loads the 32
-// candidate rows of the FP32 point-major copy with coalesced 16-byte loads
-// (two rows per instruction) into a padded shared tile, 64 dimensions at a
-// time, and each lane then runs its candidate's FMA chain in increasing d --
-// the fused exact kernel's arithmetic and order, so distances are identical.
-// The keys are bitonic-sorted by the warp.
-//
-// An uncertified query is appended to fail_list and retry[q] receives a
-// threshold for a second scan: when it had at least k candidates, their k-th
-// exact distance D_k bounds the true k-th from above, so every point of the
-// true top-k has a < D_k (1+g) + E - ||q||^2 and a second scan emitting below
-// D_k (1+g) + 2.5 E - ||q||^2 passes the check; with fewer than k candidates
-// the threshold is widened by 8 E; an overflowing list gets NaN (no second
-// scan: exact kernel).
-constexpr int TC_RR_WARPS = 4;
-constexpr int TC_RR_DCH = 64;                 // dimensions per staged chunk
-constexpr int TC_RR_STRIDE = TC_RR_DCH + 1;   // padded row: conflict-free column reads
-
-__host__ __device__ inline size_t tc_rr_warp_bytes(int d_pad, int cpow) {
-    return (((size_t)d_pad * 4 + 32 * TC_RR_STRIDE * 4 + 15) & ~size_t(15)) + (size_t)cpow * 8;
-}
-
-__global__ void __launch_bounds__(TC_RR_WARPS * 32)
-    tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
-                     const float *__restrict__ qry, long long ldq, const float *__restrict__ qn,
-                     const unsigned *__restrict__ rmax_bits, const float *__restrict__ thr,
-                     const int *__restrict__ cand, const int *__restrict__ count, int cmax,
-                     int cpow, int Q, int k, float *__restrict__ out_dist,
-                     int *__restrict__ out_idx, long long ld_out, int *__restrict__ fail_list,
-                     int *__restrict__ n_fail, float *__restrict__ retry,
-                     unsigned long long *__restrict__ cand_total) {
-    extern __shared__ unsigned char rsm[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int q = blockIdx.x * TC_RR_WARPS + warp;
-    if (q >= Q) return;
-    unsigned char *mine = rsm + (size_t)warp * tc_rr_warp_bytes(d_pad, cpow);
-    float *qv = reinterpret_cast<float *>(mine);
-    float *rows = qv + d_pad;
-    unsigned long long *keys = reinterpret_cast<unsigned long long *>(
-        mine + (((size_t)d_pad * 4 + 32 * TC_RR_STRIDE * 4 + 15) & ~size_t(15)));
-
-    const int c = count[q];
-    if (lane == 0) atomicAdd(cand_total, (unsigned long long)c);
-    if (c > cmax || c < k) {
-        if (lane == 0) {
-            fail_list[atomicAdd(n_fail, 1)] = q;
-            // too few candidates: the threshold was low; widen it by 8 E.
-            // An overflowing list goes to the exact kernel (NaN).
-            const float T = thr[q];
-            retry[q] = c < k ? T + 8.f * tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T,
-                                                         d_pad)
-                             : __int_as_float(0x7fc00000);
-        }
-        return;
-    }
-    for (int dd = lane; dd < d_pad; dd += 32) qv[dd] = dd < d ? qry[(size_t)dd * ldq + q] : 0.f;
-    __syncwarp();
-    const int *cq = cand + (size_t)q * cmax;
-    for (int g = 0; g * 32 < c; ++g) {
-        const int t = g * 32 + lane;
-        const int my_r = t < c ? cq[t] : -1;
-        float acc = 0.f;
-        for (int ch = 0; ch < d_pad; ch += TC_RR_DCH) {
-            float4 v[16];
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const int r = __shfl_sync(0xffffffffu, my_r, 2 * i + (lane >> 4));
-                v[i] = r >= 0 ? __ldg(reinterpret_cast<const float4 *>(
-                                          refT + (size_t)r * d_pad + ch) +
-                                      (lane & 15))
-                              : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                float *dst = rows + (2 * i + (lane >> 4)) * TC_RR_STRIDE + (lane & 15) * 4;
-                dst[0] = v[i].x;
-                dst[1] = v[i].y;
-                dst[2] = v[i].z;
-                dst[3] = v[i].w;
-            }
-            __syncwarp();
-            const float *myrow = rows + lane * TC_RR_STRIDE;
-#pragma unroll 16
-            for (int dd = 0; dd < TC_RR_DCH; ++dd) {
-                const float t0 = __fsub_rn(myrow[dd], qv[ch + dd]);
-                acc = __fmaf_rn(t0, t0, acc);
-            }
-            __syncwarp();
-        }
-        if (t < c) keys[t] = make_key(acc, (uint32_t)my_r);
-    }
-    int P = 1;
-    while (P < c) P <<= 1;
-    for (int t = c + lane; t < P; t += 32) keys[t] = kKeyInf;
-    __syncwarp();
-    // bitonic sort of keys[0..P), ascending
+// Ascending bitonic sort of keys[0..P) (P a power of two) by one warp.
+KNN_DI void warp_bitonic_sort(unsigned long long *keys, int P, int lane) {
     for (int size = 2; size <= P; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
             for (int t = lane; t < P / 2; t += 32) {
@@ -883,12 +801,179 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
             __syncwarp();
         }
     }
+}
+
+// Exact FP32 re-rank of each query's candidates + certification.
+// One warp per query (TC_RR_WARPS queries per block, no block-wide syncs).
+//
+// Pruning: the candidates are first sorted by their BF16-expansion value a.
+// With a_k the k-th smallest, every candidate i of the first k has exact
+// FP32 distance <= (a_k + ||q||^2 + E)(1 + gamma), and a candidate r has
+// exact FP32 distance >= (a_r + ||q||^2 - E)(1 - gamma) (E as for the
+// threshold, gamma the relative rounding of the FP32 distance chain).  A
+// candidate whose lower bound exceeds that upper bound has k strictly
+// closer candidates and cannot be in the top-k, so only the prefix with
+// a_r <= a_k + 2 E + 2 g (|a_k| + ||q||^2 + E) (g = K 2^-22 >= 4 gamma, which
+// also absorbs the roundings of this bound) is re-ranked; the k-th exact
+// distance of that prefix is the k-th of all candidates.
+//
+// The prefix is handled 32 candidates at a time, one per lane: the warp
+// copies the 32 candidate rows of the FP32 point-major copy, 64 dimensions
+// at a time, into a padded shared tile with asynchronous 16-byte copies
+// (cp.async, two rows per instruction, coalesced), double-buffered so the
+// next chunk is in flight while each lane runs its candidate's FMA chain in
+// increasing d -- the fused exact kernel's arithmetic and order, so
+// distances are identical.  The (distance, index) keys are bitonic-sorted by
+// the warp.
+//
+// An uncertified query is appended to fail_list and retry[q] receives a
+// threshold for a second scan: when it had at least k candidates, their k-th
+// exact distance D_k bounds the true k-th from above, so every point of the
+// true top-k has a < D_k (1+g) + E - ||q||^2 and a second scan emitting below
+// D_k (1+g) + 2.5 E - ||q||^2 passes the check; with fewer than k candidates
+// the threshold is widened by 8 E; an overflowing list gets NaN (no second
+// scan: exact kernel).
+constexpr int TC_RR_WARPS = 4;
+constexpr int TC_RR_DCH = 64;                 // dimensions per staged chunk
+// padded row (floats): 16-byte aligned, and 16-byte reads of one row per lane
+// fall in distinct bank groups for every 8 consecutive lanes
+constexpr int TC_RR_STRIDE = TC_RR_DCH + 4;
+constexpr int TC_RR_BUF = 32 * TC_RR_STRIDE;  // floats per staging buffer
+
+__host__ __device__ inline size_t tc_rr_warp_bytes(int d_pad, int cpow) {
+    return (size_t)d_pad * 4 + 2 * TC_RR_BUF * 4 + (size_t)cpow * 8;
+}
+
+KNN_DI void cp_async16(void *smem_dst, const void *gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)),
+                 "l"(gmem_src)
+                 : "memory");
+}
+KNN_DI void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+KNN_DI void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+__global__ void __launch_bounds__(TC_RR_WARPS * 32)
+    tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
+                     const float *__restrict__ qry, long long ldq, const float *__restrict__ qn,
+                     const unsigned *__restrict__ rmax_bits, const float *__restrict__ thr,
+                     const unsigned long long *__restrict__ cand, const int *__restrict__ count,
+                     int cmax, int cpow, int Q, int k, float *__restrict__ out_dist,
+                     int *__restrict__ out_idx, long long ld_out, int *__restrict__ fail_list,
+                     int *__restrict__ n_fail, float *__restrict__ retry,
+                     unsigned long long *__restrict__ cand_total) {
+    extern __shared__ unsigned char rsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * TC_RR_WARPS + warp;
+    if (q >= Q) return;
+    unsigned char *mine = rsm + (size_t)warp * tc_rr_warp_bytes(d_pad, cpow);
+    float *qv = reinterpret_cast<float *>(mine);
+    float *rows = qv + d_pad;   // two staging buffers
+    unsigned long long *keys = reinterpret_cast<unsigned long long *>(rows + 2 * TC_RR_BUF);
+
+    const int c = count[q];
+    if (lane == 0) atomicAdd(cand_total, (unsigned long long)c);
+    const float qq = qn[q];
+    const float r2 = __uint_as_float(*rmax_bits);
+    const float T = thr[q];
+    if (c > cmax || c < k) {
+        if (lane == 0) {
+            fail_list[atomicAdd(n_fail, 1)] = q;
+            // too few candidates: the threshold was low; widen it by 8 E.
+            // An overflowing list goes to the exact kernel (NaN).
+            retry[q] = c < k ? T + 8.f * tc_error_bound(qq, r2, T, d_pad)
+                             : __int_as_float(0x7fc00000);
+        }
+        return;
+    }
+    // candidates sorted by (a, index)
+    const unsigned long long *cq = cand + (size_t)q * cmax;
+    int P = 32;
+    while (P < c) P <<= 1;
+    for (int t = lane; t < P; t += 32) keys[t] = t < c ? cq[t] : ~0ull;
+    for (int dd = lane; dd < d_pad; dd += 32) qv[dd] = dd < d ? qry[(size_t)dd * ldq + q] : 0.f;
+    __syncwarp();
+    warp_bitonic_sort(keys, P, lane);
+    // the prefix that can still reach the top-k
+    int n_s;
+    {
+        const float ak = ord_float((uint32_t)(keys[k - 1] >> 32));
+        const float E = tc_error_bound(qq, r2, ak, d_pad);
+        const float g = (float)(d_pad + TC_NK) * 2.384185791015625e-07f;
+        const float lim = ak + 2.f * E + 2.f * g * (fabsf(ak) + qq + E);
+        const uint32_t lim_o = ord_bits(__float_as_uint(lim));
+        int cnt = 0;
+        for (int t0 = 0; t0 < c; t0 += 32) {
+            const int t = t0 + lane;
+            const bool in = t < c && (uint32_t)(keys[t] >> 32) <= lim_o;
+            cnt += __popc(__ballot_sync(0xffffffffu, in));
+        }
+        n_s = max(cnt, k);   // keys are sorted, so the kept ones are a prefix
+    }
+    // steps s = (group, chunk); the copy of step s + 1 overlaps step s
+    {
+        const int nch = d_pad / TC_RR_DCH;
+        const int total = ((n_s + 31) / 32) * nch;
+        auto issue = [&](int buf, int rr, int ch) {
+            float *dstb = rows + buf * TC_RR_BUF;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int row = 2 * i + (lane >> 4);
+                const int r = __shfl_sync(0xffffffffu, rr, row);
+                if (r >= 0)
+                    cp_async16(dstb + row * TC_RR_STRIDE + (lane & 15) * 4,
+                               refT + (size_t)r * d_pad + ch + (lane & 15) * 4);
+            }
+        };
+        int r_cur = lane < n_s ? (int)(uint32_t)keys[lane] : -1;
+        int r_nxt = r_cur;
+        issue(0, r_cur, 0);
+        cp_async_commit();
+        float acc = 0.f;
+        for (int s = 0; s < total; ++s) {
+            const int g = s / nch, ch = s - g * nch;
+            if (s + 1 < total) {
+                const int s1 = s + 1, g1 = s1 / nch, ch1 = s1 - g1 * nch;
+                if (ch1 == 0) {
+                    const int t1 = g1 * 32 + lane;
+                    r_nxt = t1 < n_s ? (int)(uint32_t)keys[t1] : -1;
+                }
+                issue(s1 & 1, r_nxt, ch1 * TC_RR_DCH);
+            }
+            cp_async_commit();
+            cp_async_wait_prev();   // step s's copies have landed
+            __syncwarp();
+            const float4 *myrow =
+                reinterpret_cast<const float4 *>(rows + (s & 1) * TC_RR_BUF + lane * TC_RR_STRIDE);
+            const float4 *qc = reinterpret_cast<const float4 *>(qv + ch * TC_RR_DCH);
+#pragma unroll
+            for (int j = 0; j < TC_RR_DCH / 4; ++j) {
+                const float4 rv = myrow[j], qq4 = qc[j];
+                float t0 = __fsub_rn(rv.x, qq4.x);
+                acc = __fmaf_rn(t0, t0, acc);
+                t0 = __fsub_rn(rv.y, qq4.y);
+                acc = __fmaf_rn(t0, t0, acc);
+                t0 = __fsub_rn(rv.z, qq4.z);
+                acc = __fmaf_rn(t0, t0, acc);
+                t0 = __fsub_rn(rv.w, qq4.w);
+                acc = __fmaf_rn(t0, t0, acc);
+            }
+            __syncwarp();   // buffer s & 1 is refilled by step s + 1's prefetch
+            if (ch == nch - 1) {
+                const int t = g * 32 + lane;
+                if (t < n_s) keys[t] = make_key(acc, (uint32_t)r_cur);
+                acc = 0.f;
+                r_cur = r_nxt;
+            }
+        }
+    }
+    int P2 = 32;
+    while (P2 < n_s) P2 <<= 1;
+    for (int t = n_s + lane; t < P2; t += 32) keys[t] = kKeyInf;
+    __syncwarp();
+    warp_bitonic_sort(keys, P2, lane);
     int failed = 0;
     if (lane == 0) {
         const float dk = key_dist2(keys[k - 1]);
-        const float qq = qn[q];
-        const float r2 = __uint_as_float(*rmax_bits);
-        const float T = thr[q];
         const float E = tc_error_bound(qq, r2, T, d_pad);
         const float dkg = dk * (1.f + (float)d_pad * 2.384185791015625e-07f);
         failed = !(dkg + E < T + qq);
@@ -1034,7 +1119,7 @@ size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     const TcPlan p = plan_tc(N, Q, d, k, num_sms);
     size_t b = (size_t)p.qtiles * TC_QT * p.d_pad * 2 + (size_t)Q * 4 * 6 + 16;
     b += (size_t)std::max(p.splits, p.splits1) * Q * TC_KS * 4;
-    b += (size_t)Q * p.cmax * 4;
+    b += (size_t)Q * p.cmax * 8;
     b += fallback_bytes(N, Q, d, k, num_sms);   // worst case: every query uncertified
     return b + 16 * 256;
 }
@@ -1067,7 +1152,8 @@ namespace {
 // (rows Q) and whose thresholds are thr.
 int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cudaStream_t st,
                     const __nv_bfloat16 *qB, int Q, const float *qry, long long ldq,
-                    const float *qn, const float *thr, int *count, int *cand, float *out_dist,
+                    const float *qn, const float *thr, int *count, unsigned long long *cand,
+                    float *out_dist,
                     int *out_idx, long long ld_out, int *fail, int *nfail, float *retry,
                     unsigned long long *cand_total, bool second) {
     const TcPlan pb = plan_tc(P.N, Q, P.d, P.k, P.num_sms);
@@ -1156,7 +1242,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     int *nfail = cv.take<int>(4);
     unsigned long long *cand_total = cv.take<unsigned long long>(1);
     float *p1 = cv.take<float>((size_t)p.splits1 * P.Q * TC_KS);
-    int *cand = cv.take<int>((size_t)P.Q * p.cmax);
+    unsigned long long *cand = cv.take<unsigned long long>((size_t)P.Q * p.cmax);
     const long long ldf = (P.Q + 3) / 4 * 4;       // second-chance buffers, sized for all queries
     float *qsub = cv.take<float>((size_t)P.d * ldf);
     float *sd = cv.take<float>((size_t)P.k * ldf);
