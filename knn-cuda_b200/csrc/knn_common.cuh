@@ -72,30 +72,6 @@ KNN_DI bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// try_wait with acquire at cluster scope: for a barrier that threads of the
-// other CTA of a pair arrive on (release.cluster).
-KNN_DI bool mbar_try_wait_cluster(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-KNN_DI bool mbar_wait_cluster(uint64_t *bar, uint32_t parity) {
-    if (mbar_try_wait_cluster(bar, parity)) return true;
-    const unsigned long long t0 = globaltimer_ns();
-    for (;;) {
-        for (int i = 0; i < 64; ++i)
-            if (mbar_try_wait_cluster(bar, parity)) return true;
-        if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
-    }
-}
-
 // Wait for the phase with the given parity to complete.  Returns false if it
 // did not complete within kWaitLimitNs (the caller records an error and
 // leaves its loop; nothing spins forever).

@@ -303,64 +303,59 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 break;
             }
             tc_fence_after();
-            const int tile = first + j * G;
-            // columns past the end of the set (zero rows from the TMA fill)
-            const int valid = a.N - tile * TC_BN;
-#pragma unroll 1
-            for (int c = 0; c < TC_BN / 32; c += 2) {
-                // two TMEM loads in flight per wait
-                uint32_t v0[32], v1[32];
-                const uint32_t tbase = tmem + ((uint32_t)(qd * 32) << 16) +
-                                       (uint32_t)((b * 2 + h) * TC_BM + c * 32);
-                tmem_ld32(tbase, v0);
-                tmem_ld32(tbase + 32, v1);
-                tmem_ld_wait(v0);
-                tmem_ld_wait(v1);
+            // the warp's 128 columns in one go; the buffer goes back to the
+            // MMA as soon as the values sit in registers
+            uint32_t v[4][32];
+            {
+                const uint32_t tb =
+                    tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)((b * 2 + h) * TC_BM);
 #pragma unroll
-                for (int half = 0; half < 2; ++half) {
-                    uint32_t *v = half ? v1 : v0;
-                    const int cvalid = valid - (c + half) * 32;
-                    if (cvalid < 32) {
+                for (int c = 0; c < 4; ++c) tmem_ld32(tb + 32 * c, v[c]);
 #pragma unroll
-                        for (int e = 0; e < 32; ++e)
-                            if (e >= cvalid) v[e] = 0x7f800000u;   // +inf
-                    }
-                    // one comparison per chunk in the common case
-                    float mn = __uint_as_float(v[0]);
-#pragma unroll
-                    for (int e = 1; e < 32; ++e) mn = fminf(mn, __uint_as_float(v[e]));
-                    const float lim = MODE == 1 ? thr : L[TC_KS - 1];
-                    if (!(mn < lim)) continue;
-                    uint32_t m = 0;
-#pragma unroll
-                    for (int e = 0; e < 32; ++e) m |= (__uint_as_float(v[e]) < lim ? 1u : 0u) << e;
-                    const int cbase = tile * TC_BN + (c + half) * 32;
-                    while (m) {
-                        const int e = __ffs(m) - 1;
-                        m &= m - 1;
-                        uint32_t xb = v[0];
-#pragma unroll
-                        for (int t = 1; t < 32; ++t) xb = (t == e) ? v[t] : xb;
-                        if (MODE == 1) {
-                            const int pos = atomicAdd(&a.count[qrow], 1);
-                            if (pos < a.cmax)
-                                a.cand[(size_t)qrow * a.cmax + pos] =
-                                    ((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e);
-                        } else {
-                            const float x = __uint_as_float(xb);
-                            if (x < L[TC_KS - 1]) {
-#pragma unroll
-                                for (int i = TC_KS - 1; i > 0; --i)
-                                    L[i] = x < L[i - 1] ? L[i - 1] : (x < L[i] ? x : L[i]);
-                                L[0] = fminf(L[0], x);
-                            }
-                        }
-                    }
-                }
+                for (int c = 0; c < 4; ++c) tmem_ld_wait(v[c]);
             }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[b]);
+            const int tile = first + j * G;
+            // columns past the end of the set (zero rows from the TMA fill)
+            const int valid = a.N - tile * TC_BN;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int cvalid = valid - c * 32;
+                if (cvalid < 32) {
+#pragma unroll
+                    for (int e = 0; e < 32; ++e)
+                        if (e >= cvalid) v[c][e] = 0x7f800000u;   // +inf
+                }
+                const float lim = MODE == 1 ? thr : L[TC_KS - 1];
+                if (!(min32(v[c]) < lim)) continue;
+                uint32_t m = 0;
+#pragma unroll
+                for (int e = 0; e < 32; ++e) m |= (__uint_as_float(v[c][e]) < lim ? 1u : 0u) << e;
+                const int cbase = tile * TC_BN + c * 32;
+                while (m) {
+                    const int e = __ffs(m) - 1;
+                    m &= m - 1;
+                    uint32_t xb = v[c][0];
+#pragma unroll
+                    for (int t = 1; t < 32; ++t) xb = (t == e) ? v[c][t] : xb;
+                    if (MODE == 1) {
+                        const int pos = atomicAdd(&a.count[qrow], 1);
+                        if (pos < a.cmax)
+                            a.cand[(size_t)qrow * a.cmax + pos] =
+                                ((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e);
+                    } else {
+                        const float x = __uint_as_float(xb);
+                        if (x < L[TC_KS - 1]) {
+#pragma unroll
+                            for (int i = TC_KS - 1; i > 0; --i)
+                                L[i] = x < L[i - 1] ? L[i - 1] : (x < L[i] ? x : L[i]);
+                            L[0] = fminf(L[0], x);
+                        }
+                    }
+                }
+            }
         }
         if (MODE == 0 && !*abort_flag && qrow < a.Q) {
             float *dst = a.p1 + ((size_t)split * a.Q + qrow) * TC_KS;
@@ -408,13 +403,16 @@ static_assert(TP_SMEM <= 232448, "pair scan kernel shared memory");
 
 struct TpArgs {
     int N, Q, kb_count, n_tiles, n_splits;   // n_tiles: 256-point tiles
-    const float *thr;       // [Q] thresholds (a units)
+    int tile_stride;        // scan tiles t of the split with t % tile_stride == 0
+    const float *thr;       // emit pass: [Q] thresholds (a units)
+    float *p1;              // sample pass: [2 n_splits][Q][TC_KS] (per column half)
     unsigned long long *cand;   // [Q][cmax] (a, index) entries
     int *count;             // [Q]
     int cmax;
     int *status;
 };
 
+template <int MODE>   // 0: threshold sample pass, 1: emit pass
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
     knn_tc_pair_scan_kernel(const __grid_constant__ CUtensorMap tmA,
                             const __grid_constant__ CUtensorMap tmB,
@@ -445,7 +443,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
     const int KB = a.kb_count;
     const int t0 = (int)((long long)a.n_tiles * split / a.n_splits);
     const int t1 = (int)((long long)a.n_tiles * (split + 1) / a.n_splits);
-    const int n_my = t1 - t0;
+    const int G = a.tile_stride;
+    const int first = ((t0 + G - 1) / G) * G;
+    const int n_my = first < t1 ? (t1 - first + G - 1) / G : 0;
 
     for (int i = threadIdx.x; i < TC_BM * TC_NK / 2; i += TC_THREADS)
         reinterpret_cast<uint32_t *>(sOnes)[i] = 0x3F803F80u;
@@ -496,7 +496,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
                 a_issued = true;
             }
             for (int j = 0; j < n_my && ok; ++j) {
-                const int row0 = (t0 + j) * TP_BN + half_row;
+                const int row0 = (first + j * G) * TP_BN + half_row;
                 const int ns = j % TP_NSLOTS;
                 if (j >= TP_NSLOTS && !mbar_wait(&n_empty[ns], ((j / TP_NSLOTS) - 1) & 1)) {
                     ok = false;
@@ -517,8 +517,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
                     if (lead) mbar_arrive_expect_tx(&b_full[s], 2 * TC_TILE_BYTES);
                     tma_load_2d_pair(sB + (size_t)s * TC_TILE_BYTES, &tmB,
                                      mapa_shared(smem_u32(&b_full[s]), 0), kb * TC_BK, row0);
-                    if (j + 2 < n_my && row0 + 2 * TP_BN < a.N)
-                        tma_prefetch_l2_2d(&tmB, kb * TC_BK, row0 + 2 * TP_BN);
+                    if (j + 2 < n_my && row0 + 2 * G * TP_BN < a.N)
+                        tma_prefetch_l2_2d(&tmB, kb * TC_BK, row0 + 2 * G * TP_BN);
                     issued = it + 1;
                 }
                 if (*abort_flag) break;
@@ -551,7 +551,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
             const uint64_t odesc = umma_desc_sw32(sOnes);
             for (int j = 0; j < n_my && ok; ++j) {
                 const int b = j & 1;
-                if (j >= 2 && !mbar_wait_cluster(&acc_empty[b], ((j >> 1) - 1) & 1)) {
+                if (j >= 2 && !mbar_wait(&acc_empty[b], ((j >> 1) - 1) & 1)) {
                     ok = false;
                     break;
                 }
@@ -600,7 +600,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
         const int qd = warp & 3;
         const int hc = (warp - 2) >> 2;
         const int qrow = qpair * TC_QT + (int)rank * TC_BM + qd * 32 + lane;
-        const float thr = qrow < a.Q ? a.thr[qrow] : -INFINITY;
+        float thr = -INFINITY;
+        if (MODE == 1 && qrow < a.Q) thr = a.thr[qrow];
+        float L[TC_KS];
+#pragma unroll
+        for (int i = 0; i < TC_KS; ++i) L[i] = INFINITY;
         for (int j = 0; j < n_my; ++j) {
             const int b = j & 1;
             const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
@@ -612,46 +616,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
                 break;
             }
             tc_fence_after();
-            const int col0 = (t0 + j) * TP_BN + hc * 128;   // first reference of this warp
-            const int valid = a.N - col0;
-#pragma unroll 1
-            for (int c = 0; c < 4; c += 2) {
-                uint32_t v0[32], v1[32];
-                const uint32_t tbase = tmem + ((uint32_t)(qd * 32) << 16) +
-                                       (uint32_t)(b * TP_BN + hc * 128 + c * 32);
-                tmem_ld32(tbase, v0);
-                tmem_ld32(tbase + 32, v1);
-                tmem_ld_wait(v0);
-                tmem_ld_wait(v1);
+            // the warp's 128 columns in one go; the buffer goes back to the
+            // MMA as soon as the values sit in registers
+            uint32_t v[4][32];
+            {
+                const uint32_t tb =
+                    tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * TP_BN + hc * 128);
 #pragma unroll
-                for (int half = 0; half < 2; ++half) {
-                    uint32_t *v = half ? v1 : v0;
-                    const int cvalid = valid - (c + half) * 32;
-                    if (cvalid < 32) {
+                for (int c = 0; c < 4; ++c) tmem_ld32(tb + 32 * c, v[c]);
 #pragma unroll
-                        for (int e = 0; e < 32; ++e)
-                            if (e >= cvalid) v[e] = 0x7f800000u;   // +inf
-                    }
-                    float mn = __uint_as_float(v[0]);
-#pragma unroll
-                    for (int e = 1; e < 32; ++e) mn = fminf(mn, __uint_as_float(v[e]));
-                    if (!(mn < thr)) continue;
-                    uint32_t m = 0;
-#pragma unroll
-                    for (int e = 0; e < 32; ++e) m |= (__uint_as_float(v[e]) < thr ? 1u : 0u) << e;
-                    const int cbase = col0 + (c + half) * 32;
-                    while (m) {
-                        const int e = __ffs(m) - 1;
-                        m &= m - 1;
-                        uint32_t xb = v[0];
-#pragma unroll
-                        for (int t = 1; t < 32; ++t) xb = (t == e) ? v[t] : xb;
-                        const int pos = atomicAdd(&a.count[qrow], 1);
-                        if (pos < a.cmax)
-                            a.cand[(size_t)qrow * a.cmax + pos] =
-                                ((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e);
-                    }
-                }
+                for (int c = 0; c < 4; ++c) tmem_ld_wait(v[c]);
             }
             tc_fence_before();
             __syncwarp();
@@ -661,6 +635,49 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
                 else
                     mbar_arrive_cluster(mapa_shared(smem_u32(&acc_empty[b]), 0));
             }
+            const int col0 = (first + j * G) * TP_BN + hc * 128;   // first reference of this warp
+            const int valid = a.N - col0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int cvalid = valid - c * 32;
+                if (cvalid < 32) {
+#pragma unroll
+                    for (int e = 0; e < 32; ++e)
+                        if (e >= cvalid) v[c][e] = 0x7f800000u;   // +inf
+                }
+                const float lim = MODE == 1 ? thr : L[TC_KS - 1];
+                if (!(min32(v[c]) < lim)) continue;
+                uint32_t m = 0;
+#pragma unroll
+                for (int e = 0; e < 32; ++e) m |= (__uint_as_float(v[c][e]) < lim ? 1u : 0u) << e;
+                const int cbase = col0 + c * 32;
+                while (m) {
+                    const int e = __ffs(m) - 1;
+                    m &= m - 1;
+                    uint32_t xb = v[c][0];
+#pragma unroll
+                    for (int t = 1; t < 32; ++t) xb = (t == e) ? v[c][t] : xb;
+                    if (MODE == 1) {
+                        const int pos = atomicAdd(&a.count[qrow], 1);
+                        if (pos < a.cmax)
+                            a.cand[(size_t)qrow * a.cmax + pos] =
+                                ((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e);
+                    } else {
+                        const float x = __uint_as_float(xb);
+                        if (x < L[TC_KS - 1]) {
+#pragma unroll
+                            for (int i = TC_KS - 1; i > 0; --i)
+                                L[i] = x < L[i - 1] ? L[i - 1] : (x < L[i] ? x : L[i]);
+                            L[0] = fminf(L[0], x);
+                        }
+                    }
+                }
+            }
+        }
+        if (MODE == 0 && !*abort_flag && qrow < a.Q) {
+            float *dst = a.p1 + ((size_t)(2 * split + hc) * a.Q + qrow) * TC_KS;
+#pragma unroll
+            for (int i = 0; i < TC_KS; ++i) dst[i] = L[i];
         }
     }
 
@@ -684,15 +701,37 @@ KNN_DI float tc_error_bound(float qq, float r2, float T, int d_pad) {
 // prep kernels
 // ---------------------------------------------------------------------------
 
-// Squared norm of each point of a dim x n set (sequential FP32 fma over d):
-// as FP32 (nrm) and/or as the norm-step row of the tensor scan (parts: h, m,
-// l = successive BF16 roundings of the remainder, so h + m + l equals the
-// norm to 2^-27 relative; each subtraction is exact by Sterbenz' lemma;
-// 13 zeros), and the largest squared norm (non-negative float bits compare
+// The norm-step row of point p: h, m, l = successive BF16 roundings of the
+// remainder of the squared norm s (each subtraction is exact by Sterbenz'
+// lemma, and h + m + l equals s to 2^-27 relative), then 13 zeros.
+KNN_DI void write_norm_row(__nv_bfloat16 *parts, int p, float s) {
+    __nv_bfloat16 hml[3];
+    if (isfinite(s)) {
+        float rem = s;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            hml[i] = __float2bfloat16_rn(rem);
+            rem = rem - __bfloat162float(hml[i]);
+        }
+    } else {
+        hml[0] = __float2bfloat16_rn(INFINITY);
+        hml[1] = hml[2] = __float2bfloat16_rn(0.f);
+    }
+    uint4 row[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+    __nv_bfloat16 *e = reinterpret_cast<__nv_bfloat16 *>(row);
+    e[0] = hml[0];
+    e[1] = hml[1];
+    e[2] = hml[2];
+    uint4 *dst = reinterpret_cast<uint4 *>(parts + (size_t)p * TC_NK);
+    dst[0] = row[0];
+    dst[1] = row[1];
+}
+
+// Squared norm of each point of a dim x n set (sequential FP32 fma over d)
+// and optionally the largest squared norm (non-negative float bits compare
 // as unsigned).
 __global__ void tc_norms_kernel(const float *__restrict__ x, int n, long long ld, int d,
-                                float *__restrict__ nrm, __nv_bfloat16 *__restrict__ parts,
-                                unsigned *__restrict__ max_bits) {
+                                float *__restrict__ nrm, unsigned *__restrict__ max_bits) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     float s = 0.f;
     if (p < n) {
@@ -700,29 +739,7 @@ __global__ void tc_norms_kernel(const float *__restrict__ x, int n, long long ld
             const float v = x[(size_t)dd * ld + p];
             s = fmaf(v, v, s);
         }
-        if (nrm) nrm[p] = s;
-        if (parts) {
-            __nv_bfloat16 hml[3];
-            if (isfinite(s)) {
-                float rem = s;
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    hml[i] = __float2bfloat16_rn(rem);
-                    rem = rem - __bfloat162float(hml[i]);
-                }
-            } else {
-                hml[0] = __float2bfloat16_rn(INFINITY);
-                hml[1] = hml[2] = __float2bfloat16_rn(0.f);
-            }
-            uint4 row[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
-            __nv_bfloat16 *e = reinterpret_cast<__nv_bfloat16 *>(row);
-            e[0] = hml[0];
-            e[1] = hml[1];
-            e[2] = hml[2];
-            uint4 *dst = reinterpret_cast<uint4 *>(parts + (size_t)p * TC_NK);
-            dst[0] = row[0];
-            dst[1] = row[1];
-        }
+        nrm[p] = s;
     }
     unsigned m = __float_as_uint(s);
 #pragma unroll
@@ -753,6 +770,52 @@ __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld,
             xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(v * scale);
             if (xt) xt[(size_t)p * d_pad + dd] = v;
         }
+    }
+}
+
+// Reference-set prep in one pass over the input: point-major BF16 and FP32
+// copies (zero-padded to d_pad) plus the norm-step row and the largest
+// squared norm.  A block owns 32 points and walks the dimensions in 32 x 32
+// tiles through shared memory (coalesced on both sides); one thread per
+// point accumulates the squared norm in increasing d with FP32 fma, the
+// order tc_norms_kernel uses.
+__global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long ld, int d,
+                                   int d_pad, __nv_bfloat16 *__restrict__ xb,
+                                   float *__restrict__ xt, __nv_bfloat16 *__restrict__ parts,
+                                   unsigned *__restrict__ max_bits) {
+    __shared__ float tile[32][33];
+    const int p0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    float s = 0.f;
+    for (int d0 = 0; d0 < d_pad; d0 += 32) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int dd = d0 + ty + 8 * i, p = p0 + tx;
+            tile[ty + 8 * i][tx] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
+        }
+        __syncthreads();
+        if (ty == 0) {
+            const int dm = min(32, d - d0);
+            for (int dd = 0; dd < dm; ++dd) s = fmaf(tile[dd][tx], tile[dd][tx], s);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int p = p0 + ty + 8 * i, dd = d0 + tx;
+            if (p < n) {
+                const float v = tile[tx][ty + 8 * i];
+                xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(v);
+                xt[(size_t)p * d_pad + dd] = v;
+            }
+        }
+        __syncthreads();
+    }
+    if (ty == 0) {
+        const int p = p0 + tx;
+        if (p < n) write_norm_row(parts, p, s);
+        unsigned m = p < n ? __float_as_uint(s) : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (tx == 0) atomicMax(max_bits, m);
     }
 }
 
@@ -1076,13 +1139,14 @@ TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
     p.splits = choose_splits(p.qtiles, p.n_tiles, 16, 2.0, num_sms);
     // the sample must hold about 2.5k points below T_q: KS * stride >= 2.5k
     p.stride1 = std::max(16, (5 * k + 2 * TC_KS - 1) / (2 * TC_KS));
-    // pass 1 scans 1/stride1 of the tiles: coarser splits amortise each
-    // CTA's set-up (query tile load, TMEM allocation, pipeline fill)
-    p.splits1 = choose_splits(p.qtiles, (p.n_tiles + p.stride1 - 1) / p.stride1, 32, 8.0,
-                              num_sms);
     p.cmax = 4 * TC_KS * p.stride1;
     p.n_tiles2 = (N + TP_BN - 1) / TP_BN;
     p.splits2 = choose_splits(p.qtiles, p.n_tiles2, 8, 2.0, std::max(1, num_sms / 2));
+    // pass 1 (CTA pairs) scans every stride1-th 256-point tile; coarser
+    // splits amortise each pair's set-up (query tile load, TMEM allocation,
+    // pipeline fill)
+    p.splits1 = choose_splits(p.qtiles, (p.n_tiles2 + p.stride1 - 1) / p.stride1, 16, 8.0,
+                              std::max(1, num_sms / 2));
     return p;
 }
 
@@ -1118,7 +1182,7 @@ static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
 size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     const TcPlan p = plan_tc(N, Q, d, k, num_sms);
     size_t b = (size_t)p.qtiles * TC_QT * p.d_pad * 2 + (size_t)Q * 4 * 6 + 16;
-    b += (size_t)std::max(p.splits, p.splits1) * Q * TC_KS * 4;
+    b += (size_t)2 * p.splits1 * Q * TC_KS * 4;
     b += (size_t)Q * p.cmax * 8;
     b += fallback_bytes(N, Q, d, k, num_sms);   // worst case: every query uncertified
     return b + 16 * 256;
@@ -1128,10 +1192,8 @@ int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, i
                    cudaStream_t st) {
     const int d_pad = (d + 63) / 64 * 64;
     if (cudaMemsetAsync(v.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess) return kErrCuda;
-    tc_norms_kernel<<<(N + 255) / 256, 256, 0, st>>>(ref, N, ldr, d, nullptr, v.refN,
-                                                     v.rmax_bits);
-    dim3 g((N + 31) / 32, d_pad / 32);
-    tc_pack_kernel<<<g, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, 1.0f, v.refB, v.refT);
+    tc_prep_ref_kernel<<<(N + 31) / 32, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, v.refB,
+                                                              v.refT, v.refN, v.rmax_bits);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
@@ -1169,12 +1231,14 @@ int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cud
         a.kb_count = p.kb;
         a.n_tiles = pb.n_tiles2;
         a.n_splits = pb.splits2;
+        a.tile_stride = 1;
         a.thr = thr;
+        a.p1 = nullptr;
         a.cand = cand;
         a.count = count;
         a.cmax = p.cmax;
         a.status = P.status;
-        knn_tc_pair_scan_kernel<<<dim3(2 * pb.qtiles, pb.splits2), TC_THREADS, TP_SMEM, st>>>(
+        knn_tc_pair_scan_kernel<1><<<dim3(2 * pb.qtiles, pb.splits2), TC_THREADS, TP_SMEM, st>>>(
             tmA, tmB, tmN, a);
     } else {
         TcArgs a;
@@ -1241,7 +1305,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     int *fail2 = cv.take<int>(P.Q);
     int *nfail = cv.take<int>(4);
     unsigned long long *cand_total = cv.take<unsigned long long>(1);
-    float *p1 = cv.take<float>((size_t)p.splits1 * P.Q * TC_KS);
+    float *p1 = cv.take<float>((size_t)2 * p.splits1 * P.Q * TC_KS);
     unsigned long long *cand = cv.take<unsigned long long>((size_t)P.Q * p.cmax);
     const long long ldf = (P.Q + 3) / 4 * 4;       // second-chance buffers, sized for all queries
     float *qsub = cv.take<float>((size_t)P.d * ldf);
@@ -1253,17 +1317,17 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     PhaseTimer *tm = P.timer;
 
     // queries: norms + BF16 K-major copy of -2 q
-    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, qn, nullptr,
-                                                       nullptr);
+    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, qn, nullptr);
     tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
         P.qry, P.Q, P.ldq, P.d, p.d_pad, -2.0f, qB, nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (tm) tm->mark(st, kPhaseTcPrepQuery);
-    if (cudaFuncSetAttribute(knn_tc_scan_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(knn_tc_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TC_SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(knn_tc_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TC_SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(knn_tc_pair_scan_kernel,
+        cudaFuncSetAttribute(knn_tc_pair_scan_kernel<0>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TP_SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(knn_tc_pair_scan_kernel<1>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TP_SMEM) != cudaSuccess)
         return kErrLaunch;
@@ -1274,23 +1338,25 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
         if (!encode_bf16_kmajor(&tmA, qB, P.Q, p.d_pad)) return kErrTensorMap;
         if (!encode_bf16_kmajor(&tmB, R.refB, P.N, p.d_pad)) return kErrTensorMap;
         if (!encode_norm_rows(&tmN, R.refN, P.N)) return kErrTensorMap;
-        TcArgs a;
+        TpArgs a;
         a.N = P.N;
         a.Q = P.Q;
         a.kb_count = p.kb;
-        a.n_tiles = p.n_tiles;
+        a.n_tiles = p.n_tiles2;
         a.n_splits = p.splits1;
         a.tile_stride = p.stride1;
-        a.thr = thr;
+        a.thr = nullptr;
         a.p1 = p1;
         a.cand = cand;
         a.count = count;
         a.cmax = p.cmax;
         a.status = P.status;
-        knn_tc_scan_kernel<0><<<dim3(p.qtiles, p.splits1), TC_THREADS, TC_SMEM, st>>>(tmA, tmB,
-                                                                                      tmN, a);
+        knn_tc_pair_scan_kernel<0><<<dim3(2 * p.qtiles, p.splits1), TC_THREADS, TP_SMEM, st>>>(
+            tmA, tmB, tmN, a);
+        if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
         if (tm) tm->mark(st, kPhaseTcPass1);
-        tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, p.splits1, P.Q, qn,
+        // two lists (column halves) per pair and split
+        tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, 2 * p.splits1, P.Q, qn,
                                                                R.rmax_bits, p.d_pad, thr, count);
         if (tm) tm->mark(st, kPhaseTcThreshold);
     }
@@ -1313,7 +1379,7 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
     // thresholds that certify (list overflows excepted)
     gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, fail,
                                                                        nf, qsub, ldf);
-    tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(qsub, nf, ldf, P.d, qn, nullptr, nullptr);
+    tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(qsub, nf, ldf, P.d, qn, nullptr);
     tc_pack_kernel<<<dim3((nf + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
         qsub, nf, ldf, P.d, p.d_pad, -2.0f, qB, nullptr);
     tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(fail, nf, retry, thr, count);

@@ -110,11 +110,10 @@ KNN_DI void cluster_sync() {
                      : "memory");
 }
 // Arrive on an mbarrier of another CTA of the cluster (shared::cluster
-// address), releasing this thread's prior writes / TMEM reads at cluster
-// scope.
+// address).  Used after tcgen05.wait::ld + tcgen05.fence::before_thread_sync:
+// the TMEM data already sits in registers when the arrive executes.
 KNN_DI void mbar_arrive_cluster(uint32_t cluster_addr) {
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
-                 : "memory");
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
 }
 // TMA 2-D load into this CTA's shared memory whose completion is counted on
 // an mbarrier of either CTA of the pair (shared::cluster address).
@@ -193,6 +192,28 @@ KNN_DI void tmem_ld_wait(uint32_t (&v)[32]) {
                    "+r"(v[30]), "+r"(v[31])
                  :
                  : "memory");
+}
+
+// Three-input minimum (sm_100): min of a, b, c; a NaN operand is ignored
+// like fminf.
+KNN_DI float min3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// Smallest of 32 accumulator values (FP32 bit patterns): a depth-4 tree
+// of 17 min instructions.
+KNN_DI float min32(const uint32_t (&v)[32]) {
+    float m[11];
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+        m[i] = min3f(__uint_as_float(v[3 * i]), __uint_as_float(v[3 * i + 1]),
+                     __uint_as_float(v[3 * i + 2]));
+    m[10] = fminf(__uint_as_float(v[30]), __uint_as_float(v[31]));
+    const float n0 = min3f(m[0], m[1], m[2]), n1 = min3f(m[3], m[4], m[5]);
+    const float n2 = min3f(m[6], m[7], m[8]), n3 = fminf(m[9], m[10]);
+    return fminf(min3f(n0, n1, n2), n3);
 }
 
 }  // namespace knnb200
