@@ -85,6 +85,12 @@ struct Buffer {
     }
 };
 
+// Host entry of knn_cublas on large sets: the reference set is copied in
+// this many chunks (after a strided sample for the threshold pass), each
+// chunk's prep and scan overlapping the copy of the next.
+constexpr int kStreamChunks = 8;
+constexpr int kStreamMinPoints = 1 << 18;
+
 struct Workspace {
     std::mutex mu;
     bool init = false;
@@ -97,6 +103,8 @@ struct Workspace {
     PhaseTimer timer;                  // optional per-phase device timing
     int *status_host = nullptr;        // pinned status word for the host path
     int *tc_stats = nullptr;           // pinned: [0] second-scan queries, [1] exact fallbacks
+    cudaStream_t copy_stream = nullptr;          // host entry: reference copies
+    cudaEvent_t copied[1 + kStreamChunks] = {};  // sample, then each chunk
 
     bool setup(int dev) {
         if (init) return true;
@@ -113,6 +121,10 @@ struct Workspace {
             return false;
         for (int i = 0; i < PhaseTimer::kMaxMarks; ++i)
             if (cudaEventCreate(&timer.ev[i]) != cudaSuccess) return false;
+        if (cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+            return false;
+        for (cudaEvent_t &e : copied)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
         init = true;
         return true;
     }
@@ -169,6 +181,108 @@ int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st) 
     t.num_sms = p.num_sms;
     t.timer = &ws.timer;
     return launch_tc(t, rv, st, ws.tc_stats);
+}
+
+// knn_cublas from pinned host memory: the reference set streams in on the
+// copy stream -- first every sample-stride-th 256-point tile (pass 1 needs
+// only those), then kStreamChunks contiguous chunks -- and the compute
+// stream prepares and scans each piece once its copy has landed, so the
+// copy of the set overlaps the threshold pass and the pass-2 scan of all
+// but the last chunk.  Sample tiles are copied twice (once in the sample,
+// once in their chunk); the second copy writes the same bytes.
+int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_host,
+                        cudaStream_t st) {
+    for (int i = 0; i < 8; ++i) ws.tc_stats[i] = 0;
+    ws.timer.begin(st);
+    if (!ws.tcref.ensure(tc_ref_bytes(p.N, p.d))) return kErrNoMemory;
+    const TcRefView rv = tc_carve_ref(ws.tcref.ptr, p.N, p.d);
+    float *ref_d = const_cast<float *>(p.ref);
+    const int T = tc_tile_points();
+    const int n_tiles = (p.N + T - 1) / T;
+    const int G = tc_sample_stride(p.N, p.Q, p.d, p.k, p.num_sms);
+    const size_t fb = sizeof(float);
+    cudaStream_t cs = ws.copy_stream;
+    // the copies start after everything queued so far on the compute stream
+    // (an earlier call may still read the reference buffer)
+    if (cudaEventRecord(ws.last_done, st) != cudaSuccess ||
+        cudaStreamWaitEvent(cs, ws.last_done, 0) != cudaSuccess)
+        return kErrCuda;
+    // sample tiles 0, G, 2G, ...: whole tiles by one 2-D copy per dimension,
+    // a ragged last tile separately
+    const int n_sample = (n_tiles + G - 1) / G;
+    const int last = (n_sample - 1) * G;
+    const bool ragged = (long long)(last + 1) * T > p.N;
+    const int n_whole = ragged ? n_sample - 1 : n_sample;
+    for (int dd = 0; dd < p.d; ++dd) {
+        float *dst = ref_d + (size_t)dd * p.ldr;
+        const float *src = ref_host + (size_t)dd * p.N;
+        if (n_whole > 0 &&
+            cudaMemcpy2DAsync(dst, (size_t)G * T * fb, src, (size_t)G * T * fb, (size_t)T * fb,
+                              n_whole, cudaMemcpyHostToDevice, cs) != cudaSuccess)
+            return kErrCuda;
+        if (ragged && cudaMemcpyAsync(dst + (size_t)last * T, src + (size_t)last * T,
+                                      ((size_t)p.N - (size_t)last * T) * fb,
+                                      cudaMemcpyHostToDevice, cs) != cudaSuccess)
+            return kErrCuda;
+    }
+    if (cudaEventRecord(ws.copied[0], cs) != cudaSuccess) return kErrCuda;
+    const int per_chunk = (n_tiles + kStreamChunks - 1) / kStreamChunks;
+    for (int c = 0; c < kStreamChunks; ++c) {
+        const long long p0 = (long long)c * per_chunk * T;
+        const long long p1 = std::min<long long>(p.N, (long long)(c + 1) * per_chunk * T);
+        if (p0 < p1 && cudaMemcpy2DAsync(ref_d + p0, (size_t)p.ldr * fb, ref_host + p0,
+                                         (size_t)p.N * fb, (size_t)(p1 - p0) * fb, p.d,
+                                         cudaMemcpyHostToDevice, cs) != cudaSuccess)
+            return kErrCuda;
+        if (cudaEventRecord(ws.copied[1 + c], cs) != cudaSuccess) return kErrCuda;
+    }
+
+    TcProblem t;
+    t.ref = p.ref;
+    t.N = p.N;
+    t.ldr = p.ldr;
+    t.qry = p.qry;
+    t.Q = p.Q;
+    t.ldq = p.ldq;
+    t.d = p.d;
+    t.k = p.k;
+    t.out_dist = p.out_dist;
+    t.out_idx = p.out_idx;
+    t.ld_out = p.ld_out;
+    t.scratch = p.scratch;
+    t.scratch_bytes = p.scratch_bytes;
+    t.status = p.status;
+    t.num_sms = p.num_sms;
+    t.timer = nullptr;
+    TcRun run;
+    int rc = tc_run_begin(t, rv, st, run);
+    if (rc != kOk) return rc;
+    if (cudaStreamWaitEvent(st, ws.copied[0], 0) != cudaSuccess ||
+        cudaMemsetAsync(rv.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess)
+        return kErrCuda;
+    if ((rc = tc_prepare_ref_tiles(rv, p.ref, p.N, p.ldr, p.d, 0, n_sample, G, st)) != kOk ||
+        (rc = tc_run_pass1(run, st)) != kOk)
+        return rc;
+    for (int c = 0; c < kStreamChunks; ++c) {
+        const int tb = c * per_chunk, te = std::min(n_tiles, (c + 1) * per_chunk);
+        if (cudaStreamWaitEvent(st, ws.copied[1 + c], 0) != cudaSuccess) return kErrCuda;
+        if (tb >= te) continue;
+        if ((rc = tc_prepare_ref_tiles(rv, p.ref, p.N, p.ldr, p.d, tb, te - tb, 1, st)) != kOk ||
+            (rc = tc_run_pass2(run, tb, te, st)) != kOk)
+            return rc;
+    }
+    return tc_run_finish(run, st, ws.tc_stats);
+}
+
+// Page-locked (or registered) host memory: only then do the copies run
+// asynchronously and overlap the scans.
+bool host_pinned(const void *ptr) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
 }
 
 int current_workspace(Workspace *&ws) {
@@ -240,8 +354,12 @@ bool host_entry(int method, const float *ref, int ref_nb, const float *query, in
     cudaStream_t st = ws->stream;
     float *ref_d = static_cast<float *>(ws->ref.ptr);
     float *qry_d = static_cast<float *>(ws->qry.ptr);
-    cudaError_t e0 = cudaMemcpy2DAsync(ref_d, ldr * sizeof(float), ref, ref_nb * sizeof(float),
-                                       ref_nb * sizeof(float), dim, cudaMemcpyHostToDevice, st);
+    const bool streamed = use_tc(method, ref_nb, query_nb, dim, k) &&
+                          ref_nb >= kStreamMinPoints && host_pinned(ref);
+    cudaError_t e0 = streamed ? cudaSuccess
+                              : cudaMemcpy2DAsync(ref_d, ldr * sizeof(float), ref,
+                                                  ref_nb * sizeof(float), ref_nb * sizeof(float),
+                                                  dim, cudaMemcpyHostToDevice, st);
     cudaError_t e1 = cudaMemcpy2DAsync(qry_d, ldq * sizeof(float), query,
                                        query_nb * sizeof(float), query_nb * sizeof(float), dim,
                                        cudaMemcpyHostToDevice, st);
@@ -268,7 +386,7 @@ bool host_entry(int method, const float *ref, int ref_nb, const float *query, in
     p.status = static_cast<int *>(ws->status.ptr);
     p.num_sms = ws->num_sms;
     p.force_splits = 0;
-    rc = enqueue(*ws, p, method, st);
+    rc = streamed ? enqueue_tc_streamed(*ws, p, ref, st) : enqueue(*ws, p, method, st);
     if (rc != kOk) {
         std::printf("ERROR: Unable to execute kernel (%s)\n", knnb200_status_string(rc));
         cudaGetLastError();

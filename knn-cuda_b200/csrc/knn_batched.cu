@@ -198,9 +198,7 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
         const BatchProb P = probs[inf.p];
         for (int i = lane; i < QPW * C::REGION; i += 32) wl[i] = kKeyInf;
         __syncwarp();
-        unsigned long long tau[QPW];
-#pragma unroll
-        for (int i = 0; i < QPW; ++i) tau[i] = kKeyInf;
+        uint32_t nb = 0;   // candidate buffer fills
         const int t0 = (int)((long long)P.n_rtiles * inf.split / P.n_splits);
         const int t1 = (int)((long long)P.n_rtiles * (inf.split + 1) / P.n_splits);
         bool alive = true;
@@ -211,8 +209,9 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
                 alive = false;
                 break;
             }
-            select_tile<QPW, KCAP>(wl, tau, acc, rt, P.N, P.k, lane);
+            select_tile<QPW, KCAP>(wl, nb, acc, rt, P.N, P.k, lane);
         }
+        flush_all<QPW, KCAP>(wl, nb, P.k, lane);
         consumer_sync();
         if (!alive || *abort_flag) break;
         const int q0 = inf.qtile * C::BQ;
@@ -365,7 +364,7 @@ int knnb200_batched_plan_create(const knnb200_problem *in, int count, int item_s
     int kmax = 1;
     for (int i = 0; i < count; ++i) kmax = std::max(kmax, in[i].k);
     pl->kcap = kmax <= 32 ? 32 : kmax <= 64 ? 64 : kmax <= 128 ? 128 : 256;
-    pl->qpw = pl->kcap == 256 ? 2 : 4;
+    pl->qpw = pl->kcap == 256 ? EX_QPW_K256 : EX_QPW;
     const int bq = pl->qpw * EX_WARPS;
 
     // records, cut into items of about `item_stages` pipeline stages
@@ -484,10 +483,10 @@ int knnb200_batched_run(knnb200_batched_plan *pl, void *stream) {
     if (cudaGetLastError() != cudaSuccess) return KNNB200_ELAUNCH;
     cudaError_t e;
     switch (pl->kcap) {
-        case 32: e = launch_batched_t<4, 32>(pl, st); break;
-        case 64: e = launch_batched_t<4, 64>(pl, st); break;
-        case 128: e = launch_batched_t<4, 128>(pl, st); break;
-        default: e = launch_batched_t<2, 256>(pl, st); break;
+        case 32: e = launch_batched_t<EX_QPW, 32>(pl, st); break;
+        case 64: e = launch_batched_t<EX_QPW, 64>(pl, st); break;
+        case 128: e = launch_batched_t<EX_QPW, 128>(pl, st); break;
+        default: e = launch_batched_t<EX_QPW_K256, 256>(pl, st); break;
     }
     if (e != cudaSuccess) return KNNB200_ELAUNCH;
     if (pl->n_tasks > 0) {

@@ -98,9 +98,7 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
     unsigned long long *wl = lists + (size_t)warp * QPW * C::REGION;
     for (int i = lane; i < QPW * C::REGION; i += 32) wl[i] = kKeyInf;
     __syncwarp();
-    unsigned long long tau[QPW];
-#pragma unroll
-    for (int i = 0; i < QPW; ++i) tau[i] = kKeyInf;
+    uint32_t nb = 0;   // candidate buffer fills
 
     int it = 0;
     for (int rt = t0; rt < t1; ++rt) {
@@ -108,8 +106,9 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
         if (!consume_ref_tile<QPW, KCAP>(acc, stages, full, empty, abort_flag, it, a.n_dchunks,
                                          warp, lane, a.status))
             break;
-        select_tile<QPW, KCAP>(wl, tau, acc, rt, a.N, a.k, lane);
+        select_tile<QPW, KCAP>(wl, nb, acc, rt, a.N, a.k, lane);
     }
+    flush_all<QPW, KCAP>(wl, nb, a.k, lane);
 
     consumer_sync();
     if (*abort_flag) return;
@@ -200,10 +199,10 @@ void shape_of(ExactShape &s) {
 }
 
 bool choose_shape(int N, int Q, int d, int k, int num_sms, ExactShape &s) {
-    if (k <= 32) shape_of<4, 32>(s);
-    else if (k <= 64) shape_of<4, 64>(s);
-    else if (k <= 128) shape_of<4, 128>(s);
-    else if (k <= 256) shape_of<2, 256>(s);
+    if (k <= 32) shape_of<EX_QPW, 32>(s);
+    else if (k <= 64) shape_of<EX_QPW, 64>(s);
+    else if (k <= 128) shape_of<EX_QPW, 128>(s);
+    else if (k <= 256) shape_of<EX_QPW_K256, 256>(s);
     else return false;
     s.n_rtiles = (N + EX_BR - 1) / EX_BR;
     s.n_dchunks = (d + EX_BD - 1) / EX_BD;
@@ -318,10 +317,10 @@ int launch_exact(const ExactProblem &p, cudaStream_t st) {
 
     cudaError_t e;
     switch (s.kcap) {
-        case 32: e = launch_t<4, 32>(mr, mq, a, qtiles, st); break;
-        case 64: e = launch_t<4, 64>(mr, mq, a, qtiles, st); break;
-        case 128: e = launch_t<4, 128>(mr, mq, a, qtiles, st); break;
-        default: e = launch_t<2, 256>(mr, mq, a, qtiles, st); break;
+        case 32: e = launch_t<EX_QPW, 32>(mr, mq, a, qtiles, st); break;
+        case 64: e = launch_t<EX_QPW, 64>(mr, mq, a, qtiles, st); break;
+        case 128: e = launch_t<EX_QPW, 128>(mr, mq, a, qtiles, st); break;
+        default: e = launch_t<EX_QPW_K256, 256>(mr, mq, a, qtiles, st); break;
     }
     if (e != cudaSuccess) return kErrLaunch;
     if (p.timer) p.timer->mark(st, kPhaseExactMain);

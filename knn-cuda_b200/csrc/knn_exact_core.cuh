@@ -11,6 +11,8 @@ constexpr int EX_BR = 256;       // reference points per tile
 constexpr int EX_BD = 16;        // dimensions per pipeline stage
 constexpr int EX_CB = 128;       // candidate slots per query (one half tile)
 constexpr int EX_WARPS = 16;     // consumer warps
+constexpr int EX_QPW = 4;        // queries per warp for k <= 128
+constexpr int EX_QPW_K256 = 2;   // queries per warp for 128 < k <= 256
 constexpr int EX_THREADS = (EX_WARPS + 1) * 32;
 constexpr int EX_STAGES = 3;
 
@@ -83,13 +85,47 @@ KNN_DI void warp_merge(unsigned long long *L, int c, int k, int lane) {
     __syncwarp();
 }
 
+// Buffer fill of query i (warp-uniform), one byte per query.
+KNN_DI int nbuf_get(uint32_t nb, int i) { return (int)((nb >> (8 * i)) & 0xffu); }
+KNN_DI uint32_t nbuf_set(uint32_t nb, int i, int v) {
+    return (nb & ~(0xffu << (8 * i))) | ((uint32_t)v << (8 * i));
+}
+
+// Merge query i's buffered candidates into its list (whose k-th key is the
+// query's threshold tau).
+template <int QPW, int KCAP>
+KNN_DI void flush_query(unsigned long long *wl, uint32_t &nb, int i, int k, int lane) {
+    constexpr int REGION = KCAP + EX_CB;
+    const int c = nbuf_get(nb, i);
+    if (c > 0) {
+        warp_merge<KCAP>(wl + i * REGION, c, k, lane);
+        nb = nbuf_set(nb, i, 0);
+    }
+}
+
+// Merge every query's buffered candidates (end of a reference range).
+template <int QPW, int KCAP>
+KNN_DI void flush_all(unsigned long long *wl, uint32_t &nb, int k, int lane) {
+    static_assert(QPW <= 4 && EX_CB < 256, "buffer fills packed in one word");
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) flush_query<QPW, KCAP>(wl, nb, i, k, lane);
+}
+
 // Filter one half tile (4 reference points per lane) against each query's
-// threshold, append survivors to the candidate buffers and merge.
+// threshold tau (the k-th key of its list) and append the survivors to the
+// query's candidate buffer.  The buffer is merged into the list only when
+// this half tile's survivors would not fit: tau then lags the candidates
+// seen, so more points pass, but merges become rare (the gap between them
+// grows geometrically as the list tightens) instead of one per half tile
+// that holds any survivor.  nb packs the warp-uniform buffer fills.
 // d2(i, j) gives the squared distance of query i to the lane's j-th point.
 template <int QPW, int KCAP, typename D2>
-KNN_DI void select_half(unsigned long long *wl, unsigned long long (&tau)[QPW], D2 d2,
-                        uint32_t rbase, int N, int k, int lane) {
+KNN_DI void select_half(unsigned long long *wl, uint32_t &nb, D2 d2, uint32_t rbase, int N,
+                        int k, int lane) {
     constexpr int REGION = KCAP + EX_CB;
+    unsigned long long tau[QPW];
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) tau[i] = wl[i * REGION + k - 1];
     uint32_t pm[QPW];
     bool any = false;
 #pragma unroll
@@ -105,11 +141,16 @@ KNN_DI void select_half(unsigned long long *wl, unsigned long long (&tau)[QPW], 
     }
     if (!__any_sync(0xffffffffu, any)) return;
     const unsigned lt = (1u << lane) - 1u;
-    int cnt[QPW];
 #pragma unroll
     for (int i = 0; i < QPW; ++i) {
+        const int m_i = (int)__reduce_add_sync(0xffffffffu, (unsigned)__popc(pm[i]));
+        if (m_i == 0) continue;
+        if (nbuf_get(nb, i) + m_i > EX_CB) {
+            __syncwarp();
+            flush_query<QPW, KCAP>(wl, nb, i, k, lane);
+        }
         unsigned long long *cb = wl + i * REGION + KCAP;
-        int c = 0;
+        int c = nbuf_get(nb, i);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const bool p = (pm[i] >> j) & 1u;
@@ -117,17 +158,9 @@ KNN_DI void select_half(unsigned long long *wl, unsigned long long (&tau)[QPW], 
             if (p) cb[c + __popc(m & lt)] = make_key(d2(i, j), rbase + j);
             c += __popc(m);
         }
-        cnt[i] = c;
+        nb = nbuf_set(nb, i, c);
     }
     __syncwarp();
-#pragma unroll
-    for (int i = 0; i < QPW; ++i) {
-        if (cnt[i] > 0) {
-            unsigned long long *L = wl + i * REGION;
-            warp_merge<KCAP>(L, cnt[i], k, lane);
-            tau[i] = L[k - 1];
-        }
-    }
 }
 
 
@@ -162,10 +195,10 @@ KNN_DI bool consume_ref_tile(f32x2_t (&acc)[QPW][4], const float *stages, uint64
         const float *rs = stages + (size_t)s * C::STAGE_FLOATS + C::Q_FLOATS + lane * 4;
 #pragma unroll 4
         for (int dd = 0; dd < EX_BD; ++dd) {
-            const float4 ra = *reinterpret_cast<const float4 *>(rs + dd * EX_BR);
-            const float4 rb = *reinterpret_cast<const float4 *>(rs + dd * EX_BR + 128);
-            const f32x2_t r0 = f2_pack(ra.x, ra.y), r1 = f2_pack(ra.z, ra.w);
-            const f32x2_t r2 = f2_pack(rb.x, rb.y), r3 = f2_pack(rb.z, rb.w);
+            // 16-byte loads straight into packed pairs (x, y), (z, w)
+            const ulonglong2 ra = *reinterpret_cast<const ulonglong2 *>(rs + dd * EX_BR);
+            const ulonglong2 rb = *reinterpret_cast<const ulonglong2 *>(rs + dd * EX_BR + 128);
+            const f32x2_t r0 = ra.x, r1 = ra.y, r2 = rb.x, r3 = rb.y;
             const f32x2_t *qp = reinterpret_cast<const f32x2_t *>(qs + dd * 2 * C::BQ);
 #pragma unroll
             for (int i = 0; i < QPW; ++i) {
@@ -185,15 +218,15 @@ KNN_DI bool consume_ref_tile(f32x2_t (&acc)[QPW][4], const float *stages, uint64
 
 // Select both halves of a consumed tile (reference points rt*256 + ...).
 template <int QPW, int KCAP>
-KNN_DI void select_tile(unsigned long long *wl, unsigned long long (&tau)[QPW],
-                        f32x2_t (&acc)[QPW][4], int rt, int N, int k, int lane) {
+KNN_DI void select_tile(unsigned long long *wl, uint32_t &nb, f32x2_t (&acc)[QPW][4], int rt,
+                        int N, int k, int lane) {
     const uint32_t rb0 = (uint32_t)rt * EX_BR + lane * 4;
     select_half<QPW, KCAP>(
-        wl, tau,
+        wl, nb,
         [&](int i, int j) { return (j & 1) ? f2_hi(acc[i][j >> 1]) : f2_lo(acc[i][j >> 1]); },
         rb0, N, k, lane);
     select_half<QPW, KCAP>(
-        wl, tau,
+        wl, nb,
         [&](int i, int j) {
             return (j & 1) ? f2_hi(acc[i][2 + (j >> 1)]) : f2_lo(acc[i][2 + (j >> 1)]);
         },

@@ -146,6 +146,35 @@ size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms);
 TcRefView tc_carve_ref(void *mem, int N, int d);
 int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, int d,
                    cudaStream_t st);
+// Staged form of launch_tc, for callers that stream the reference set in:
+// tc_run_begin (scratch carve, query prep), tc_run_pass1 (threshold sample:
+// every tc_sample_stride-th 256-point tile must be prepared), tc_run_pass2
+// over 256-point tile ranges as they become ready (each range prepared),
+// tc_run_finish (re-rank, certification, second chance; every tile prepared
+// and the maximum norm final).  launch_tc = all four over the whole set.
+struct TcRun {
+    TcProblem P;
+    TcRefView R;
+    int d_pad, kb, qtiles, n_tiles2, splits1, stride1, cmax;
+    long long ldf;
+    __nv_bfloat16 *qB;
+    float *qn, *thr, *retry, *p1, *qsub, *sd;
+    int *count, *fail, *fail2, *nfail, *si;
+    unsigned long long *cand_total, *cand;
+    unsigned char *xs;
+    size_t xcap;
+};
+int tc_tile_points();   // points per tile of the staged API (256)
+int tc_sample_stride(int N, int Q, int d, int k, int num_sms);
+// Prepare the 256-point tiles tile0 + i * tile_stride, i < n_tiles (the
+// maximum norm accumulates; tc_prepare_ref zeroes it and prepares all).
+int tc_prepare_ref_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
+                         int tile0, int n_tiles, int tile_stride, cudaStream_t st);
+int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun &run);
+int tc_run_pass1(TcRun &run, cudaStream_t st);
+int tc_run_pass2(TcRun &run, int tile_begin, int tile_end, cudaStream_t st);
+int tc_run_finish(TcRun &run, cudaStream_t st, int *host_stats);
+
 // Queues the tensor-core k-NN.  Synchronises once to learn how many queries
 // failed certification; those get a second scan with thresholds that
 // certify, and queries whose candidate list overflowed are recomputed by the

@@ -402,7 +402,8 @@ constexpr size_t TP_SMEM = 1024 + TP_OFF_BAR + TP_NBARS * 8 + 16;
 static_assert(TP_SMEM <= 232448, "pair scan kernel shared memory");
 
 struct TpArgs {
-    int N, Q, kb_count, n_tiles, n_splits;   // n_tiles: 256-point tiles
+    int N, Q, kb_count;
+    int tile_base, n_tiles, n_splits;   // 256-point tiles [tile_base, tile_base + n_tiles)
     int tile_stride;        // scan tiles t of the split with t % tile_stride == 0
     const float *thr;       // emit pass: [Q] thresholds (a units)
     float *p1;              // sample pass: [2 n_splits][Q][TC_KS] (per column half)
@@ -441,8 +442,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
     const bool lead = rank == 0;
     const int qpair = blockIdx.x >> 1, split = blockIdx.y;
     const int KB = a.kb_count;
-    const int t0 = (int)((long long)a.n_tiles * split / a.n_splits);
-    const int t1 = (int)((long long)a.n_tiles * (split + 1) / a.n_splits);
+    const int t0 = a.tile_base + (int)((long long)a.n_tiles * split / a.n_splits);
+    const int t1 = a.tile_base + (int)((long long)a.n_tiles * (split + 1) / a.n_splits);
     const int G = a.tile_stride;
     const int first = ((t0 + G - 1) / G) * G;
     const int n_my = first < t1 ? (t1 - first + G - 1) / G : 0;
@@ -775,16 +776,18 @@ __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld,
 
 // Reference-set prep in one pass over the input: point-major BF16 and FP32
 // copies (zero-padded to d_pad) plus the norm-step row and the largest
-// squared norm.  A block owns 32 points and walks the dimensions in 32 x 32
-// tiles through shared memory (coalesced on both sides); one thread per
-// point accumulates the squared norm in increasing d with FP32 fma, the
+// squared norm, for the 256-point tiles tile0 + i * tile_stride (eight
+// blocks per tile).  A block owns 32 points and walks the dimensions in
+// 32 x 32 tiles through shared memory (coalesced on both sides); one thread
+// per point accumulates the squared norm in increasing d with FP32 fma, the
 // order tc_norms_kernel uses.
 __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long ld, int d,
-                                   int d_pad, __nv_bfloat16 *__restrict__ xb,
-                                   float *__restrict__ xt, __nv_bfloat16 *__restrict__ parts,
+                                   int d_pad, int tile0, int tile_stride,
+                                   __nv_bfloat16 *__restrict__ xb, float *__restrict__ xt,
+                                   __nv_bfloat16 *__restrict__ parts,
                                    unsigned *__restrict__ max_bits) {
     __shared__ float tile[32][33];
-    const int p0 = blockIdx.x * 32;
+    const int p0 = (tile0 + (int)(blockIdx.x >> 3) * tile_stride) * TP_BN + (blockIdx.x & 7) * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     float s = 0.f;
     for (int d0 = 0; d0 < d_pad; d0 += 32) {
@@ -1108,8 +1111,8 @@ bool encode_norm_rows(CUtensorMap *m, const void *base, int rows) {
 constexpr int kTcCmaxPow2Max = 2048;
 
 struct TcPlan {
-    int d_pad, kb, qtiles, n_tiles, splits, splits1, stride1, cmax;
-    int n_tiles2, splits2;   // pair scan: 256-point tiles, splits over CTA pairs
+    int d_pad, kb, qtiles, stride1, cmax;
+    int n_tiles2, splits1;   // 256-point tiles; pass-1 splits over CTA pairs
 };
 
 // Splits that fill whole waves of one CTA per SM for `tiles` tiles per
@@ -1135,13 +1138,10 @@ TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
     p.d_pad = (d + 63) / 64 * 64;
     p.kb = p.d_pad / 64;
     p.qtiles = (Q + TC_QT - 1) / TC_QT;
-    p.n_tiles = (N + TC_BN - 1) / TC_BN;
-    p.splits = choose_splits(p.qtiles, p.n_tiles, 16, 2.0, num_sms);
     // the sample must hold about 2.5k points below T_q: KS * stride >= 2.5k
     p.stride1 = std::max(16, (5 * k + 2 * TC_KS - 1) / (2 * TC_KS));
     p.cmax = 4 * TC_KS * p.stride1;
     p.n_tiles2 = (N + TP_BN - 1) / TP_BN;
-    p.splits2 = choose_splits(p.qtiles, p.n_tiles2, 8, 2.0, std::max(1, num_sms / 2));
     // pass 1 (CTA pairs) scans every stride1-th 256-point tile; coarser
     // splits amortise each pair's set-up (query tile load, TMEM allocation,
     // pipeline fill)
@@ -1190,12 +1190,21 @@ size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
 
 int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, int d,
                    cudaStream_t st) {
-    const int d_pad = (d + 63) / 64 * 64;
     if (cudaMemsetAsync(v.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess) return kErrCuda;
-    tc_prep_ref_kernel<<<(N + 31) / 32, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, v.refB,
-                                                              v.refT, v.refN, v.rmax_bits);
+    return tc_prepare_ref_tiles(v, ref, N, ldr, d, 0, (N + TP_BN - 1) / TP_BN, 1, st);
+}
+
+int tc_prepare_ref_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
+                         int tile0, int n_tiles, int tile_stride, cudaStream_t st) {
+    if (n_tiles <= 0) return kOk;
+    const int d_pad = (d + 63) / 64 * 64;
+    tc_prep_ref_kernel<<<n_tiles * 8, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, tile0,
+                                                            tile_stride, v.refB, v.refT, v.refN,
+                                                            v.rmax_bits);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
+
+int tc_tile_points() { return TP_BN; }
 
 TcRefView tc_carve_ref(void *mem, int N, int d) {
     const int d_pad = (d + 63) / 64 * 64;
@@ -1210,59 +1219,66 @@ TcRefView tc_carve_ref(void *mem, int N, int d) {
 
 namespace {
 
-// Pass-2 scan + exact re-rank for a batch of queries whose BF16 copy is qB
-// (rows Q) and whose thresholds are thr.
-int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cudaStream_t st,
-                    const __nv_bfloat16 *qB, int Q, const float *qry, long long ldq,
-                    const float *qn, const float *thr, int *count, unsigned long long *cand,
-                    float *out_dist,
-                    int *out_idx, long long ld_out, int *fail, int *nfail, float *retry,
-                    unsigned long long *cand_total, bool second) {
-    const TcPlan pb = plan_tc(P.N, Q, P.d, P.k, P.num_sms);
-    const bool pair = !second;   // the full scan runs on CTA pairs
+// Emission scan of the reference tiles [tb, te) (256-point tiles) for the Q
+// queries whose BF16 copy is qB: CTA pairs (pair = true) or one CTA per 256
+// queries (second-chance scan of few queries).
+int emit_scan(const TcRun &r, cudaStream_t st, const __nv_bfloat16 *qB, int Q, const float *thr,
+              int tb, int te, bool pair) {
+    const TcProblem &P = r.P;
     CUtensorMap tmA, tmB, tmN;
-    if (!encode_bf16_kmajor(&tmA, qB, Q, p.d_pad)) return kErrTensorMap;
-    if (!encode_bf16_kmajor(&tmB, R.refB, P.N, p.d_pad)) return kErrTensorMap;
-    if (!encode_norm_rows(&tmN, R.refN, P.N)) return kErrTensorMap;
+    if (!encode_bf16_kmajor(&tmA, qB, Q, r.d_pad)) return kErrTensorMap;
+    if (!encode_bf16_kmajor(&tmB, r.R.refB, P.N, r.d_pad)) return kErrTensorMap;
+    if (!encode_norm_rows(&tmN, r.R.refN, P.N)) return kErrTensorMap;
+    const int qtiles = (Q + TC_QT - 1) / TC_QT;
     if (pair) {
         TpArgs a;
         a.N = P.N;
         a.Q = Q;
-        a.kb_count = p.kb;
-        a.n_tiles = pb.n_tiles2;
-        a.n_splits = pb.splits2;
+        a.kb_count = r.kb;
+        a.tile_base = tb;
+        a.n_tiles = te - tb;
+        a.n_splits = choose_splits(qtiles, te - tb, 8, 2.0, std::max(1, P.num_sms / 2));
         a.tile_stride = 1;
         a.thr = thr;
         a.p1 = nullptr;
-        a.cand = cand;
-        a.count = count;
-        a.cmax = p.cmax;
+        a.cand = r.cand;
+        a.count = r.count;
+        a.cmax = r.cmax;
         a.status = P.status;
-        knn_tc_pair_scan_kernel<1><<<dim3(2 * pb.qtiles, pb.splits2), TC_THREADS, TP_SMEM, st>>>(
+        knn_tc_pair_scan_kernel<1><<<dim3(2 * qtiles, a.n_splits), TC_THREADS, TP_SMEM, st>>>(
             tmA, tmB, tmN, a);
     } else {
+        // 128-point tiles of the same range
+        const int n_tiles = std::min((P.N + TC_BN - 1) / TC_BN, 2 * te) - 2 * tb;
         TcArgs a;
         a.N = P.N;
         a.Q = Q;
-        a.kb_count = p.kb;
-        a.n_tiles = p.n_tiles;
-        a.n_splits = pb.splits;
+        a.kb_count = r.kb;
+        a.n_tiles = n_tiles;
+        a.n_splits = choose_splits(qtiles, n_tiles, 16, 2.0, P.num_sms);
         a.tile_stride = 1;
         a.thr = thr;
         a.p1 = nullptr;
-        a.cand = cand;
-        a.count = count;
-        a.cmax = p.cmax;
+        a.cand = r.cand;
+        a.count = r.count;
+        a.cmax = r.cmax;
         a.status = P.status;
-        knn_tc_scan_kernel<1><<<dim3(pb.qtiles, pb.splits), TC_THREADS, TC_SMEM, st>>>(
+        if (tb != 0) return kErrInvalid;   // the single-CTA scan covers the whole set
+        knn_tc_scan_kernel<1><<<dim3(qtiles, a.n_splits), TC_THREADS, TC_SMEM, st>>>(
             tmA, tmB, tmN, a);
     }
-    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-    if (P.timer) P.timer->mark(st, second ? kPhaseTcRetryScan : kPhaseTcPass2);
-    if (cudaMemsetAsync(nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
+    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
+}
+
+// Exact re-rank + certification of Q queries (see tc_rerank_kernel).
+int rerank(const TcRun &r, cudaStream_t st, int Q, const float *qry, long long ldq,
+           const float *qn, const float *thr, float *out_dist, int *out_idx, long long ld_out,
+           int *fail) {
+    const TcProblem &P = r.P;
+    if (cudaMemsetAsync(r.nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
     int cpow = 1;
-    while (cpow < p.cmax) cpow <<= 1;
-    const size_t rsmem = TC_RR_WARPS * tc_rr_warp_bytes(p.d_pad, cpow);
+    while (cpow < r.cmax) cpow <<= 1;
+    const size_t rsmem = TC_RR_WARPS * tc_rr_warp_bytes(r.d_pad, cpow);
     // one fixed limit (the largest any shape uses) for every launch, so that
     // calls from several host threads never lower it under each other
     const size_t rsmem_max = TC_RR_WARPS * tc_rr_warp_bytes(TC_KBMAX * TC_BK, kTcCmaxPow2Max);
@@ -1271,11 +1287,9 @@ int scan_and_rerank(const TcProblem &P, const TcRefView &R, const TcPlan &p, cud
                              (int)rsmem_max) != cudaSuccess)
         return kErrLaunch;
     tc_rerank_kernel<<<(Q + TC_RR_WARPS - 1) / TC_RR_WARPS, TC_RR_WARPS * 32, rsmem, st>>>(
-        R.refT, P.d, p.d_pad, qry, ldq, qn, R.rmax_bits, thr, cand, count, p.cmax, cpow, Q, P.k,
-        out_dist, out_idx, ld_out, fail, nfail, retry, cand_total);
-    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-    if (P.timer) P.timer->mark(st, second ? kPhaseTcRetryRerank : kPhaseTcRerank);
-    return kOk;
+        r.R.refT, P.d, r.d_pad, qry, ldq, qn, r.R.rmax_bits, thr, r.cand, r.count, r.cmax, cpow,
+        Q, P.k, out_dist, out_idx, ld_out, fail, r.nfail, r.retry, r.cand_total);
+    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
 int read_count(const int *dev, int *host_pinned, cudaStream_t st, int &out) {
@@ -1289,39 +1303,48 @@ int read_count(const int *dev, int *host_pinned, cudaStream_t st, int &out) {
 
 }  // namespace
 
-int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_stats) {
-    int *host_tmp = host_stats + 2;
-    host_stats[0] = host_stats[1] = 0;
-    host_stats[4] = host_stats[5] = 0;
-    const TcPlan p = plan_tc(P.N, P.Q, P.d, P.k, P.num_sms);
+int tc_sample_stride(int N, int Q, int d, int k, int num_sms) {
+    return plan_tc(N, Q, d, k, num_sms).stride1;
+}
+
+int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun &r) {
     if (!tc_supported(P.N, P.Q, P.d, P.k)) return kErrUnsupported;
+    const TcPlan p = plan_tc(P.N, P.Q, P.d, P.k, P.num_sms);
+    r.P = P;
+    r.R = R;
+    r.d_pad = p.d_pad;
+    r.kb = p.kb;
+    r.qtiles = p.qtiles;
+    r.n_tiles2 = p.n_tiles2;
+    r.splits1 = p.splits1;
+    r.stride1 = p.stride1;
+    r.cmax = p.cmax;
     Carve cv{static_cast<unsigned char *>(P.scratch), 0, P.scratch_bytes};
-    __nv_bfloat16 *qB = cv.take<__nv_bfloat16>((size_t)p.qtiles * TC_QT * p.d_pad);
-    float *qn = cv.take<float>(P.Q);
-    float *thr = cv.take<float>(P.Q);
-    float *retry = cv.take<float>(P.Q);
-    int *count = cv.take<int>(P.Q);
-    int *fail = cv.take<int>(P.Q);
-    int *fail2 = cv.take<int>(P.Q);
-    int *nfail = cv.take<int>(4);
-    unsigned long long *cand_total = cv.take<unsigned long long>(1);
-    float *p1 = cv.take<float>((size_t)2 * p.splits1 * P.Q * TC_KS);
-    unsigned long long *cand = cv.take<unsigned long long>((size_t)P.Q * p.cmax);
-    const long long ldf = (P.Q + 3) / 4 * 4;       // second-chance buffers, sized for all queries
-    float *qsub = cv.take<float>((size_t)P.d * ldf);
-    float *sd = cv.take<float>((size_t)P.k * ldf);
-    int *si = cv.take<int>((size_t)P.k * ldf);
-    unsigned char *xs = cv.take<unsigned char>(0);
-    const size_t xcap = P.scratch_bytes > cv.used ? P.scratch_bytes - cv.used : 0;
+    r.qB = cv.take<__nv_bfloat16>((size_t)p.qtiles * TC_QT * p.d_pad);
+    r.qn = cv.take<float>(P.Q);
+    r.thr = cv.take<float>(P.Q);
+    r.retry = cv.take<float>(P.Q);
+    r.count = cv.take<int>(P.Q);
+    r.fail = cv.take<int>(P.Q);
+    r.fail2 = cv.take<int>(P.Q);
+    r.nfail = cv.take<int>(4);
+    r.cand_total = cv.take<unsigned long long>(1);
+    r.p1 = cv.take<float>((size_t)2 * p.splits1 * P.Q * TC_KS);
+    r.cand = cv.take<unsigned long long>((size_t)P.Q * p.cmax);
+    r.ldf = (P.Q + 3) / 4 * 4;   // second-chance buffers, sized for all queries
+    r.qsub = cv.take<float>((size_t)P.d * r.ldf);
+    r.sd = cv.take<float>((size_t)P.k * r.ldf);
+    r.si = cv.take<int>((size_t)P.k * r.ldf);
+    r.xs = cv.take<unsigned char>(0);
     if (cv.used > P.scratch_bytes) return kErrScratch;
-    PhaseTimer *tm = P.timer;
+    r.xcap = P.scratch_bytes - cv.used;
 
     // queries: norms + BF16 K-major copy of -2 q
-    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, qn, nullptr);
+    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, r.qn, nullptr);
     tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
-        P.qry, P.Q, P.ldq, P.d, p.d_pad, -2.0f, qB, nullptr);
+        P.qry, P.Q, P.ldq, P.d, p.d_pad, -2.0f, r.qB, nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-    if (tm) tm->mark(st, kPhaseTcPrepQuery);
+    if (P.timer) P.timer->mark(st, kPhaseTcPrepQuery);
     if (cudaFuncSetAttribute(knn_tc_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TC_SMEM) != cudaSuccess ||
         cudaFuncSetAttribute(knn_tc_pair_scan_kernel<0>,
@@ -1331,64 +1354,86 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TP_SMEM) != cudaSuccess)
         return kErrLaunch;
-
-    // pass 1: thresholds from a strided sample of the reference tiles
-    {
-        CUtensorMap tmA, tmB, tmN;
-        if (!encode_bf16_kmajor(&tmA, qB, P.Q, p.d_pad)) return kErrTensorMap;
-        if (!encode_bf16_kmajor(&tmB, R.refB, P.N, p.d_pad)) return kErrTensorMap;
-        if (!encode_norm_rows(&tmN, R.refN, P.N)) return kErrTensorMap;
-        TpArgs a;
-        a.N = P.N;
-        a.Q = P.Q;
-        a.kb_count = p.kb;
-        a.n_tiles = p.n_tiles2;
-        a.n_splits = p.splits1;
-        a.tile_stride = p.stride1;
-        a.thr = nullptr;
-        a.p1 = p1;
-        a.cand = cand;
-        a.count = count;
-        a.cmax = p.cmax;
-        a.status = P.status;
-        knn_tc_pair_scan_kernel<0><<<dim3(2 * p.qtiles, p.splits1), TC_THREADS, TP_SMEM, st>>>(
-            tmA, tmB, tmN, a);
-        if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-        if (tm) tm->mark(st, kPhaseTcPass1);
-        // two lists (column halves) per pair and split
-        tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(p1, 2 * p.splits1, P.Q, qn,
-                                                               R.rmax_bits, p.d_pad, thr, count);
-        if (tm) tm->mark(st, kPhaseTcThreshold);
-    }
-    // pass 2 + re-rank of every query
-    if (cudaMemsetAsync(cand_total, 0, sizeof(unsigned long long), st) != cudaSuccess)
+    if (cudaMemsetAsync(r.cand_total, 0, sizeof(unsigned long long), st) != cudaSuccess)
         return kErrCuda;
-    int rc = scan_and_rerank(P, R, p, st, qB, P.Q, P.qry, P.ldq, qn, thr, count, cand,
-                             P.out_dist, P.out_idx, P.ld_out, fail, nfail, retry, cand_total,
-                             false);
+    return kOk;
+}
+
+int tc_run_pass1(TcRun &r, cudaStream_t st) {
+    const TcProblem &P = r.P;
+    CUtensorMap tmA, tmB, tmN;
+    if (!encode_bf16_kmajor(&tmA, r.qB, P.Q, r.d_pad)) return kErrTensorMap;
+    if (!encode_bf16_kmajor(&tmB, r.R.refB, P.N, r.d_pad)) return kErrTensorMap;
+    if (!encode_norm_rows(&tmN, r.R.refN, P.N)) return kErrTensorMap;
+    TpArgs a;
+    a.N = P.N;
+    a.Q = P.Q;
+    a.kb_count = r.kb;
+    a.tile_base = 0;
+    a.n_tiles = r.n_tiles2;
+    a.n_splits = r.splits1;
+    a.tile_stride = r.stride1;
+    a.thr = nullptr;
+    a.p1 = r.p1;
+    a.cand = r.cand;
+    a.count = r.count;
+    a.cmax = r.cmax;
+    a.status = P.status;
+    knn_tc_pair_scan_kernel<0><<<dim3(2 * r.qtiles, r.splits1), TC_THREADS, TP_SMEM, st>>>(
+        tmA, tmB, tmN, a);
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    if (P.timer) P.timer->mark(st, kPhaseTcPass1);
+    // two lists (column halves) per pair and split; resets the counts
+    tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(r.p1, 2 * r.splits1, P.Q, r.qn,
+                                                           r.R.rmax_bits, r.d_pad, r.thr,
+                                                           r.count);
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    if (P.timer) P.timer->mark(st, kPhaseTcThreshold);
+    return kOk;
+}
+
+int tc_run_pass2(TcRun &r, int tile_begin, int tile_end, cudaStream_t st) {
+    tile_end = std::min(tile_end, r.n_tiles2);
+    if (tile_begin >= tile_end) return kOk;
+    const int rc = emit_scan(r, st, r.qB, r.P.Q, r.thr, tile_begin, tile_end, true);
+    if (rc == kOk && r.P.timer) r.P.timer->mark(st, kPhaseTcPass2);
+    return rc;
+}
+
+int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
+    const TcProblem &P = r.P;
+    PhaseTimer *tm = P.timer;
+    int *host_tmp = host_stats + 2;
+    host_stats[0] = host_stats[1] = 0;
+    host_stats[4] = host_stats[5] = 0;
+    int rc = rerank(r, st, P.Q, P.qry, P.ldq, r.qn, r.thr, P.out_dist, P.out_idx, P.ld_out,
+                    r.fail);
     if (rc != kOk) return rc;
+    if (tm) tm->mark(st, kPhaseTcRerank);
     int nf = 0;
-    if (cudaMemcpyAsync(host_stats + 4, cand_total, sizeof(unsigned long long),
+    if (cudaMemcpyAsync(host_stats + 4, r.cand_total, sizeof(unsigned long long),
                         cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return kErrCuda;
-    if ((rc = read_count(nfail, host_tmp, st, nf)) != kOk) return rc;
+    if ((rc = read_count(r.nfail, host_tmp, st, nf)) != kOk) return rc;
     host_stats[0] = nf;
     if (nf == 0) return kOk;
 
     // second chance: the uncertified queries, compacted, scanned again with
     // thresholds that certify (list overflows excepted)
-    gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, fail,
-                                                                       nf, qsub, ldf);
-    tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(qsub, nf, ldf, P.d, qn, nullptr);
-    tc_pack_kernel<<<dim3((nf + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
-        qsub, nf, ldf, P.d, p.d_pad, -2.0f, qB, nullptr);
-    tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(fail, nf, retry, thr, count);
+    gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, r.fail,
+                                                                       nf, r.qsub, r.ldf);
+    tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(r.qsub, nf, r.ldf, P.d, r.qn, nullptr);
+    tc_pack_kernel<<<dim3((nf + 31) / 32, r.d_pad / 32), dim3(32, 8), 0, st>>>(
+        r.qsub, nf, r.ldf, P.d, r.d_pad, -2.0f, r.qB, nullptr);
+    tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(r.fail, nf, r.retry, r.thr, r.count);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-    rc = scan_and_rerank(P, R, p, st, qB, nf, qsub, ldf, qn, thr, count, cand, sd, si, ldf,
-                         fail2, nfail, retry, cand_total, true);
+    if ((rc = emit_scan(r, st, r.qB, nf, r.thr, 0, r.n_tiles2, false)) != kOk) return rc;
+    if (tm) tm->mark(st, kPhaseTcRetryScan);
+    rc = rerank(r, st, nf, r.qsub, r.ldf, r.qn, r.thr, r.sd, r.si, r.ldf, r.fail2);
     if (rc != kOk) return rc;
+    if (tm) tm->mark(st, kPhaseTcRetryRerank);
     int nf2 = 0;
-    if ((rc = read_count(nfail, host_tmp, st, nf2)) != kOk) return rc;
+    if ((rc = read_count(r.nfail, host_tmp, st, nf2)) != kOk) return rc;
     host_stats[1] = nf2;
     if (nf2 > 0) {
         // still uncertified (list overflow): the exact kernel recomputes the
@@ -1396,21 +1441,21 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
         const long long per_split = (long long)nf * P.k * 8;
         const int splits = (int)std::max<long long>(
             1, std::min<long long>(exact_plan_splits(P.N, nf, P.d, P.k, P.num_sms),
-                                   (long long)(xcap / per_split)));
+                                   (long long)(r.xcap / per_split)));
         ExactProblem x;
         x.ref = P.ref;
         x.N = P.N;
         x.ldr = P.ldr;
-        x.qry = qsub;
+        x.qry = r.qsub;
         x.Q = nf;
-        x.ldq = ldf;
+        x.ldq = r.ldf;
         x.d = P.d;
         x.k = P.k;
-        x.out_dist = sd;
-        x.out_idx = si;
-        x.ld_out = ldf;
-        x.scratch = xs;
-        x.scratch_bytes = xcap;
+        x.out_dist = r.sd;
+        x.out_idx = r.si;
+        x.ld_out = r.ldf;
+        x.scratch = r.xs;
+        x.scratch_bytes = r.xcap;
         x.status = P.status;
         x.num_sms = P.num_sms;
         x.force_splits = splits;
@@ -1418,10 +1463,19 @@ int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host
         if ((rc = launch_exact(x, st)) != kOk) return rc;
     }
     scatter_results_kernel<<<dim3((nf + 127) / 128, P.k), 128, 0, st>>>(
-        sd, si, ldf, fail, nf, P.out_dist, P.out_idx, P.ld_out);
+        r.sd, r.si, r.ldf, r.fail, nf, P.out_dist, P.out_idx, P.ld_out);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (tm) tm->mark(st, kPhaseTcFallback);
     return kOk;
+}
+
+int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_stats) {
+    TcRun r;
+    int rc = tc_run_begin(P, R, st, r);
+    if (rc == kOk) rc = tc_run_pass1(r, st);
+    if (rc == kOk) rc = tc_run_pass2(r, 0, r.n_tiles2, st);
+    if (rc == kOk) rc = tc_run_finish(r, st, host_stats);
+    return rc;
 }
 
 }  // namespace knnb200

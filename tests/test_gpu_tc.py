@@ -126,3 +126,28 @@ def test_fallback_path_exercised(knncuda, gpu):
     assert second > 0 and exact <= second
     assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
     assert np.array_equal(ic, ig)
+
+
+@pytest.mark.parametrize("n,dim,k", [(262144, 64, 20),     # tile-aligned, 8 whole chunks
+                                     (299108, 96, 100),    # ragged last sample tile and chunk
+                                     (1 << 20, 256, 100)])  # the headline shape
+def test_cublas_host_streamed_from_pinned_memory(knncuda, gpu, n, dim, k):
+    """knn_cublas from page-locked host buffers on a large set streams the
+    reference set in (sample tiles first, then chunks, each scanned once it
+    has landed); the answer equals knn_cuda_global's bit for bit."""
+    import torch
+
+    rng = np.random.default_rng(n + dim)
+    q = 300
+    ref = torch.from_numpy(rng.random((dim, n), dtype=np.float32)).pin_memory().numpy()
+    query = torch.from_numpy(rng.random((dim, q), dtype=np.float32)).pin_memory().numpy()
+    d0, i0 = np.empty((k, q), np.float32), np.empty((k, q), np.int32)
+    d1 = torch.empty((k, q), dtype=torch.float32).pin_memory().numpy()
+    i1 = torch.empty((k, q), dtype=torch.int32).pin_memory().numpy()
+    assert knncuda.knn_cuda_global(ref, n, query, q, dim, k, d0, i0)
+    for _ in range(2):   # the second call reuses the workspace's buffers
+        d1[:] = -1
+        i1[:] = -1
+        assert knncuda.knn_cublas(ref, n, query, q, dim, k, d1, i1)
+        assert np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
+        assert np.array_equal(i0, i1)
