@@ -45,36 +45,70 @@ KNN_DI int rank_pow2(const unsigned long long *L, unsigned long long x) {
     return pos + (L[pos] < x ? 1 : 0);
 }
 
-// Merge c unsorted candidate keys (L[KCAP .. KCAP+c)) into the sorted list
-// L[0..k) held by one warp.  Every key's final position is its rank in the
-// union: list element at p -> p + #(candidates below it); candidate x ->
-// #(list below x) + #(candidates below x).  Keys are unique (distinct
-// indices), so the positions form a permutation; positions >= k are dropped.
+// Ascending bitonic sort of 128 keys held by one warp, four per lane
+// (element e = b * 32 + lane in v[b]): lane partners by shuffle, register
+// partners in place.
+KNN_DI void warp_sort128(unsigned long long (&v)[4], int lane) {
+#pragma unroll
+    for (int size = 2; size <= 128; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            if (stride >= 32) {
+                const int rs = stride >> 5;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    if (b & rs) continue;
+                    const bool up = (((b << 5) | lane) & size) == 0;
+                    const unsigned long long x = v[b], y = v[b | rs];
+                    const bool sw = (x > y) == up;
+                    v[b] = sw ? y : x;
+                    v[b | rs] = sw ? x : y;
+                }
+            } else {
+                const bool lower = (lane & stride) == 0;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const bool up = (((b << 5) | lane) & size) == 0;
+                    const unsigned long long x = v[b];
+                    const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, stride);
+                    const unsigned long long mn = x < y ? x : y, mx = x < y ? y : x;
+                    v[b] = (lower == up) ? mn : mx;
+                }
+            }
+        }
+    }
+}
+
+// Merge c (<= EX_CB) unsorted candidate keys (L[KCAP .. KCAP+c)) into the
+// sorted list L[0..k) held by one warp.  The candidates are sorted in
+// registers and written back sorted; then every key's final position is its
+// index plus its rank in the other sorted array (binary search).  Keys are
+// unique (distinct indices), so the positions form a permutation; positions
+// >= k are dropped.
 template <int KCAP>
 KNN_DI void warp_merge(unsigned long long *L, int c, int k, int lane) {
     constexpr int LPL = KCAP / 32;
     constexpr int CPL = EX_CB / 32;
-    const unsigned long long *C = L + KCAP;
+    static_assert(CPL == 4, "warp_sort128 holds four keys per lane");
+    unsigned long long *C = L + KCAP;
     unsigned long long lv[LPL], cv[CPL];
-    int lp[LPL], cp[CPL];
-#pragma unroll
-    for (int a = 0; a < LPL; ++a) {
-        lv[a] = L[a * 32 + lane];
-        lp[a] = a * 32 + lane;
-    }
 #pragma unroll
     for (int b = 0; b < CPL; ++b) {
         const int t = b * 32 + lane;
         cv[b] = t < c ? C[t] : kKeyInf;
-        cp[b] = rank_pow2<KCAP>(L, cv[b]);
     }
-    for (int t = 0; t < c; ++t) {
-        const unsigned long long x = C[t];
+    warp_sort128(cv, lane);
 #pragma unroll
-        for (int a = 0; a < LPL; ++a) lp[a] += x < lv[a] ? 1 : 0;
+    for (int a = 0; a < LPL; ++a) lv[a] = L[a * 32 + lane];
+    __syncwarp();
 #pragma unroll
-        for (int b = 0; b < CPL; ++b) cp[b] += x < cv[b] ? 1 : 0;
-    }
+    for (int b = 0; b < CPL; ++b) C[b * 32 + lane] = cv[b];
+    __syncwarp();
+    int lp[LPL], cp[CPL];
+#pragma unroll
+    for (int a = 0; a < LPL; ++a) lp[a] = a * 32 + lane + rank_pow2<EX_CB>(C, lv[a]);
+#pragma unroll
+    for (int b = 0; b < CPL; ++b) cp[b] = b * 32 + lane + rank_pow2<KCAP>(L, cv[b]);
     __syncwarp();
 #pragma unroll
     for (int a = 0; a < LPL; ++a)
@@ -104,10 +138,11 @@ KNN_DI void flush_query(unsigned long long *wl, uint32_t &nb, int i, int k, int 
 }
 
 // Merge every query's buffered candidates (end of a reference range).
+// (Loops over queries are not unrolled: one inlined copy of the merge.)
 template <int QPW, int KCAP>
 KNN_DI void flush_all(unsigned long long *wl, uint32_t &nb, int k, int lane) {
     static_assert(QPW <= 4 && EX_CB < 256, "buffer fills packed in one word");
-#pragma unroll
+#pragma unroll 1
     for (int i = 0; i < QPW; ++i) flush_query<QPW, KCAP>(wl, nb, i, k, lane);
 }
 
@@ -141,14 +176,22 @@ KNN_DI void select_half(unsigned long long *wl, uint32_t &nb, D2 d2, uint32_t rb
     }
     if (!__any_sync(0xffffffffu, any)) return;
     const unsigned lt = (1u << lane) - 1u;
+    // queries whose buffer cannot take this half tile's survivors: merge first
+    uint32_t full_mask = 0;
 #pragma unroll
     for (int i = 0; i < QPW; ++i) {
         const int m_i = (int)__reduce_add_sync(0xffffffffu, (unsigned)__popc(pm[i]));
-        if (m_i == 0) continue;
-        if (nbuf_get(nb, i) + m_i > EX_CB) {
-            __syncwarp();
-            flush_query<QPW, KCAP>(wl, nb, i, k, lane);
-        }
+        if (nbuf_get(nb, i) + m_i > EX_CB) full_mask |= 1u << i;
+    }
+    if (full_mask) {
+        __syncwarp();
+#pragma unroll 1
+        for (int i = 0; i < QPW; ++i)
+            if ((full_mask >> i) & 1u) flush_query<QPW, KCAP>(wl, nb, i, k, lane);
+    }
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) {
+        if (__ballot_sync(0xffffffffu, pm[i] != 0) == 0) continue;
         unsigned long long *cb = wl + i * REGION + KCAP;
         int c = nbuf_get(nb, i);
 #pragma unroll
