@@ -54,6 +54,7 @@ CASES = [
     (10, 33, 1000, 8, 33),      # k == ref_nb, ragged
     (11, 5000, 1, 256, 100),    # Q = 1
     (12, 65, 40, 200, 64),
+    (13, 140000, 40, 16, 50),   # large set, many reference splits
 ]
 
 
@@ -86,6 +87,25 @@ def test_duplicate_points_tie_order(knncuda, oracle, gpu):
     assert np.array_equal(i[same], gt_i[same])
     d64, i64 = oracle.knn_f64(ref, query, 12, threads=THREADS)
     check_exact(d, i, ref, query, d64, i64)
+
+
+def test_split_lists_with_duplicates(knncuda, oracle, gpu):
+    # a large set (several reference splits, buffered merges) in which every
+    # point appears 4 times: split lists and their merge must still keep the
+    # lower index first among equal keys
+    rng = np.random.default_rng(22)
+    base = rng.random((24, 40000), dtype=np.float32)
+    ref = np.ascontiguousarray(np.tile(base, (1, 4)))
+    query = np.ascontiguousarray(base[:, :30] + 1e-3)
+    d, i = knncuda.knn(ref, query, 40)
+    gt_d, gt_i = oracle.knn_c(ref, query, 40, threads=THREADS)
+    same = np.isclose(d, gt_d, rtol=0, atol=0)
+    assert same.mean() > 0.5
+    assert np.array_equal(i[same], gt_i[same])
+    d64, i64 = oracle.knn_f64(ref, query, 40, threads=THREADS)
+    check_exact(d, i, ref, query, d64, i64)
+    # copies come in runs of 4 equal distances with indices p, p + 40000, ...
+    assert np.all(np.diff(d, axis=0) >= 0)
 
 
 def test_equidistant_ring(knncuda, gpu):
