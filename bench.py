@@ -56,8 +56,12 @@ METRIC = "kNN queries/sec (N=1M,d=256,k=100): FP32 exact vs BF16+rerank @ recall
 UNIT = "queries/s"
 
 # DRAM traffic (read + write bytes) per launch of the dominant kernel, from
-# the ncu capture summarised in profiles/ (None until captured for a kernel).
-NCU_TRAFFIC_BYTES = {}
+# the ncu capture summarised in profiles/, keyed by (kernel, workload,
+# queries); None for a configuration that was not captured.
+NCU_TRAFFIC_BYTES = {
+    # dram__bytes_read.sum 1,037,806,336 + dram__bytes_write.sum 42,388,224
+    ("knn_tc_pair_scan_kernel<1>", "mixture256", 16384): 1037806336 + 42388224,
+}
 
 
 def parse_args(argv=None):
@@ -390,11 +394,13 @@ def run_ours(args, D: Dist):
                 "api": "knn_cublas (drop-in C-ABI, pinned host buffers)",
                 "ms_per_step": e2e["bf16_rerank"] * 1e3},
         "gpu_launches": launches * args.steps,
-        "roofline": {"bound": "tensor", "kernel": "knn_tc_scan_kernel<1> (pass-2 scan)",
+        "roofline": {"bound": "tensor",
+                     "kernel": "knn_tc_pair_scan_kernel<1> (pass-2 scan on CTA pairs)",
                      "achieved": achieved / 1e12 if achieved else None,
                      "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
                      "frac": achieved / peak if achieved else None,
-                     "traffic": NCU_TRAFFIC_BYTES.get("knn_tc_scan_kernel<1>"),
+                     "traffic": NCU_TRAFFIC_BYTES.get(
+                         ("knn_tc_pair_scan_kernel<1>", w.name, qn)),
                      "algorithmic": "2*d_pad flops per (query, reference) pair, d_pad=256",
                      "peak_source": peaks["source"]},
         "clocks": head.get("clocks"),
