@@ -111,7 +111,10 @@ KNNB200_API int knnb200_refset_knn(knnb200_refset *rs, const float *query, int q
  * admitted only while the working memory of all batches in flight stays
  * within memory_budget_bytes (one batch is always admitted).  Requests of
  * different k share a batch (top-k_max, each takes its first k rows), and a
- * request's result does not depend on its batch. */
+ * request's result does not depend on its batch.  Each slot's device buffers
+ * are allocated at creation for a full batch at k = 128 (KNNB200_ENOMEM if
+ * they do not fit), so no allocation happens on the request path unless a
+ * batch needs k > 128. */
 typedef struct knnb200_server knnb200_server;
 KNNB200_API int knnb200_server_create(knnb200_refset *rs, int slots, size_t memory_budget_bytes,
                                       int max_batch_queries, int method, knnb200_server **out);

@@ -311,6 +311,10 @@ struct knnb200_server {
 
 namespace {
 
+// Slot buffers are sized at server creation for a full batch at this k
+// (larger k grows them on first use).
+constexpr int kPresizeK = 128;
+
 size_t batch_bytes(const knnb200_server *s, int Q, int kmax) {
     const knnb200_refset *rs = s->rs;
     return (size_t)rs->d * round_up(Q, 64) * 4 + (size_t)kmax * Q * 8 +
@@ -437,6 +441,22 @@ int knnb200_server_create(knnb200_refset *rs, int slots, size_t memory_budget_by
             delete s;
             return KNNB200_ECUDA;
         }
+    // Size every slot for a full batch at k = kPresizeK now: growing a
+    // buffer later frees device memory, which synchronises the whole device
+    // and stalls every slot's batch in flight.
+    const int kq = std::min(kPresizeK, rs->N);
+    const long long ldq = round_up(max_batch_queries, 64);
+    for (int i = 0; i < slots; ++i) {
+        Slot &sl = s->slots[i];
+        if (!sl.qry.ensure((size_t)rs->d * ldq * 4) ||
+            !sl.dist.ensure((size_t)kq * max_batch_queries * 4) ||
+            !sl.idx.ensure((size_t)kq * max_batch_queries * 4) ||
+            !sl.scratch.ensure(scratch_need(rs, method, max_batch_queries, kq))) {
+            for (int j = 0; j < slots; ++j) s->slots[j].destroy();
+            delete s;
+            return KNNB200_ENOMEM;
+        }
+    }
     for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker_loop, s, i);
     *out = s;
     return KNNB200_OK;
