@@ -93,6 +93,62 @@ struct TcArgs {
     int *status;
 };
 
+// Bit e set iff v[e] < lim: independent compares, then a 3-input OR tree
+// (depth 4) instead of a 32-long dependent chain.
+KNN_DI uint32_t below_mask(const uint32_t (&v)[32], float lim) {
+    uint32_t b[32];
+#pragma unroll
+    for (int e = 0; e < 32; ++e) b[e] = __uint_as_float(v[e]) < lim ? (1u << e) : 0u;
+    uint32_t t[11];
+#pragma unroll
+    for (int i = 0; i < 10; ++i) t[i] = b[3 * i] | b[3 * i + 1] | b[3 * i + 2];
+    t[10] = b[30] | b[31];
+    const uint32_t u0 = t[0] | t[1] | t[2], u1 = t[3] | t[4] | t[5];
+    const uint32_t u2 = t[6] | t[7] | t[8], u3 = t[9] | t[10];
+    return u0 | u1 | u2 | u3;
+}
+
+// v[e] for a run-time e: a binary select tree on e's bits (depth 5)
+// instead of a 31-long dependent chain; v stays in registers.
+KNN_DI uint32_t select32(const uint32_t (&v)[32], int e) {
+    uint32_t s16[16], s8[8], s4[4];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) s16[i] = (e & 1) ? v[2 * i + 1] : v[2 * i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s8[i] = (e & 2) ? s16[2 * i + 1] : s16[2 * i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) s4[i] = (e & 4) ? s8[2 * i + 1] : s8[2 * i];
+    const uint32_t s2a = (e & 8) ? s4[1] : s4[0], s2b = (e & 8) ? s4[3] : s4[2];
+    return (e & 16) ? s2b : s2a;
+}
+
+// Candidates found by one epilogue thread, appended to its query's list
+// later with one atomicAdd that reserves all their slots: the append's
+// round trip then overlaps the wait for the next accumulator instead of
+// lengthening the test of the current one (the next tile's TMEM load waits
+// for that test).
+struct PendingCands {
+    static constexpr int kMax = 4;
+    unsigned long long e[kMax];
+    int n = 0;
+    KNN_DI void flush(int *count, unsigned long long *cand, int cmax, int qrow) {
+        if (n == 0) return;
+        const int pos = atomicAdd(&count[qrow], n);
+#pragma unroll
+        for (int p = 0; p < kMax; ++p)
+            if (p < n && pos + p < cmax) cand[(size_t)qrow * cmax + pos + p] = e[p];
+        n = 0;
+    }
+    KNN_DI void push(unsigned long long key, int *count, unsigned long long *cand, int cmax,
+                     int qrow) {
+        if (n == kMax) flush(count, cand, cmax, qrow);
+#pragma unroll
+        for (int p = 0; p < kMax; ++p)
+            if (p == n) e[p] = key;
+        ++n;
+    }
+};
+
 template <int MODE>   // 0: threshold sample pass, 1: emit pass
 __global__ void __launch_bounds__(TC_THREADS, 1)
     knn_tc_scan_kernel(const __grid_constant__ CUtensorMap tmA,
@@ -292,8 +348,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         float L[TC_KS];
 #pragma unroll
         for (int i = 0; i < TC_KS; ++i) L[i] = INFINITY;
+        PendingCands pend;
         for (int j = 0; j < n_my; ++j) {
             const int b = j & 1;
+            if (MODE == 1) pend.flush(a.count, a.cand, a.cmax, qrow);
             const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
             if (__any_sync(0xffffffffu, !got || *abort_flag != 0)) {
                 if (lane == 0) {
@@ -330,21 +388,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 const float lim = MODE == 1 ? thr : L[TC_KS - 1];
                 if (!(min32(v[c]) < lim)) continue;
-                uint32_t m = 0;
-#pragma unroll
-                for (int e = 0; e < 32; ++e) m |= (__uint_as_float(v[c][e]) < lim ? 1u : 0u) << e;
+                uint32_t m = below_mask(v[c], lim);
                 const int cbase = tile * TC_BN + c * 32;
                 while (m) {
                     const int e = __ffs(m) - 1;
                     m &= m - 1;
-                    uint32_t xb = v[c][0];
-#pragma unroll
-                    for (int t = 1; t < 32; ++t) xb = (t == e) ? v[c][t] : xb;
+                    const uint32_t xb = select32(v[c], e);
                     if (MODE == 1) {
-                        const int pos = atomicAdd(&a.count[qrow], 1);
-                        if (pos < a.cmax)
-                            a.cand[(size_t)qrow * a.cmax + pos] =
-                                ((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e);
+                        pend.push(((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e),
+                                  a.count, a.cand, a.cmax, qrow);
                     } else {
                         const float x = __uint_as_float(xb);
                         if (x < L[TC_KS - 1]) {
@@ -357,6 +409,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
             }
         }
+        if (MODE == 1) pend.flush(a.count, a.cand, a.cmax, qrow);
         if (MODE == 0 && !*abort_flag && qrow < a.Q) {
             float *dst = a.p1 + ((size_t)split * a.Q + qrow) * TC_KS;
 #pragma unroll
@@ -388,6 +441,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // barrier on every path.
 // ---------------------------------------------------------------------------
 constexpr int TP_BN = 256;            // reference points per pair tile
+constexpr int TP_EPI_WARPS = 8;       // two per TMEM lane quadrant, 128 columns each
+constexpr int TP_COLS = TP_BN / (TP_EPI_WARPS / 4);   // columns per epilogue warp
+constexpr int TP_CHUNKS = TP_COLS / 32;
+constexpr int TP_THREADS = 32 * (2 + TP_EPI_WARPS);   // warp 0 TMA, warp 1 MMA, epilogue
+constexpr int TP_LISTS = TP_EPI_WARPS / 4;             // pass-1 lists per query and split
 constexpr int TP_STAGES = 8;
 constexpr int TP_NSLOTS = 4;
 constexpr uint32_t TP_IDESC = umma_idesc_bf16(2 * TC_BM, TP_BN);
@@ -406,7 +464,7 @@ struct TpArgs {
     int tile_base, n_tiles, n_splits;   // 256-point tiles [tile_base, tile_base + n_tiles)
     int tile_stride;        // scan tiles t of the split with t % tile_stride == 0
     const float *thr;       // emit pass: [Q] thresholds (a units)
-    float *p1;              // sample pass: [2 n_splits][Q][TC_KS] (per column half)
+    float *p1;              // sample pass: [TP_LISTS n_splits][Q][TC_KS] (per column range)
     unsigned long long *cand;   // [Q][cmax] (a, index) entries
     int *count;             // [Q]
     int cmax;
@@ -414,7 +472,7 @@ struct TpArgs {
 };
 
 template <int MODE>   // 0: threshold sample pass, 1: emit pass
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
     knn_tc_pair_scan_kernel(const __grid_constant__ CUtensorMap tmA,
                             const __grid_constant__ CUtensorMap tmB,
                             const __grid_constant__ CUtensorMap tmN, TpArgs a) {
@@ -448,7 +506,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
     const int first = ((t0 + G - 1) / G) * G;
     const int n_my = first < t1 ? (t1 - first + G - 1) / G : 0;
 
-    for (int i = threadIdx.x; i < TC_BM * TC_NK / 2; i += TC_THREADS)
+    for (int i = threadIdx.x; i < TC_BM * TC_NK / 2; i += TP_THREADS)
         reinterpret_cast<uint32_t *>(sOnes)[i] = 0x3F803F80u;
     fence_proxy_async_smem();
     if (warp == 0 && lane == 0) {
@@ -463,7 +521,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], 2 * TC_EPI_WARPS);
+            mbar_init(&acc_empty[b], 2 * TP_EPI_WARPS);
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -595,9 +653,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
         }
         __syncwarp();
     } else {
-        // ---------------- epilogue (8 warps per CTA) ----------------
-        // Warp w: TMEM lane quadrant w % 4 (32 query rows), column half
-        // (w - 2) / 4 (128 of the tile's 256 reference points).
+        // ---------------- epilogue (TP_EPI_WARPS warps per CTA) ----------------
+        // Warp w: TMEM lane quadrant w % 4 (32 query rows), column range
+        // (w - 2) / 4 (TP_COLS of the tile's 256 reference points).
         const int qd = warp & 3;
         const int hc = (warp - 2) >> 2;
         const int qrow = qpair * TC_QT + (int)rank * TC_BM + qd * 32 + lane;
@@ -606,8 +664,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
         float L[TC_KS];
 #pragma unroll
         for (int i = 0; i < TC_KS; ++i) L[i] = INFINITY;
+        PendingCands pend;
         for (int j = 0; j < n_my; ++j) {
             const int b = j & 1;
+            if (MODE == 1) pend.flush(a.count, a.cand, a.cmax, qrow);
             const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
             if (__any_sync(0xffffffffu, !got || *abort_flag != 0)) {
                 if (lane == 0) {
@@ -619,14 +679,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
             tc_fence_after();
             // the warp's 128 columns in one go; the buffer goes back to the
             // MMA as soon as the values sit in registers
-            uint32_t v[4][32];
+            uint32_t v[TP_CHUNKS][32];
             {
                 const uint32_t tb =
-                    tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * TP_BN + hc * 128);
+                    tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * TP_BN + hc * TP_COLS);
 #pragma unroll
-                for (int c = 0; c < 4; ++c) tmem_ld32(tb + 32 * c, v[c]);
+                for (int c = 0; c < TP_CHUNKS; ++c) tmem_ld32(tb + 32 * c, v[c]);
 #pragma unroll
-                for (int c = 0; c < 4; ++c) tmem_ld_wait(v[c]);
+                for (int c = 0; c < TP_CHUNKS; ++c) tmem_ld_wait(v[c]);
             }
             tc_fence_before();
             __syncwarp();
@@ -636,10 +696,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
                 else
                     mbar_arrive_cluster(mapa_shared(smem_u32(&acc_empty[b]), 0));
             }
-            const int col0 = (first + j * G) * TP_BN + hc * 128;   // first reference of this warp
+            const int col0 = (first + j * G) * TP_BN + hc * TP_COLS;   // first reference of this warp
             const int valid = a.N - col0;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
+            for (int c = 0; c < TP_CHUNKS; ++c) {
                 const int cvalid = valid - c * 32;
                 if (cvalid < 32) {
 #pragma unroll
@@ -648,21 +708,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
                 }
                 const float lim = MODE == 1 ? thr : L[TC_KS - 1];
                 if (!(min32(v[c]) < lim)) continue;
-                uint32_t m = 0;
-#pragma unroll
-                for (int e = 0; e < 32; ++e) m |= (__uint_as_float(v[c][e]) < lim ? 1u : 0u) << e;
+                uint32_t m = below_mask(v[c], lim);
                 const int cbase = col0 + c * 32;
                 while (m) {
                     const int e = __ffs(m) - 1;
                     m &= m - 1;
-                    uint32_t xb = v[c][0];
-#pragma unroll
-                    for (int t = 1; t < 32; ++t) xb = (t == e) ? v[c][t] : xb;
+                    const uint32_t xb = select32(v[c], e);
                     if (MODE == 1) {
-                        const int pos = atomicAdd(&a.count[qrow], 1);
-                        if (pos < a.cmax)
-                            a.cand[(size_t)qrow * a.cmax + pos] =
-                                ((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e);
+                        pend.push(((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e),
+                                  a.count, a.cand, a.cmax, qrow);
                     } else {
                         const float x = __uint_as_float(xb);
                         if (x < L[TC_KS - 1]) {
@@ -675,8 +729,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
                 }
             }
         }
+        if (MODE == 1) pend.flush(a.count, a.cand, a.cmax, qrow);
         if (MODE == 0 && !*abort_flag && qrow < a.Q) {
-            float *dst = a.p1 + ((size_t)(2 * split + hc) * a.Q + qrow) * TC_KS;
+            float *dst = a.p1 + ((size_t)(TP_LISTS * split + hc) * a.Q + qrow) * TC_KS;
 #pragma unroll
             for (int i = 0; i < TC_KS; ++i) dst[i] = L[i];
         }
@@ -1182,7 +1237,7 @@ static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
 size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     const TcPlan p = plan_tc(N, Q, d, k, num_sms);
     size_t b = (size_t)p.qtiles * TC_QT * p.d_pad * 2 + (size_t)Q * 4 * 6 + 16;
-    b += (size_t)2 * p.splits1 * Q * TC_KS * 4;
+    b += (size_t)TP_LISTS * p.splits1 * Q * TC_KS * 4;
     b += (size_t)Q * p.cmax * 8;
     b += fallback_bytes(N, Q, d, k, num_sms);   // worst case: every query uncertified
     return b + 16 * 256;
@@ -1245,7 +1300,7 @@ int emit_scan(const TcRun &r, cudaStream_t st, const __nv_bfloat16 *qB, int Q, c
         a.count = r.count;
         a.cmax = r.cmax;
         a.status = P.status;
-        knn_tc_pair_scan_kernel<1><<<dim3(2 * qtiles, a.n_splits), TC_THREADS, TP_SMEM, st>>>(
+        knn_tc_pair_scan_kernel<1><<<dim3(2 * qtiles, a.n_splits), TP_THREADS, TP_SMEM, st>>>(
             tmA, tmB, tmN, a);
     } else {
         // 128-point tiles of the same range
@@ -1329,7 +1384,7 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     r.fail2 = cv.take<int>(P.Q);
     r.nfail = cv.take<int>(4);
     r.cand_total = cv.take<unsigned long long>(1);
-    r.p1 = cv.take<float>((size_t)2 * p.splits1 * P.Q * TC_KS);
+    r.p1 = cv.take<float>((size_t)TP_LISTS * p.splits1 * P.Q * TC_KS);
     r.cand = cv.take<unsigned long long>((size_t)P.Q * p.cmax);
     r.ldf = (P.Q + 3) / 4 * 4;   // second-chance buffers, sized for all queries
     r.qsub = cv.take<float>((size_t)P.d * r.ldf);
@@ -1379,12 +1434,12 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
     a.count = r.count;
     a.cmax = r.cmax;
     a.status = P.status;
-    knn_tc_pair_scan_kernel<0><<<dim3(2 * r.qtiles, r.splits1), TC_THREADS, TP_SMEM, st>>>(
+    knn_tc_pair_scan_kernel<0><<<dim3(2 * r.qtiles, r.splits1), TP_THREADS, TP_SMEM, st>>>(
         tmA, tmB, tmN, a);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (P.timer) P.timer->mark(st, kPhaseTcPass1);
-    // two lists (column halves) per pair and split; resets the counts
-    tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(r.p1, 2 * r.splits1, P.Q, r.qn,
+    // TP_LISTS lists (column ranges) per pair and split; resets the counts
+    tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(r.p1, TP_LISTS * r.splits1, P.Q, r.qn,
                                                            r.R.rmax_bits, r.d_pad, r.thr,
                                                            r.count);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
