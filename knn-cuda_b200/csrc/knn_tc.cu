@@ -952,8 +952,9 @@ KNN_DI void warp_bitonic_sort(unsigned long long *keys, int P, int lane) {
 // exact distance D_k bounds the true k-th from above, so every point of the
 // true top-k has a < D_k (1+g) + E - ||q||^2 and a second scan emitting below
 // D_k (1+g) + 2.5 E - ||q||^2 passes the check; with fewer than k candidates
-// the threshold is widened by 8 E; an overflowing list gets NaN (no second
-// scan: exact kernel).
+// the threshold is widened by 8 E; an overflowing list keeps its threshold
+// for a second scan with a longer list (final_pass = 0) or gets NaN (exact
+// kernel).
 constexpr int TC_RR_WARPS = 4;
 constexpr int TC_RR_DCH = 64;                 // dimensions per staged chunk
 // padded row (floats): 16-byte aligned, and 16-byte reads of one row per lane
@@ -981,10 +982,10 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
                      int cmax, int cpow, int Q, int k, float *__restrict__ out_dist,
                      int *__restrict__ out_idx, long long ld_out, int *__restrict__ fail_list,
                      int *__restrict__ n_fail, float *__restrict__ retry,
-                     unsigned long long *__restrict__ cand_total) {
+                     unsigned long long *__restrict__ cand_total, int final_pass) {
     extern __shared__ unsigned char rsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int q = blockIdx.x * TC_RR_WARPS + warp;
+    const int q = blockIdx.x * (blockDim.x >> 5) + warp;
     if (q >= Q) return;
     unsigned char *mine = rsm + (size_t)warp * tc_rr_warp_bytes(d_pad, cpow);
     float *qv = reinterpret_cast<float *>(mine);
@@ -1000,9 +1001,11 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
         if (lane == 0) {
             fail_list[atomicAdd(n_fail, 1)] = q;
             // too few candidates: the threshold was low; widen it by 8 E.
-            // An overflowing list goes to the exact kernel (NaN).
+            // An overflowing list is scanned again with the same threshold
+            // and a longer list; overflowing that too, it goes to the exact
+            // kernel (NaN).
             retry[q] = c < k ? T + 8.f * tc_error_bound(qq, r2, T, d_pad)
-                             : __int_as_float(0x7fc00000);
+                             : (final_pass ? __int_as_float(0x7fc00000) : T);
         }
         return;
     }
@@ -1161,9 +1164,13 @@ bool encode_norm_rows(CUtensorMap *m, const void *base, int rows) {
                      (uint64_t)TC_NK, TC_NK, TC_BN, CU_TENSOR_MAP_SWIZZLE_32B);
 }
 
-// Largest candidate-list capacity (rounded to a power of two) of any shape:
-// k <= 128 gives stride1 <= 20 and cmax = 4 * KS * stride1 <= 1280.
-constexpr int kTcCmaxPow2Max = 2048;
+// Candidate lists: first scan cmax = 4 * KS * stride1 (<= 1280 for k <=
+// 128); the second scan of the queries whose list overflowed reuses the
+// whole list buffer, up to kTcCmaxRetry entries per query.  The re-rank
+// kernel's shared memory (keys padded to a power of two) is capped at
+// kRerankSmem per block: fewer warps per block for long lists.
+constexpr int kTcCmaxRetry = 8192;
+constexpr size_t kRerankSmem = 200 * 1024;
 
 struct TcPlan {
     int d_pad, kb, qtiles, stride1, cmax;
@@ -1278,7 +1285,7 @@ namespace {
 // queries whose BF16 copy is qB: CTA pairs (pair = true) or one CTA per 256
 // queries (second-chance scan of few queries).
 int emit_scan(const TcRun &r, cudaStream_t st, const __nv_bfloat16 *qB, int Q, const float *thr,
-              int tb, int te, bool pair) {
+              int cmax, int tb, int te, bool pair) {
     const TcProblem &P = r.P;
     CUtensorMap tmA, tmB, tmN;
     if (!encode_bf16_kmajor(&tmA, qB, Q, r.d_pad)) return kErrTensorMap;
@@ -1298,7 +1305,7 @@ int emit_scan(const TcRun &r, cudaStream_t st, const __nv_bfloat16 *qB, int Q, c
         a.p1 = nullptr;
         a.cand = r.cand;
         a.count = r.count;
-        a.cmax = r.cmax;
+        a.cmax = cmax;
         a.status = P.status;
         knn_tc_pair_scan_kernel<1><<<dim3(2 * qtiles, a.n_splits), TP_THREADS, TP_SMEM, st>>>(
             tmA, tmB, tmN, a);
@@ -1316,7 +1323,7 @@ int emit_scan(const TcRun &r, cudaStream_t st, const __nv_bfloat16 *qB, int Q, c
         a.p1 = nullptr;
         a.cand = r.cand;
         a.count = r.count;
-        a.cmax = r.cmax;
+        a.cmax = cmax;
         a.status = P.status;
         if (tb != 0) return kErrInvalid;   // the single-CTA scan covers the whole set
         knn_tc_scan_kernel<1><<<dim3(qtiles, a.n_splits), TC_THREADS, TC_SMEM, st>>>(
@@ -1325,25 +1332,28 @@ int emit_scan(const TcRun &r, cudaStream_t st, const __nv_bfloat16 *qB, int Q, c
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
-// Exact re-rank + certification of Q queries (see tc_rerank_kernel).
-int rerank(const TcRun &r, cudaStream_t st, int Q, const float *qry, long long ldq,
+// Exact re-rank + certification of Q queries (see tc_rerank_kernel) whose
+// candidate lists have stride cmax.
+int rerank(const TcRun &r, cudaStream_t st, int Q, int cmax, const float *qry, long long ldq,
            const float *qn, const float *thr, float *out_dist, int *out_idx, long long ld_out,
-           int *fail) {
+           int *fail, bool final_pass) {
     const TcProblem &P = r.P;
     if (cudaMemsetAsync(r.nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
     int cpow = 1;
-    while (cpow < r.cmax) cpow <<= 1;
-    const size_t rsmem = TC_RR_WARPS * tc_rr_warp_bytes(r.d_pad, cpow);
-    // one fixed limit (the largest any shape uses) for every launch, so that
-    // calls from several host threads never lower it under each other
-    const size_t rsmem_max = TC_RR_WARPS * tc_rr_warp_bytes(TC_KBMAX * TC_BK, kTcCmaxPow2Max);
-    if (rsmem > rsmem_max ||
+    while (cpow < cmax) cpow <<= 1;
+    int warps = TC_RR_WARPS;
+    while (warps > 1 && (size_t)warps * tc_rr_warp_bytes(r.d_pad, cpow) > kRerankSmem) warps >>= 1;
+    const size_t rsmem = (size_t)warps * tc_rr_warp_bytes(r.d_pad, cpow);
+    // one fixed limit for every launch, so that calls from several host
+    // threads never lower it under each other
+    if (rsmem > kRerankSmem ||
         cudaFuncSetAttribute(tc_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)rsmem_max) != cudaSuccess)
+                             (int)kRerankSmem) != cudaSuccess)
         return kErrLaunch;
-    tc_rerank_kernel<<<(Q + TC_RR_WARPS - 1) / TC_RR_WARPS, TC_RR_WARPS * 32, rsmem, st>>>(
-        r.R.refT, P.d, r.d_pad, qry, ldq, qn, r.R.rmax_bits, thr, r.cand, r.count, r.cmax, cpow,
-        Q, P.k, out_dist, out_idx, ld_out, fail, r.nfail, r.retry, r.cand_total);
+    tc_rerank_kernel<<<(Q + warps - 1) / warps, warps * 32, rsmem, st>>>(
+        r.R.refT, P.d, r.d_pad, qry, ldq, qn, r.R.rmax_bits, thr, r.cand, r.count, cmax, cpow,
+        Q, P.k, out_dist, out_idx, ld_out, fail, r.nfail, r.retry, r.cand_total,
+        final_pass ? 1 : 0);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
@@ -1450,7 +1460,7 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
 int tc_run_pass2(TcRun &r, int tile_begin, int tile_end, cudaStream_t st) {
     tile_end = std::min(tile_end, r.n_tiles2);
     if (tile_begin >= tile_end) return kOk;
-    const int rc = emit_scan(r, st, r.qB, r.P.Q, r.thr, tile_begin, tile_end, true);
+    const int rc = emit_scan(r, st, r.qB, r.P.Q, r.thr, r.cmax, tile_begin, tile_end, true);
     if (rc == kOk && r.P.timer) r.P.timer->mark(st, kPhaseTcPass2);
     return rc;
 }
@@ -1461,8 +1471,8 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     int *host_tmp = host_stats + 2;
     host_stats[0] = host_stats[1] = 0;
     host_stats[4] = host_stats[5] = 0;
-    int rc = rerank(r, st, P.Q, P.qry, P.ldq, r.qn, r.thr, P.out_dist, P.out_idx, P.ld_out,
-                    r.fail);
+    int rc = rerank(r, st, P.Q, r.cmax, P.qry, P.ldq, r.qn, r.thr, P.out_dist, P.out_idx,
+                    P.ld_out, r.fail, false);
     if (rc != kOk) return rc;
     if (tm) tm->mark(st, kPhaseTcRerank);
     int nf = 0;
@@ -1482,9 +1492,12 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
         r.qsub, nf, r.ldf, P.d, r.d_pad, -2.0f, r.qB, nullptr);
     tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(r.fail, nf, r.retry, r.thr, r.count);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-    if ((rc = emit_scan(r, st, r.qB, nf, r.thr, 0, r.n_tiles2, false)) != kOk) return rc;
+    // the compacted queries share the whole list buffer (Q * cmax entries)
+    const int cmax2 = (int)std::min<long long>(
+        kTcCmaxRetry, std::max<long long>(r.cmax, (long long)P.Q * r.cmax / nf));
+    if ((rc = emit_scan(r, st, r.qB, nf, r.thr, cmax2, 0, r.n_tiles2, false)) != kOk) return rc;
     if (tm) tm->mark(st, kPhaseTcRetryScan);
-    rc = rerank(r, st, nf, r.qsub, r.ldf, r.qn, r.thr, r.sd, r.si, r.ldf, r.fail2);
+    rc = rerank(r, st, nf, cmax2, r.qsub, r.ldf, r.qn, r.thr, r.sd, r.si, r.ldf, r.fail2, true);
     if (rc != kOk) return rc;
     if (tm) tm->mark(st, kPhaseTcRetryRerank);
     int nf2 = 0;

@@ -128,6 +128,23 @@ def test_fallback_path_exercised(knncuda, gpu):
     assert np.array_equal(ic, ig)
 
 
+def test_overflowing_lists_rescanned_with_longer_lists(knncuda, gpu):
+    """Clusters whose in-cluster distance spread is below the BF16 error
+    slack: most candidate lists overflow on the first scan; the second scan
+    gives those queries longer lists instead of sending them to the exact
+    kernel.  Results must equal knn_cuda_global bit for bit."""
+    import workloads
+
+    w = workloads.WORKLOADS["mixture128"]
+    ref, query = workloads.generate(w, ref_nb=262144, query_nb=1000)
+    dg, ig = knncuda.knn(ref, query, w.k, "global")
+    dc, ic = knncuda.knn(ref, query, w.k, "cublas")
+    second, exact = knncuda.last_fallback_counts()
+    assert second > 0 and exact < second, (second, exact)
+    assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
+    assert np.array_equal(ic, ig)
+
+
 @pytest.mark.parametrize("n,dim,k", [(262144, 64, 20),     # tile-aligned, 8 whole chunks
                                      (299108, 96, 100),    # ragged last sample tile and chunk
                                      (1 << 20, 256, 100)])  # the headline shape
