@@ -7,8 +7,8 @@
 //   * A CTA owns BQ queries (one query tile) and one contiguous slice
 //     ("split") of the reference set.  Reference tiles of 256 points x 16
 //     dimensions and the matching 16 x BQ query slab are brought into shared
-//     memory by TMA (one producer warp, a 4-stage mbarrier ring).
-//   * 8 consumer warps; warp w owns QPW queries, lane l owns the 8
+//     memory by TMA (one producer warp, a 3-stage mbarrier ring).
+//   * 16 consumer warps; warp w owns QPW queries, lane l owns the 8
 //     reference points {4l..4l+3, 128+4l..128+4l+3} of each tile, so every
 //     lane accumulates a QPW x 8 block of squared distances in registers as
 //     sum_d (r_d - q_d)^2 with one rounding per sub and one fused
@@ -16,12 +16,14 @@
 //     order of the reference's compute_distances inner loop
 //     (code/knncuda.cu:77-80), so squared distances are bit-identical to it.
 //   * Selection is warp-local.  Each query keeps its k smallest
-//     (distance, index) keys sorted in shared memory and a threshold tau =
-//     the k-th key in registers.  After each half tile the warp ballots the
-//     keys below tau into a candidate buffer and merges them into the list by
-//     rank counting (no sort network).  Ordering by the 64-bit key
-//     (distance bits, index) reproduces the reference's tie rule: equal
-//     distances keep the lower index (code/knncuda.cu:172, :178).
+//     (distance, index) keys sorted in shared memory; the k-th key is the
+//     threshold.  After each half tile the warp ballots the keys below it
+//     into a 128-slot candidate buffer, which is merged into the list only
+//     when it would overflow (a register bitonic sort of the buffer, then
+//     every key placed at its index plus its rank in the other array).
+//     Ordering by the 64-bit key (distance bits, index) reproduces the
+//     reference's tie rule: equal distances keep the lower index
+//     (code/knncuda.cu:172, :178).
 //   * With one split the kernel writes sqrt(distance) and the index straight
 //     into the k x query_nb output; with several splits it writes each
 //     split's sorted keys to scratch and knn_merge_splits_kernel merges them.
