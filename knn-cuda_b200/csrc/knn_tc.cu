@@ -51,30 +51,15 @@
 
 namespace knnb200 {
 
-constexpr int TC_BM = 128;            // rows (queries) per MMA tile
-constexpr int TC_QT = 2 * TC_BM;      // queries per CTA (two A tiles share each B tile)
-constexpr int TC_BN = 128;            // reference points per tile
+constexpr int TC_BM = 128;            // rows (queries) per CTA of a pair, points per CTA half-tile
+constexpr int TC_QT = 2 * TC_BM;      // queries per CTA pair
 constexpr int TC_BK = 64;             // K block: 64 bf16 = 128 B (one swizzle row)
 constexpr int TC_KBMAX = 4;           // d_pad <= 256
-constexpr int TC_STAGES = 5;
-constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;   // 16 KB (A or B K-block tile)
+constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;   // 16 KB (A or B K-block tile of one CTA)
 constexpr int TC_NK = 16;             // norm step: K = 16 (h, m, l, 13 zeros)
-constexpr int TC_NORM_BYTES = TC_BN * TC_NK * 2;   // 4 KB norm tile (32-byte swizzle)
-constexpr int TC_NSLOTS = 3;          // norm tiles in flight
+constexpr int TC_NORM_BYTES = TC_BM * TC_NK * 2;   // 4 KB norm tile (32-byte swizzle)
 constexpr int TC_KS = 16;             // pass-1 per-row list length
-constexpr int TC_EPI_WARPS = 8;       // two per TMEM lane quadrant (one per query tile)
-constexpr int TC_THREADS = 32 * (2 + TC_EPI_WARPS);   // warp 0 TMA, warp 1 MMA, 2..9 epilogue
-constexpr uint32_t TC_TMEM_COLS = 512;   // 2 accumulator buffers x 2 A tiles x 128
-constexpr uint32_t TC_IDESC = umma_idesc_bf16(TC_BM, TC_BN);
-
-constexpr size_t TC_OFF_A = 0;
-constexpr size_t TC_OFF_ONES = (size_t)2 * TC_KBMAX * TC_TILE_BYTES;           // 128 KB
-constexpr size_t TC_OFF_B = TC_OFF_ONES + (size_t)TC_BM * TC_NK * 2;           // +4 KB
-constexpr size_t TC_OFF_N = TC_OFF_B + (size_t)TC_STAGES * TC_TILE_BYTES;       // +80 KB
-constexpr size_t TC_OFF_BAR = TC_OFF_N + (size_t)TC_NSLOTS * TC_NORM_BYTES;     // +12 KB
-constexpr int TC_NBARS = 1 + 2 * TC_STAGES + 2 * TC_NSLOTS + 2 + 2 + 1;
-constexpr size_t TC_SMEM = 1024 + TC_OFF_BAR + TC_NBARS * 8 + 16;
-static_assert(TC_SMEM <= 232448, "scan kernel shared memory");
+constexpr uint32_t TC_TMEM_COLS = 512;   // 2 accumulator buffers x 256 columns
 
 // Candidate entries: (order-preserving bits of a) << 32 | reference index,
 // so that unsigned order is (a, index) order for every non-NaN a.
@@ -82,16 +67,6 @@ KNN_DI uint32_t ord_bits(uint32_t f) { return (f & 0x80000000u) ? ~f : (f | 0x80
 KNN_DI float ord_float(uint32_t o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
 }
-
-struct TcArgs {
-    int N, Q, kb_count, n_tiles, n_splits, tile_stride;
-    const float *thr;       // pass 2: [Q] thresholds (a units)
-    float *p1;              // pass 1: [n_splits][Q][TC_KS]
-    unsigned long long *cand;   // pass 2: [Q][cmax] (a, index) entries
-    int *count;             // pass 2: [Q]
-    int cmax;
-    int *status;
-};
 
 // Bit e set iff v[e] < lim: independent compares, then a 3-input OR tree
 // (depth 4) instead of a 32-long dependent chain.
@@ -149,289 +124,17 @@ struct PendingCands {
     }
 };
 
-template <int MODE>   // 0: threshold sample pass, 1: emit pass
-__global__ void __launch_bounds__(TC_THREADS, 1)
-    knn_tc_scan_kernel(const __grid_constant__ CUtensorMap tmA,
-                       const __grid_constant__ CUtensorMap tmB,
-                       const __grid_constant__ CUtensorMap tmN, TcArgs a) {
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char *base = reinterpret_cast<unsigned char *>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char *sA = base + TC_OFF_A;
-    unsigned char *sOnes = base + TC_OFF_ONES;
-    unsigned char *sB = base + TC_OFF_B;
-    unsigned char *sN = base + TC_OFF_N;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(base + TC_OFF_BAR);
-    uint64_t *a_full = bars;
-    uint64_t *b_full = bars + 1;
-    uint64_t *b_empty = b_full + TC_STAGES;
-    uint64_t *n_full = b_empty + TC_STAGES;
-    uint64_t *n_empty = n_full + TC_NSLOTS;
-    uint64_t *acc_full = n_empty + TC_NSLOTS;
-    uint64_t *acc_empty = acc_full + 2;
-    uint64_t *drain = acc_empty + 2;
-    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + TC_NBARS);
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int qtile = blockIdx.x, split = blockIdx.y;
-    const int KB = a.kb_count;
-    // this CTA's reference tiles: [t0, t1) with t % tile_stride == 0
-    const int t0 = (int)((long long)a.n_tiles * split / a.n_splits);
-    const int t1 = (int)((long long)a.n_tiles * (split + 1) / a.n_splits);
-    const int G = a.tile_stride;
-    const int first = ((t0 + G - 1) / G) * G;
-    const int n_my = first < t1 ? (t1 - first + G - 1) / G : 0;
-
-    // the ones tile of the norm step (every element 1.0 bf16, so the
-    // swizzle does not move anything)
-    for (int i = threadIdx.x; i < TC_BM * TC_NK / 2; i += TC_THREADS)
-        reinterpret_cast<uint32_t *>(sOnes)[i] = 0x3F803F80u;
-    fence_proxy_async_smem();
-    if (warp == 0 && lane == 0) {
-        mbar_init(a_full, 1);
-        for (int s = 0; s < TC_STAGES; ++s) {
-            mbar_init(&b_full[s], 1);
-            mbar_init(&b_empty[s], 1);
-        }
-        for (int s = 0; s < TC_NSLOTS; ++s) {
-            mbar_init(&n_full[s], 1);
-            mbar_init(&n_empty[s], 1);
-        }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], TC_EPI_WARPS);
-        }
-        mbar_init(drain, 1);
-        *abort_flag = 0;
-        fence_mbar_init();
-        prefetch_tensormap(&tmA);
-        prefetch_tensormap(&tmB);
-        prefetch_tensormap(&tmN);
-    }
-    if (warp == 1) {
-        tmem_alloc(tmem_holder, TC_TMEM_COLS);
-        tmem_relinquish();
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tmem_holder;
-
-    if (warp == 0) {
-        // ------------------------- TMA producer --------------------------
-        if (lane == 0) {
-            int issued = 0, n_issued = 0;
-            bool a_issued = false, ok = true;
-            if (n_my > 0) {
-                mbar_arrive_expect_tx(a_full, (uint32_t)(2 * KB * TC_TILE_BYTES));
-                for (int h = 0; h < 2; ++h)
-                    for (int kb = 0; kb < KB; ++kb)
-                        tma_load_2d(sA + (size_t)(h * TC_KBMAX + kb) * TC_TILE_BYTES, &tmA, a_full,
-                                    kb * TC_BK, qtile * TC_QT + h * TC_BM);
-                a_issued = true;
-            }
-            for (int j = 0; j < n_my && ok; ++j) {
-                const int row0 = (first + j * G) * TC_BN;
-                const int ns = j % TC_NSLOTS;
-                if (j >= TC_NSLOTS && !mbar_wait(&n_empty[ns], ((j / TC_NSLOTS) - 1) & 1)) {
-                    ok = false;
-                    break;
-                }
-                if (*abort_flag) break;
-                mbar_arrive_expect_tx(&n_full[ns], TC_NORM_BYTES);
-                tma_load_2d(sN + (size_t)ns * TC_NORM_BYTES, &tmN, &n_full[ns], 0, row0);
-                n_issued = j + 1;
-                for (int kb = 0; kb < KB; ++kb) {
-                    const int it = j * KB + kb, s = it % TC_STAGES;
-                    if (it >= TC_STAGES && !mbar_wait(&b_empty[s], ((it / TC_STAGES) - 1) & 1)) {
-                        ok = false;
-                        break;
-                    }
-                    if (*abort_flag) break;
-                    mbar_arrive_expect_tx(&b_full[s], TC_TILE_BYTES);
-                    tma_load_2d(sB + (size_t)s * TC_TILE_BYTES, &tmB, &b_full[s], kb * TC_BK,
-                                row0);
-                    // pull the block two tiles ahead into L2 so the ring's
-                    // loads see L2 rather than DRAM latency
-                    if (j + 2 < n_my)
-                        tma_prefetch_l2_2d(&tmB, kb * TC_BK, (first + (j + 2) * G) * TC_BN);
-                    issued = it + 1;
-                }
-                if (*abort_flag) break;
-            }
-            if (!ok) {
-                atomicMax(a.status, (int)kDevTimeoutEmpty);
-                *abort_flag = 1;
-            }
-            // every TMA write into this CTA's shared memory has landed
-            for (int it = max(0, issued - TC_STAGES); it < issued; ++it)
-                if (!mbar_wait(&b_full[it % TC_STAGES], (it / TC_STAGES) & 1))
-                    atomicMax(a.status, (int)kDevTimeoutDrain);
-            for (int j = max(0, n_issued - TC_NSLOTS); j < n_issued; ++j)
-                if (!mbar_wait(&n_full[j % TC_NSLOTS], (j / TC_NSLOTS) & 1))
-                    atomicMax(a.status, (int)kDevTimeoutDrain);
-            if (a_issued && !mbar_wait(a_full, 0)) atomicMax(a.status, (int)kDevTimeoutDrain);
-        }
-        __syncwarp();
-    } else if (warp == 1) {
-        // ------------------------- MMA issuer ----------------------------
-        if (lane == 0) {
-            bool ok = n_my == 0 || mbar_wait(a_full, 0);
-            bool issued_mma = false;
-            tc_fence_after();
-            const uint64_t odesc = umma_desc_sw32(sOnes);
-            for (int j = 0; j < n_my && ok; ++j) {
-                const int b = j & 1;
-                if (j >= 2 && !mbar_wait(&acc_empty[b], ((j >> 1) - 1) & 1)) {
-                    ok = false;
-                    break;
-                }
-                // norm step first: D = ones x (h, m, l) = ||r||^2 per column
-                const int ns = j % TC_NSLOTS;
-                if (!mbar_wait(&n_full[ns], (j / TC_NSLOTS) & 1) || *abort_flag) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint64_t ndesc = umma_desc_sw32(sN + (size_t)ns * TC_NORM_BYTES);
-#pragma unroll
-                for (int h = 0; h < 2; ++h)
-                    umma_bf16(tmem + (uint32_t)((b * 2 + h) * TC_BM), odesc, ndesc, TC_IDESC, 0u);
-                umma_commit(&n_empty[ns]);
-                issued_mma = true;
-                for (int kb = 0; kb < KB; ++kb) {
-                    const int it = j * KB + kb, s = it % TC_STAGES;
-                    if (!mbar_wait(&b_full[s], (it / TC_STAGES) & 1) || *abort_flag) {
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint64_t bdesc = umma_desc_sw128(sB + (size_t)s * TC_TILE_BYTES);
-#pragma unroll
-                    for (int k = 0; k < TC_BK / 16; ++k) {
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const uint64_t adesc = umma_desc_sw128(
-                                sA + (size_t)(h * TC_KBMAX + kb) * TC_TILE_BYTES);
-                            umma_bf16(tmem + (uint32_t)((b * 2 + h) * TC_BM),
-                                      adesc + (uint64_t)(2 * k), bdesc + (uint64_t)(2 * k),
-                                      TC_IDESC, 1u);
-                        }
-                    }
-                    umma_commit(&b_empty[s]);
-                }
-                if (!ok) break;
-                umma_commit(&acc_full[b]);
-            }
-            if (!ok) {
-                atomicMax(a.status, (int)kDevTimeoutFull);
-                *abort_flag = 1;
-            }
-            // every MMA issued by this thread has completed before teardown
-            if (issued_mma) {
-                umma_commit(drain);
-                if (!mbar_wait(drain, 0)) atomicMax(a.status, (int)kDevTimeoutDrain);
-            }
-        }
-        __syncwarp();
-    } else {
-        // ------------------------- epilogue (8 warps) --------------------
-        // Warp w reads TMEM lane quadrant w % 4 of query tile h = (w - 2) / 4:
-        // one query row per thread, 128 reference columns per tile; the
-        // accumulator already is a = ||r||^2 - 2 r.q.
-        const int qd = warp & 3;
-        const int h = (warp - 2) >> 2;
-        const int qrow = qtile * TC_QT + h * TC_BM + qd * 32 + lane;
-        float thr = -INFINITY;
-        if (MODE == 1 && qrow < a.Q) thr = a.thr[qrow];
-        float L[TC_KS];
-#pragma unroll
-        for (int i = 0; i < TC_KS; ++i) L[i] = INFINITY;
-        PendingCands pend;
-        for (int j = 0; j < n_my; ++j) {
-            const int b = j & 1;
-            if (MODE == 1) pend.flush(a.count, a.cand, a.cmax, qrow);
-            const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
-            if (__any_sync(0xffffffffu, !got || *abort_flag != 0)) {
-                if (lane == 0) {
-                    if (!got) atomicMax(a.status, (int)kDevTimeoutFull);
-                    *abort_flag = 1;
-                }
-                break;
-            }
-            tc_fence_after();
-            // the warp's 128 columns in one go; the buffer goes back to the
-            // MMA as soon as the values sit in registers
-            uint32_t v[4][32];
-            {
-                const uint32_t tb =
-                    tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)((b * 2 + h) * TC_BM);
-#pragma unroll
-                for (int c = 0; c < 4; ++c) tmem_ld32(tb + 32 * c, v[c]);
-#pragma unroll
-                for (int c = 0; c < 4; ++c) tmem_ld_wait(v[c]);
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[b]);
-            const int tile = first + j * G;
-            // columns past the end of the set (zero rows from the TMA fill)
-            const int valid = a.N - tile * TC_BN;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int cvalid = valid - c * 32;
-                if (cvalid < 32) {
-#pragma unroll
-                    for (int e = 0; e < 32; ++e)
-                        if (e >= cvalid) v[c][e] = 0x7f800000u;   // +inf
-                }
-                const float lim = MODE == 1 ? thr : L[TC_KS - 1];
-                if (!(min32(v[c]) < lim)) continue;
-                uint32_t m = below_mask(v[c], lim);
-                const int cbase = tile * TC_BN + c * 32;
-                while (m) {
-                    const int e = __ffs(m) - 1;
-                    m &= m - 1;
-                    const uint32_t xb = select32(v[c], e);
-                    if (MODE == 1) {
-                        pend.push(((unsigned long long)ord_bits(xb) << 32) | (uint32_t)(cbase + e),
-                                  a.count, a.cand, a.cmax, qrow);
-                    } else {
-                        const float x = __uint_as_float(xb);
-                        if (x < L[TC_KS - 1]) {
-#pragma unroll
-                            for (int i = TC_KS - 1; i > 0; --i)
-                                L[i] = x < L[i - 1] ? L[i - 1] : (x < L[i] ? x : L[i]);
-                            L[0] = fminf(L[0], x);
-                        }
-                    }
-                }
-            }
-        }
-        if (MODE == 1) pend.flush(a.count, a.cand, a.cmax, qrow);
-        if (MODE == 0 && !*abort_flag && qrow < a.Q) {
-            float *dst = a.p1 + ((size_t)split * a.Q + qrow) * TC_KS;
-#pragma unroll
-            for (int i = 0; i < TC_KS; ++i) dst[i] = L[i];
-        }
-    }
-
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (warp == 1) tmem_dealloc(tmem, TC_TMEM_COLS);
-}
-
 // ---------------------------------------------------------------------------
-// Pass-2 scan on CTA pairs (cta_group::2).  A cluster of two CTAs owns 256
-// queries (128 per CTA, resident) and walks its reference range in tiles of
-// 256 points, each CTA loading its 128-point half of every K block.  The
-// even CTA issues M = 256, N = 256 MMAs whose operands come from both CTAs'
-// shared memory, so each SM's tensor core reads 8 KB of operands per 1 MFLOP
-// instead of 16 KB (two 128 x 128 MMAs sharing one B tile): the scan is
-// tensor-bound rather than shared-memory-bound.  Each CTA's epilogue reads
-// its own 128 accumulator rows x 256 columns from TMEM.
+// The tensor scan on CTA pairs (cta_group::2): pass 1 (MODE 0, every
+// tile_stride-th tile), pass 2 and the second-chance scan (MODE 1).  A
+// cluster of two CTAs owns 256 queries (128 per CTA, resident) and walks its
+// reference range in tiles of 256 points, each CTA loading its 128-point
+// half of every K block.  The even CTA issues M = 256, N = 256 MMAs whose
+// operands come from both CTAs' shared memory, so each SM's tensor core
+// reads 8 KB of operands per 1 MFLOP instead of the 16 KB of two 128 x 128
+// MMAs sharing one B tile: the scan is tensor-bound rather than
+// shared-memory-bound.  Each CTA's epilogue reads its own 128 accumulator
+// rows x 256 columns from TMEM.
 //
 // Synchronisation: the full barriers live in the even CTA and count the TMA
 // bytes of both CTAs (the even CTA's producer expects both shares); the
@@ -1161,7 +864,7 @@ bool encode_bf16_kmajor(CUtensorMap *m, const void *base, int rows, int d_pad) {
 // Norm-step rows [rows][16] BF16, 128-row boxes with the 32-byte swizzle.
 bool encode_norm_rows(CUtensorMap *m, const void *base, int rows) {
     return encode_2d(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, (uint64_t)TC_NK, (uint64_t)rows,
-                     (uint64_t)TC_NK, TC_NK, TC_BN, CU_TENSOR_MAP_SWIZZLE_32B);
+                     (uint64_t)TC_NK, TC_NK, TC_BM, CU_TENSOR_MAP_SWIZZLE_32B);
 }
 
 // Candidate lists: first scan cmax = 4 * KS * stride1 (<= 1280 for k <=
@@ -1282,53 +985,31 @@ TcRefView tc_carve_ref(void *mem, int N, int d) {
 namespace {
 
 // Emission scan of the reference tiles [tb, te) (256-point tiles) for the Q
-// queries whose BF16 copy is qB: CTA pairs (pair = true) or one CTA per 256
-// queries (second-chance scan of few queries).
+// queries whose BF16 copy is qB, lists of stride cmax.
 int emit_scan(const TcRun &r, cudaStream_t st, const __nv_bfloat16 *qB, int Q, const float *thr,
-              int cmax, int tb, int te, bool pair) {
+              int cmax, int tb, int te) {
     const TcProblem &P = r.P;
     CUtensorMap tmA, tmB, tmN;
     if (!encode_bf16_kmajor(&tmA, qB, Q, r.d_pad)) return kErrTensorMap;
     if (!encode_bf16_kmajor(&tmB, r.R.refB, P.N, r.d_pad)) return kErrTensorMap;
     if (!encode_norm_rows(&tmN, r.R.refN, P.N)) return kErrTensorMap;
     const int qtiles = (Q + TC_QT - 1) / TC_QT;
-    if (pair) {
-        TpArgs a;
-        a.N = P.N;
-        a.Q = Q;
-        a.kb_count = r.kb;
-        a.tile_base = tb;
-        a.n_tiles = te - tb;
-        a.n_splits = choose_splits(qtiles, te - tb, 8, 2.0, std::max(1, P.num_sms / 2));
-        a.tile_stride = 1;
-        a.thr = thr;
-        a.p1 = nullptr;
-        a.cand = r.cand;
-        a.count = r.count;
-        a.cmax = cmax;
-        a.status = P.status;
-        knn_tc_pair_scan_kernel<1><<<dim3(2 * qtiles, a.n_splits), TP_THREADS, TP_SMEM, st>>>(
-            tmA, tmB, tmN, a);
-    } else {
-        // 128-point tiles of the same range
-        const int n_tiles = std::min((P.N + TC_BN - 1) / TC_BN, 2 * te) - 2 * tb;
-        TcArgs a;
-        a.N = P.N;
-        a.Q = Q;
-        a.kb_count = r.kb;
-        a.n_tiles = n_tiles;
-        a.n_splits = choose_splits(qtiles, n_tiles, 16, 2.0, P.num_sms);
-        a.tile_stride = 1;
-        a.thr = thr;
-        a.p1 = nullptr;
-        a.cand = r.cand;
-        a.count = r.count;
-        a.cmax = cmax;
-        a.status = P.status;
-        if (tb != 0) return kErrInvalid;   // the single-CTA scan covers the whole set
-        knn_tc_scan_kernel<1><<<dim3(qtiles, a.n_splits), TC_THREADS, TC_SMEM, st>>>(
-            tmA, tmB, tmN, a);
-    }
+    TpArgs a;
+    a.N = P.N;
+    a.Q = Q;
+    a.kb_count = r.kb;
+    a.tile_base = tb;
+    a.n_tiles = te - tb;
+    a.n_splits = choose_splits(qtiles, te - tb, 8, 2.0, std::max(1, P.num_sms / 2));
+    a.tile_stride = 1;
+    a.thr = thr;
+    a.p1 = nullptr;
+    a.cand = r.cand;
+    a.count = r.count;
+    a.cmax = cmax;
+    a.status = P.status;
+    knn_tc_pair_scan_kernel<1><<<dim3(2 * qtiles, a.n_splits), TP_THREADS, TP_SMEM, st>>>(
+        tmA, tmB, tmN, a);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
@@ -1410,9 +1091,7 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
         P.qry, P.Q, P.ldq, P.d, p.d_pad, -2.0f, r.qB, nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (P.timer) P.timer->mark(st, kPhaseTcPrepQuery);
-    if (cudaFuncSetAttribute(knn_tc_scan_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TC_SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(knn_tc_pair_scan_kernel<0>,
+    if (cudaFuncSetAttribute(knn_tc_pair_scan_kernel<0>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TP_SMEM) != cudaSuccess ||
         cudaFuncSetAttribute(knn_tc_pair_scan_kernel<1>,
@@ -1460,7 +1139,7 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
 int tc_run_pass2(TcRun &r, int tile_begin, int tile_end, cudaStream_t st) {
     tile_end = std::min(tile_end, r.n_tiles2);
     if (tile_begin >= tile_end) return kOk;
-    const int rc = emit_scan(r, st, r.qB, r.P.Q, r.thr, r.cmax, tile_begin, tile_end, true);
+    const int rc = emit_scan(r, st, r.qB, r.P.Q, r.thr, r.cmax, tile_begin, tile_end);
     if (rc == kOk && r.P.timer) r.P.timer->mark(st, kPhaseTcPass2);
     return rc;
 }
@@ -1495,7 +1174,7 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     // the compacted queries share the whole list buffer (Q * cmax entries)
     const int cmax2 = (int)std::min<long long>(
         kTcCmaxRetry, std::max<long long>(r.cmax, (long long)P.Q * r.cmax / nf));
-    if ((rc = emit_scan(r, st, r.qB, nf, r.thr, cmax2, 0, r.n_tiles2, false)) != kOk) return rc;
+    if ((rc = emit_scan(r, st, r.qB, nf, r.thr, cmax2, 0, r.n_tiles2)) != kOk) return rc;
     if (tm) tm->mark(st, kPhaseTcRetryScan);
     rc = rerank(r, st, nf, cmax2, r.qsub, r.ldf, r.qn, r.thr, r.sd, r.si, r.ldf, r.fail2, true);
     if (rc != kOk) return rc;
