@@ -199,6 +199,14 @@ KNNB200_API const char *knnb200_status_string(int code);
  * the roofline denominator of the FP32 direct-form path. */
 KNNB200_API double knnb200_measure_fp32_peak(int iters, void *stream);
 
+/* Self-test of the bounded waits (no counterpart in the reference, whose
+ * kernels have no waits): one warp waits on an mbarrier that nothing
+ * completes, gives up after limit_ns (0 < limit_ns <= 1e9) like every
+ * pipelined kernel of this library does after its own limit, and the call
+ * returns KNNB200_ETIMEOUT with the device context still usable.
+ * KNNB200_OK would mean the wait completed, which cannot happen. */
+KNNB200_API int knnb200_selftest_wait_timeout(long long limit_ns, void *stream);
+
 /* For the last knn_cublas-method call on the current device: the total
  * number of candidates the first tensor-core scan emitted (*candidates), the
  * number of queries that failed the first certification and were scanned a

@@ -75,13 +75,14 @@ KNN_DI bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 // Wait for the phase with the given parity to complete.  Returns false if it
 // did not complete within kWaitLimitNs (the caller records an error and
 // leaves its loop; nothing spins forever).
-KNN_DI bool mbar_wait(uint64_t *bar, uint32_t parity) {
+KNN_DI bool mbar_wait(uint64_t *bar, uint32_t parity,
+                      unsigned long long limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (;;) {
         for (int i = 0; i < 64; ++i)
             if (mbar_try_wait(bar, parity)) return true;
-        if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
     }
 }
 

@@ -1,4 +1,5 @@
-// knn_probe.cu -- FP32 CUDA-core throughput calibration.
+// knn_probe.cu -- FP32 CUDA-core throughput calibration, and a self-test of
+// the bounded waits every pipelined kernel relies on.
 //
 // The exact direct-form path is bound by FP32 CUDA-core issue, a peak that
 // the measured copy-bandwidth / bf16-GEMM peaks do not cover, so the bench
@@ -30,7 +31,42 @@ __global__ void __launch_bounds__(256) ffma_peak_kernel(float *out, int iters, f
     if (s == 12345.678f) out[0] = s;   // keeps the chains live
 }
 
+// One warp waits on an mbarrier that nothing arrives on, through the same
+// bounded wait as the pipelined kernels, with a short limit; on giving up it
+// records the timeout in *status and returns normally.
+__global__ void wait_timeout_selftest_kernel(int *status, unsigned long long limit_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    const bool got = mbar_wait(&bar, 0, limit_ns);
+    if (threadIdx.x == 0) *status = got ? (int)kDevOk : (int)kDevTimeoutFull;
+}
+
 }  // namespace knnb200
+
+extern "C" KNNB200_API int knnb200_selftest_wait_timeout(long long limit_ns, void *stream) {
+    using namespace knnb200;
+    if (limit_ns <= 0 || limit_ns > 1000000000ll) return KNNB200_EINVAL;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return KNNB200_ENODEV;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int *status = nullptr;
+    if (cudaMallocAsync(reinterpret_cast<void **>(&status), sizeof(int), st) != cudaSuccess)
+        return KNNB200_ENOMEM;
+    int h = -1;
+    wait_timeout_selftest_kernel<<<1, 32, 0, st>>>(status, (unsigned long long)limit_ns);
+    const bool ok = cudaGetLastError() == cudaSuccess &&
+                    cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st) ==
+                        cudaSuccess &&
+                    cudaStreamSynchronize(st) == cudaSuccess;
+    cudaFreeAsync(status, st);
+    cudaStreamSynchronize(st);
+    if (!ok) return KNNB200_ECUDA;
+    return h == kDevOk ? KNNB200_OK : KNNB200_ETIMEOUT;
+}
 
 extern "C" KNNB200_API double knnb200_measure_fp32_peak(int iters, void *stream) {
     using namespace knnb200;

@@ -43,7 +43,7 @@ C_SYMBOLS = (
     "knnb200_cuda_global", "knnb200_cuda_texture", "knnb200_cublas", "knnb200_knn_device",
     "knnb200_sync_status", "knnb200_scratch_bytes", "knnb200_plan_splits",
     "knnb200_release_workspace", "knnb200_status_string", "knnb200_version",
-    "knnb200_measure_fp32_peak", "knnb200_last_tc_stats",
+    "knnb200_measure_fp32_peak", "knnb200_last_tc_stats", "knnb200_selftest_wait_timeout",
     "knnb200_knn_device_noalloc", "knnb200_set_phase_timing", "knnb200_last_phase_times",
     "knnb200_refset_create", "knnb200_refset_destroy", "knnb200_refset_device_bytes",
     "knnb200_refset_knn", "knnb200_server_create", "knnb200_server_submit",
@@ -99,6 +99,8 @@ def lib():
         L.knnb200_status_string.argtypes = [ctypes.c_int]
         L.knnb200_measure_fp32_peak.restype = ctypes.c_double
         L.knnb200_measure_fp32_peak.argtypes = [ctypes.c_int, ctypes.c_void_p]
+        L.knnb200_selftest_wait_timeout.restype = ctypes.c_int
+        L.knnb200_selftest_wait_timeout.argtypes = [ctypes.c_longlong, ctypes.c_void_p]
         L.knnb200_knn_device_noalloc.restype = ctypes.c_int
         L.knnb200_knn_device_noalloc.argtypes = [
             ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int,
@@ -460,6 +462,13 @@ def scratch_bytes(ref_nb, query_nb, dim, k, method="global") -> int:
 
 def plan_splits(ref_nb, query_nb, dim, k) -> int:
     return lib().knnb200_plan_splits(ref_nb, query_nb, dim, k)
+
+
+def selftest_wait_timeout(limit_ns: int = 50_000_000) -> int:
+    """Run the bounded-wait self-test (a wait that nothing completes) on the
+    current device's default stream; returns the KNNB200_* code
+    (KNNB200_ETIMEOUT = 5 expected)."""
+    return lib().knnb200_selftest_wait_timeout(int(limit_ns), None)
 
 
 def measure_fp32_peak(iters: int = 4096, stream=None) -> float:
