@@ -254,13 +254,16 @@ int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_h
     t.status = p.status;
     t.num_sms = p.num_sms;
     t.timer = nullptr;
-    TcRun run;
-    int rc = tc_run_begin(t, rv, st, run);
-    if (rc != kOk) return rc;
+    // the translation comes from the sample tiles; the query prep (in
+    // tc_run_begin) needs it
     if (cudaStreamWaitEvent(st, ws.copied[0], 0) != cudaSuccess ||
         cudaMemsetAsync(rv.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess)
         return kErrCuda;
-    if ((rc = tc_prepare_ref_tiles(rv, p.ref, p.N, p.ldr, p.d, 0, n_sample, G, st)) != kOk ||
+    int rc = tc_center_from_tiles(rv, p.ref, p.N, p.ldr, p.d, 4 * G, st);   // sample subset
+    if (rc != kOk) return rc;
+    TcRun run;
+    if ((rc = tc_run_begin(t, rv, st, run)) != kOk ||
+        (rc = tc_prepare_ref_tiles(rv, p.ref, p.N, p.ldr, p.d, 0, n_sample, G, st)) != kOk ||
         (rc = tc_run_pass1(run, st)) != kOk)
         return rc;
     for (int c = 0; c < kStreamChunks; ++c) {

@@ -119,7 +119,8 @@ struct TcRefView {
     __nv_bfloat16 *refB;    // [N][d_pad] BF16, K-major
     float *refT;            // [N][d_pad] FP32 point-major (re-rank gathers)
     __nv_bfloat16 *refN;    // [N][16] squared norm as three BF16 parts, then zeros
-    unsigned *rmax_bits;    // largest squared norm (float bits)
+    unsigned *rmax_bits;    // largest squared norm of ref - center (float bits)
+    float *center;          // [d_pad] translation of both sets before the BF16 expansion
 };
 
 struct TcProblem {
@@ -166,8 +167,13 @@ struct TcRun {
 };
 int tc_tile_points();   // points per tile of the staged API (256)
 int tc_sample_stride(int N, int Q, int d, int k, int num_sms);
+// The translation (center) from every tile_stride-th 256-point tile; must
+// run before any tile is prepared.
+int tc_center_from_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
+                         int tile_stride, cudaStream_t st);
 // Prepare the 256-point tiles tile0 + i * tile_stride, i < n_tiles (the
-// maximum norm accumulates; tc_prepare_ref zeroes it and prepares all).
+// maximum norm accumulates; tc_prepare_ref zeroes it, computes the center
+// and prepares all).
 int tc_prepare_ref_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
                          int tile0, int n_tiles, int tile_stride, cudaStream_t st);
 int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun &run);

@@ -60,6 +60,7 @@ constexpr int TC_NK = 16;             // norm step: K = 16 (h, m, l, 13 zeros)
 constexpr int TC_NORM_BYTES = TC_BM * TC_NK * 2;   // 4 KB norm tile (32-byte swizzle)
 constexpr int TC_KS = 16;             // pass-1 per-row list length
 constexpr uint32_t TC_TMEM_COLS = 512;   // 2 accumulator buffers x 256 columns
+constexpr int kCenterStride = 64;     // the translation is the mean of every 64th tile
 
 // Candidate entries: (order-preserving bits of a) << 32 | reference index,
 // so that unsigned order is (a, index) order for every non-NaN a.
@@ -486,16 +487,17 @@ KNN_DI void write_norm_row(__nv_bfloat16 *parts, int p, float s) {
     dst[1] = row[1];
 }
 
-// Squared norm of each point of a dim x n set (sequential FP32 fma over d)
-// and optionally the largest squared norm (non-negative float bits compare
-// as unsigned).
+// Squared norm of each point of a dim x n set, translated by -center
+// (sequential FP32 fma over d), and optionally the largest squared norm
+// (non-negative float bits compare as unsigned).
 __global__ void tc_norms_kernel(const float *__restrict__ x, int n, long long ld, int d,
-                                float *__restrict__ nrm, unsigned *__restrict__ max_bits) {
+                                const float *__restrict__ center, float *__restrict__ nrm,
+                                unsigned *__restrict__ max_bits) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     float s = 0.f;
     if (p < n) {
         for (int dd = 0; dd < d; ++dd) {
-            const float v = x[(size_t)dd * ld + p];
+            const float v = x[(size_t)dd * ld + p] - center[dd];
             s = fmaf(v, v, s);
         }
         nrm[p] = s;
@@ -506,12 +508,12 @@ __global__ void tc_norms_kernel(const float *__restrict__ x, int n, long long ld
     if ((threadIdx.x & 31) == 0 && max_bits) atomicMax(max_bits, m);
 }
 
-// dim x n (row pitch ld) FP32 -> n x d_pad BF16 of scale * x (scale a power
-// of two, so bf16(scale x) = scale bf16(x)) and optionally FP32 x,
-// zero-padded in [d, d_pad).  32 x 32 tiles through shared memory.
+// dim x n (row pitch ld) FP32 -> n x d_pad BF16 of scale * (x - center)
+// (scale a power of two, so bf16(scale y) = scale bf16(y)), zero-padded in
+// [d, d_pad).  32 x 32 tiles through shared memory.
 __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld, int d,
-                               int d_pad, float scale, __nv_bfloat16 *__restrict__ xb,
-                               float *__restrict__ xt) {
+                               int d_pad, const float *__restrict__ center, float scale,
+                               __nv_bfloat16 *__restrict__ xb) {
     __shared__ float tile[32][33];
     const int p0 = blockIdx.x * 32, d0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -525,26 +527,66 @@ __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld,
     for (int i = 0; i < 4; ++i) {
         const int p = p0 + ty + 8 * i, dd = d0 + tx;
         if (p < n && dd < d_pad) {
-            const float v = tile[tx][ty + 8 * i];
+            const float v = dd < d ? tile[tx][ty + 8 * i] - center[dd] : 0.f;
             xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(v * scale);
-            if (xt) xt[(size_t)p * d_pad + dd] = v;
         }
     }
 }
 
+// The translation c applied to both sets before the BF16 expansion (squared
+// distances do not change, but the expansion's error bound scales with the
+// norms): the mean of the 256-point tiles 0, stride, 2 stride, ... (n_tiles
+// of them), one block per dimension, a fixed-order reduction.  c = 0 in
+// [d, d_pad).
+__global__ void __launch_bounds__(256)
+    tc_center_kernel(const float *__restrict__ x, int n, long long ld, int d, int tile_stride,
+                     int n_tiles, float *__restrict__ center) {
+    __shared__ float part[256];
+    __shared__ int cnt[256];
+    const int dd = blockIdx.x;
+    // thread t sums point t of every sample tile, in four independent chains
+    float s4[4] = {0.f, 0.f, 0.f, 0.f};
+    int c = 0;
+    if (dd < d) {
+        const float *row = x + (size_t)dd * ld;
+#pragma unroll 4
+        for (int t = 0; t < n_tiles; ++t) {
+            const long long p = ((long long)t * tile_stride) * TP_BN + threadIdx.x;
+            if (p < n) {
+                s4[t & 3] += row[p];
+                ++c;
+            }
+        }
+    }
+    part[threadIdx.x] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+    cnt[threadIdx.x] = c;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            part[threadIdx.x] += part[threadIdx.x + h];
+            cnt[threadIdx.x] += cnt[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) center[dd] = cnt[0] > 0 ? part[0] / (float)cnt[0] : 0.f;
+}
+
 // Reference-set prep in one pass over the input: point-major BF16 and FP32
-// copies (zero-padded to d_pad) plus the norm-step row and the largest
-// squared norm, for the 256-point tiles tile0 + i * tile_stride (eight
+// copies (zero-padded to d_pad; the BF16 one of x - center, the FP32 one of
+// x itself) plus the norm-step row and the largest squared norm of
+// x - center, for the 256-point tiles tile0 + i * tile_stride (eight
 // blocks per tile).  A block owns 32 points and walks the dimensions in
 // 32 x 32 tiles through shared memory (coalesced on both sides); one thread
 // per point accumulates the squared norm in increasing d with FP32 fma, the
 // order tc_norms_kernel uses.
 __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long ld, int d,
                                    int d_pad, int tile0, int tile_stride,
+                                   const float *__restrict__ center,
                                    __nv_bfloat16 *__restrict__ xb, float *__restrict__ xt,
                                    __nv_bfloat16 *__restrict__ parts,
                                    unsigned *__restrict__ max_bits) {
     __shared__ float tile[32][33];
+    __shared__ float cs[32];   // the chunk's translation
     const int p0 = (tile0 + (int)(blockIdx.x >> 3) * tile_stride) * TP_BN + (blockIdx.x & 7) * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     float s = 0.f;
@@ -554,17 +596,21 @@ __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long
             const int dd = d0 + ty + 8 * i, p = p0 + tx;
             tile[ty + 8 * i][tx] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
         }
+        if (ty == 1) cs[tx] = d0 + tx < d ? center[d0 + tx] : 0.f;
         __syncthreads();
         if (ty == 0) {
             const int dm = min(32, d - d0);
-            for (int dd = 0; dd < dm; ++dd) s = fmaf(tile[dd][tx], tile[dd][tx], s);
+            for (int dd = 0; dd < dm; ++dd) {
+                const float v = tile[dd][tx] - cs[dd];
+                s = fmaf(v, v, s);
+            }
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int p = p0 + ty + 8 * i, dd = d0 + tx;
             if (p < n) {
                 const float v = tile[tx][ty + 8 * i];
-                xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(v);
+                xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(dd < d ? v - cs[tx] : 0.f);
                 xt[(size_t)p * d_pad + dd] = v;
             }
         }
@@ -935,7 +981,8 @@ bool tc_supported(int N, int Q, int d, int k) {
 
 size_t tc_ref_bytes(int N, int d) {
     const int d_pad = (d + 63) / 64 * 64;
-    return (size_t)N * d_pad * 2 + (size_t)N * d_pad * 4 + (size_t)N * TC_NK * 2 + 4 * 256;
+    return (size_t)N * d_pad * 2 + (size_t)N * d_pad * 4 + (size_t)N * TC_NK * 2 +
+           (size_t)d_pad * 4 + 5 * 256;
 }
 
 static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
@@ -956,7 +1003,17 @@ size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
 int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, int d,
                    cudaStream_t st) {
     if (cudaMemsetAsync(v.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess) return kErrCuda;
-    return tc_prepare_ref_tiles(v, ref, N, ldr, d, 0, (N + TP_BN - 1) / TP_BN, 1, st);
+    const int n_tiles = (N + TP_BN - 1) / TP_BN;
+    const int rc = tc_center_from_tiles(v, ref, N, ldr, d, kCenterStride, st);
+    return rc != kOk ? rc : tc_prepare_ref_tiles(v, ref, N, ldr, d, 0, n_tiles, 1, st);
+}
+
+int tc_center_from_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
+                         int tile_stride, cudaStream_t st) {
+    const int d_pad = (d + 63) / 64 * 64;
+    const int n_sample = ((N + TP_BN - 1) / TP_BN + tile_stride - 1) / tile_stride;
+    tc_center_kernel<<<d_pad, 256, 0, st>>>(ref, N, ldr, d, tile_stride, n_sample, v.center);
+    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
 int tc_prepare_ref_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
@@ -964,8 +1021,8 @@ int tc_prepare_ref_tiles(const TcRefView &v, const float *ref, int N, long long 
     if (n_tiles <= 0) return kOk;
     const int d_pad = (d + 63) / 64 * 64;
     tc_prep_ref_kernel<<<n_tiles * 8, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, tile0,
-                                                            tile_stride, v.refB, v.refT, v.refN,
-                                                            v.rmax_bits);
+                                                            tile_stride, v.center, v.refB, v.refT,
+                                                            v.refN, v.rmax_bits);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
@@ -979,6 +1036,7 @@ TcRefView tc_carve_ref(void *mem, int N, int d) {
     v.refT = cv.take<float>((size_t)N * d_pad);
     v.refN = cv.take<__nv_bfloat16>((size_t)N * TC_NK);
     v.rmax_bits = cv.take<unsigned>(1);
+    v.center = cv.take<float>(d_pad);
     return v;
 }
 
@@ -1086,9 +1144,10 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     r.xcap = P.scratch_bytes - cv.used;
 
     // queries: norms + BF16 K-major copy of -2 q
-    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, r.qn, nullptr);
+    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, R.center, r.qn,
+                                                       nullptr);
     tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
-        P.qry, P.Q, P.ldq, P.d, p.d_pad, -2.0f, r.qB, nullptr);
+        P.qry, P.Q, P.ldq, P.d, p.d_pad, R.center, -2.0f, r.qB);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (P.timer) P.timer->mark(st, kPhaseTcPrepQuery);
     if (cudaFuncSetAttribute(knn_tc_pair_scan_kernel<0>,
@@ -1166,9 +1225,10 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     // thresholds that certify (list overflows excepted)
     gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, r.fail,
                                                                        nf, r.qsub, r.ldf);
-    tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(r.qsub, nf, r.ldf, P.d, r.qn, nullptr);
+    tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(r.qsub, nf, r.ldf, P.d, r.R.center, r.qn,
+                                                      nullptr);
     tc_pack_kernel<<<dim3((nf + 31) / 32, r.d_pad / 32), dim3(32, 8), 0, st>>>(
-        r.qsub, nf, r.ldf, P.d, r.d_pad, -2.0f, r.qB, nullptr);
+        r.qsub, nf, r.ldf, P.d, r.d_pad, r.R.center, -2.0f, r.qB);
     tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(r.fail, nf, r.retry, r.thr, r.count);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     // the compacted queries share the whole list buffer (Q * cmax entries)

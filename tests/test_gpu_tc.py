@@ -114,16 +114,46 @@ def test_device_entry_cublas(knncuda, gpu):
     assert np.array_equal(i.cpu().numpy(), hi)
 
 
+def _far_clusters(seed, dim, n, centres, radius, sigma):
+    """Tight clusters around centres in random directions at distance radius
+    from the origin: the set's mean is near 0, so translating it does not
+    shrink the norms, while in-cluster distances are tiny against them."""
+    rng = np.random.default_rng(seed)
+    c = rng.standard_normal((dim, centres))
+    c *= radius / np.linalg.norm(c, axis=0, keepdims=True)
+    pick = rng.integers(0, centres, size=n)
+    x = c[:, pick] + sigma * rng.standard_normal((dim, n))
+    return np.ascontiguousarray(x, dtype=np.float32)
+
+
 def test_fallback_path_exercised(knncuda, gpu):
-    """Uniform data in 256-d with a small reference set: the BF16 error bound
-    is wide relative to the gaps, so many queries miss the first certification
-    and take the second scan (and possibly the exact kernel); results must
-    still equal knn_cuda_global."""
-    ref, query = _uniform(31, 256, 32768, 400)
+    """16 tight clusters at radius 6 in 256-d: the BF16 error bound exceeds
+    the in-cluster spread, every point of the query's cluster becomes a
+    candidate and the lists overflow, so queries take the second scan (and
+    the exact kernel); results must still equal knn_cuda_global."""
+    ref = _far_clusters(31, 256, 32768, 16, 6.0, 0.05)
+    query = _far_clusters(31, 256, 32768 + 400, 16, 6.0, 0.05)[:, 32768:].copy()
     dg, ig = knncuda.knn(ref, query, 100, "global")
     dc, ic = knncuda.knn(ref, query, 100, "cublas")
     second, exact = knncuda.last_fallback_counts()
     assert second > 0 and exact <= second
+    assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
+    assert np.array_equal(ic, ig)
+
+
+def test_offset_data_is_translated_before_the_bf16_scan(knncuda, gpu):
+    """All coordinates in [50, 51): norms are ~100x the distances, so the BF16
+    expansion's error bound would swallow every distance gap.  The scan works
+    on both sets translated by a sample mean (distances unchanged), so the
+    queries certify without the exact kernel, and results equal
+    knn_cuda_global bit for bit."""
+    rng = np.random.default_rng(37)
+    ref = (rng.random((64, 65536), dtype=np.float32) + np.float32(50)).astype(np.float32)
+    query = (rng.random((64, 300), dtype=np.float32) + np.float32(50)).astype(np.float32)
+    dg, ig = knncuda.knn(ref, query, 20, "global")
+    dc, ic = knncuda.knn(ref, query, 20, "cublas")
+    second, exact = knncuda.last_fallback_counts()
+    assert exact == 0, (second, exact)
     assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
     assert np.array_equal(ic, ig)
 
