@@ -86,9 +86,13 @@ struct Buffer {
 };
 
 // Host entry of knn_cublas on large sets: the reference set is copied in
-// this many chunks (after a strided sample for the threshold pass), each
-// chunk's prep and scan overlapping the copy of the next.
+// this many chunks (after the sample runs of the threshold pass), each
+// chunk's prep and scan overlapping the copy of the next.  Relative chunk
+// sizes: the last ones shrink so that little scanning is left once the last
+// byte has landed (each chunk's scan still ends before the next chunk's
+// copy: the scan runs about 2.5x faster than the copy).
 constexpr int kStreamChunks = 8;
+constexpr int kStreamWeights[kStreamChunks] = {8, 8, 8, 8, 6, 4, 2, 1};
 constexpr int kStreamMinPoints = 1 << 18;
 
 struct Workspace {
@@ -183,13 +187,32 @@ int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st) 
     return launch_tc(t, rv, st, ws.tc_stats);
 }
 
+// Calls fn(g0, g1) for each maximal range of tiles [g0, g1) of [tb, te)
+// outside the runs of the sample pattern s.
+template <class F>
+int for_each_gap(const TileRuns &s, int tb, int te, F fn) {
+    int t = tb;
+    while (t < te) {
+        const int r0 = (t / s.period) * s.period;   // first tile of this period's run
+        if (t < r0 + s.run) {
+            t = std::min(te, r0 + s.run);
+            continue;
+        }
+        const int g1 = std::min(te, r0 + s.period);
+        const int rc = fn(t, g1);
+        if (rc != kOk) return rc;
+        t = g1;
+    }
+    return kOk;
+}
+
 // knn_cublas from pinned host memory: the reference set streams in on the
-// copy stream -- first every sample-stride-th 256-point tile (pass 1 needs
-// only those), then kStreamChunks contiguous chunks -- and the compute
-// stream prepares and scans each piece once its copy has landed, so the
-// copy of the set overlaps the threshold pass and the pass-2 scan of all
-// but the last chunk.  Sample tiles are copied twice (once in the sample,
-// once in their chunk); the second copy writes the same bytes.
+// copy stream -- first the sample runs of the threshold pass (runs of
+// consecutive 256-point tiles, one 2-D copy per run), then kStreamChunks
+// contiguous chunks without those runs -- and the compute stream prepares
+// and scans each piece once its copy has landed, so the copy of the set
+// overlaps the threshold pass and the pass-2 scan of all but the last
+// (smallest) chunk.  Every byte crosses the bus once.
 int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_host,
                         cudaStream_t st) {
     for (int i = 0; i < 8; ++i) ws.tc_stats[i] = 0;
@@ -199,41 +222,38 @@ int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_h
     float *ref_d = const_cast<float *>(p.ref);
     const int T = tc_tile_points();
     const int n_tiles = (p.N + T - 1) / T;
-    const int G = tc_sample_stride(p.N, p.Q, p.d, p.k, p.num_sms);
+    const TileRuns sample = tc_sample_runs(p.N, p.Q, p.d, p.k, p.num_sms);
     const size_t fb = sizeof(float);
     cudaStream_t cs = ws.copy_stream;
+    // points [t0 T, t1 T) of every dimension, one 2-D copy
+    auto copy_tiles = [&](int t0, int t1) -> int {
+        const size_t p0 = (size_t)t0 * T, p1 = std::min<size_t>(p.N, (size_t)t1 * T);
+        if (p0 >= p1) return kOk;
+        return cudaMemcpy2DAsync(ref_d + p0, (size_t)p.ldr * fb, ref_host + p0, (size_t)p.N * fb,
+                                 (p1 - p0) * fb, p.d, cudaMemcpyHostToDevice,
+                                 cs) == cudaSuccess
+                   ? kOk
+                   : kErrCuda;
+    };
     // the copies start after everything queued so far on the compute stream
     // (an earlier call may still read the reference buffer)
     if (cudaEventRecord(ws.last_done, st) != cudaSuccess ||
         cudaStreamWaitEvent(cs, ws.last_done, 0) != cudaSuccess)
         return kErrCuda;
-    // sample tiles 0, G, 2G, ...: whole tiles by one 2-D copy per dimension,
-    // a ragged last tile separately
-    const int n_sample = (n_tiles + G - 1) / G;
-    const int last = (n_sample - 1) * G;
-    const bool ragged = (long long)(last + 1) * T > p.N;
-    const int n_whole = ragged ? n_sample - 1 : n_sample;
-    for (int dd = 0; dd < p.d; ++dd) {
-        float *dst = ref_d + (size_t)dd * p.ldr;
-        const float *src = ref_host + (size_t)dd * p.N;
-        if (n_whole > 0 &&
-            cudaMemcpy2DAsync(dst, (size_t)G * T * fb, src, (size_t)G * T * fb, (size_t)T * fb,
-                              n_whole, cudaMemcpyHostToDevice, cs) != cudaSuccess)
-            return kErrCuda;
-        if (ragged && cudaMemcpyAsync(dst + (size_t)last * T, src + (size_t)last * T,
-                                      ((size_t)p.N - (size_t)last * T) * fb,
-                                      cudaMemcpyHostToDevice, cs) != cudaSuccess)
-            return kErrCuda;
-    }
+    int rc = kOk;
+    for (int t = 0; t < n_tiles && rc == kOk; t += sample.period)
+        rc = copy_tiles(t, std::min(n_tiles, t + sample.run));
+    if (rc != kOk) return rc;
     if (cudaEventRecord(ws.copied[0], cs) != cudaSuccess) return kErrCuda;
-    const int per_chunk = (n_tiles + kStreamChunks - 1) / kStreamChunks;
+    int bound[kStreamChunks + 1], wsum = 0;
+    for (int c = 0; c < kStreamChunks; ++c) wsum += kStreamWeights[c];
+    bound[0] = 0;
+    for (int c = 0, acc = 0; c < kStreamChunks; ++c) {
+        acc += kStreamWeights[c];
+        bound[c + 1] = (int)((long long)n_tiles * acc / wsum);
+    }
     for (int c = 0; c < kStreamChunks; ++c) {
-        const long long p0 = (long long)c * per_chunk * T;
-        const long long p1 = std::min<long long>(p.N, (long long)(c + 1) * per_chunk * T);
-        if (p0 < p1 && cudaMemcpy2DAsync(ref_d + p0, (size_t)p.ldr * fb, ref_host + p0,
-                                         (size_t)p.N * fb, (size_t)(p1 - p0) * fb, p.d,
-                                         cudaMemcpyHostToDevice, cs) != cudaSuccess)
-            return kErrCuda;
+        if ((rc = for_each_gap(sample, bound[c], bound[c + 1], copy_tiles)) != kOk) return rc;
         if (cudaEventRecord(ws.copied[1 + c], cs) != cudaSuccess) return kErrCuda;
     }
 
@@ -254,24 +274,25 @@ int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_h
     t.status = p.status;
     t.num_sms = p.num_sms;
     t.timer = nullptr;
-    // the translation comes from the sample tiles; the query prep (in
-    // tc_run_begin) needs it
+    // the translation comes from every fourth sample tile; the query prep
+    // (in tc_run_begin) needs it
     if (cudaStreamWaitEvent(st, ws.copied[0], 0) != cudaSuccess ||
         cudaMemsetAsync(rv.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess)
         return kErrCuda;
-    int rc = tc_center_from_tiles(rv, p.ref, p.N, p.ldr, p.d, 4 * G, st);   // sample subset
-    if (rc != kOk) return rc;
+    if ((rc = tc_center_from_tiles(rv, p.ref, p.N, p.ldr, p.d, sample, 4, st)) != kOk) return rc;
     TcRun run;
     if ((rc = tc_run_begin(t, rv, st, run)) != kOk ||
-        (rc = tc_prepare_ref_tiles(rv, p.ref, p.N, p.ldr, p.d, 0, n_sample, G, st)) != kOk ||
+        (rc = tc_prepare_ref_tiles(rv, p.ref, p.N, p.ldr, p.d, 0, sample, st)) != kOk ||
         (rc = tc_run_pass1(run, st)) != kOk)
         return rc;
+    auto prep_tiles = [&](int t0, int t1) {
+        return tc_prepare_ref_tiles(rv, p.ref, p.N, p.ldr, p.d, t0, contiguous_tiles(t1 - t0), st);
+    };
     for (int c = 0; c < kStreamChunks; ++c) {
-        const int tb = c * per_chunk, te = std::min(n_tiles, (c + 1) * per_chunk);
         if (cudaStreamWaitEvent(st, ws.copied[1 + c], 0) != cudaSuccess) return kErrCuda;
-        if (tb >= te) continue;
-        if ((rc = tc_prepare_ref_tiles(rv, p.ref, p.N, p.ldr, p.d, tb, te - tb, 1, st)) != kOk ||
-            (rc = tc_run_pass2(run, tb, te, st)) != kOk)
+        if (bound[c] >= bound[c + 1]) continue;
+        if ((rc = for_each_gap(sample, bound[c], bound[c + 1], prep_tiles)) != kOk ||
+            (rc = tc_run_pass2(run, bound[c], bound[c + 1], st)) != kOk)
             return rc;
     }
     return tc_run_finish(run, st, ws.tc_stats);

@@ -141,6 +141,19 @@ struct TcProblem {
     PhaseTimer *timer = nullptr;
 };
 
+// A sample of the 256-point tiles: `run` consecutive tiles out of every
+// `period` (unit u is tile (u / run) * period + u % run), `units` of them.
+// Runs rather than single tiles keep the host-to-device copy of a sample in
+// long contiguous segments.
+struct TileRuns {
+    int run, period, units;
+    __host__ __device__ int tile(int u) const { return (u / run) * period + u % run; }
+    // units of the pattern among the tiles [0, t)
+    __host__ __device__ int count_below(int t) const {
+        return (t / period) * run + (t % period < run ? t % period : run);
+    }
+};
+
 bool tc_supported(int N, int Q, int d, int k);
 size_t tc_ref_bytes(int N, int d);
 size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms);
@@ -149,14 +162,15 @@ int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, i
                    cudaStream_t st);
 // Staged form of launch_tc, for callers that stream the reference set in:
 // tc_run_begin (scratch carve, query prep), tc_run_pass1 (threshold sample:
-// every tc_sample_stride-th 256-point tile must be prepared), tc_run_pass2
-// over 256-point tile ranges as they become ready (each range prepared),
-// tc_run_finish (re-rank, certification, second chance; every tile prepared
-// and the maximum norm final).  launch_tc = all four over the whole set.
+// the tiles of tc_sample_runs must be prepared), tc_run_pass2 over 256-point
+// tile ranges as they become ready (each range prepared), tc_run_finish
+// (re-rank, certification, second chance; every tile prepared and the
+// maximum norm final).  launch_tc = all four over the whole set.
 struct TcRun {
     TcProblem P;
     TcRefView R;
-    int d_pad, kb, qtiles, n_tiles2, splits1, stride1, cmax;
+    TileRuns sample;
+    int d_pad, kb, qtiles, n_tiles2, splits1, cmax;
     long long ldf;
     __nv_bfloat16 *qB;
     float *qn, *thr, *retry, *p1, *qsub, *sd;
@@ -166,16 +180,18 @@ struct TcRun {
     size_t xcap;
 };
 int tc_tile_points();   // points per tile of the staged API (256)
-int tc_sample_stride(int N, int Q, int d, int k, int num_sms);
-// The translation (center) from every tile_stride-th 256-point tile; must
-// run before any tile is prepared.
+TileRuns tc_sample_runs(int N, int Q, int d, int k, int num_sms);
+// The translation (center) from the tiles of units 0, step, 2 step, ... of
+// `tiles`; must run before any tile is prepared.
 int tc_center_from_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
-                         int tile_stride, cudaStream_t st);
-// Prepare the 256-point tiles tile0 + i * tile_stride, i < n_tiles (the
-// maximum norm accumulates; tc_prepare_ref zeroes it, computes the center
-// and prepares all).
+                         const TileRuns &tiles, int step, cudaStream_t st);
+// Prepare the tiles tile0 + tiles.tile(u), u < tiles.units (the maximum
+// norm accumulates; tc_prepare_ref zeroes it, computes the center and
+// prepares all).
 int tc_prepare_ref_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
-                         int tile0, int n_tiles, int tile_stride, cudaStream_t st);
+                         int tile0, const TileRuns &tiles, cudaStream_t st);
+// Every tile of [tile0, tile0 + n) as a pattern.
+inline TileRuns contiguous_tiles(int n) { return TileRuns{1, 1, n}; }
 int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun &run);
 int tc_run_pass1(TcRun &run, cudaStream_t st);
 int tc_run_pass2(TcRun &run, int tile_begin, int tile_end, cudaStream_t st);

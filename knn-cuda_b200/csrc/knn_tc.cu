@@ -126,8 +126,8 @@ struct PendingCands {
 };
 
 // ---------------------------------------------------------------------------
-// The tensor scan on CTA pairs (cta_group::2): pass 1 (MODE 0, every
-// tile_stride-th tile), pass 2 and the second-chance scan (MODE 1).  A
+// The tensor scan on CTA pairs (cta_group::2): pass 1 (MODE 0, the tiles
+// of a sample pattern), pass 2 and the second-chance scan (MODE 1).  A
 // cluster of two CTAs owns 256 queries (128 per CTA, resident) and walks its
 // reference range in tiles of 256 points, each CTA loading its 128-point
 // half of every K block.  The even CTA issues M = 256, N = 256 MMAs whose
@@ -165,8 +165,8 @@ static_assert(TP_SMEM <= 232448, "pair scan kernel shared memory");
 
 struct TpArgs {
     int N, Q, kb_count;
-    int tile_base, n_tiles, n_splits;   // 256-point tiles [tile_base, tile_base + n_tiles)
-    int tile_stride;        // scan tiles t of the split with t % tile_stride == 0
+    int tile_base, n_splits;
+    TileRuns tiles;         // scan tiles tile_base + tiles.tile(u), u < tiles.units
     const float *thr;       // emit pass: [Q] thresholds (a units)
     float *p1;              // sample pass: [TP_LISTS n_splits][Q][TC_KS] (per column range)
     unsigned long long *cand;   // [Q][cmax] (a, index) entries
@@ -204,11 +204,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
     const bool lead = rank == 0;
     const int qpair = blockIdx.x >> 1, split = blockIdx.y;
     const int KB = a.kb_count;
-    const int t0 = a.tile_base + (int)((long long)a.n_tiles * split / a.n_splits);
-    const int t1 = a.tile_base + (int)((long long)a.n_tiles * (split + 1) / a.n_splits);
-    const int G = a.tile_stride;
-    const int first = ((t0 + G - 1) / G) * G;
-    const int n_my = first < t1 ? (t1 - first + G - 1) / G : 0;
+    // this split's units [u0, u0 + n_my)
+    const int u0 = (int)((long long)a.tiles.units * split / a.n_splits);
+    const int n_my = (int)((long long)a.tiles.units * (split + 1) / a.n_splits) - u0;
 
     for (int i = threadIdx.x; i < TC_BM * TC_NK / 2; i += TP_THREADS)
         reinterpret_cast<uint32_t *>(sOnes)[i] = 0x3F803F80u;
@@ -259,7 +257,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                 a_issued = true;
             }
             for (int j = 0; j < n_my && ok; ++j) {
-                const int row0 = (first + j * G) * TP_BN + half_row;
+                const int row0 = (a.tile_base + a.tiles.tile(u0 + j)) * TP_BN + half_row;
                 const int ns = j % TP_NSLOTS;
                 if (j >= TP_NSLOTS && !mbar_wait(&n_empty[ns], ((j / TP_NSLOTS) - 1) & 1)) {
                     ok = false;
@@ -270,6 +268,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                 tma_load_2d_pair(sN + (size_t)ns * TC_NORM_BYTES, &tmN,
                                  mapa_shared(smem_u32(&n_full[ns]), 0), 0, row0);
                 n_issued = j + 1;
+                const int row_ahead = j + 2 < n_my
+                                          ? (a.tile_base + a.tiles.tile(u0 + j + 2)) * TP_BN + half_row
+                                          : a.N;
                 for (int kb = 0; kb < KB; ++kb) {
                     const int it = j * KB + kb, s = it % TP_STAGES;
                     if (it >= TP_STAGES && !mbar_wait(&b_empty[s], ((it / TP_STAGES) - 1) & 1)) {
@@ -280,8 +281,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                     if (lead) mbar_arrive_expect_tx(&b_full[s], 2 * TC_TILE_BYTES);
                     tma_load_2d_pair(sB + (size_t)s * TC_TILE_BYTES, &tmB,
                                      mapa_shared(smem_u32(&b_full[s]), 0), kb * TC_BK, row0);
-                    if (j + 2 < n_my && row0 + 2 * G * TP_BN < a.N)
-                        tma_prefetch_l2_2d(&tmB, kb * TC_BK, row0 + 2 * G * TP_BN);
+                    if (row_ahead < a.N) tma_prefetch_l2_2d(&tmB, kb * TC_BK, row_ahead);
                     issued = it + 1;
                 }
                 if (*abort_flag) break;
@@ -400,7 +400,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                 else
                     mbar_arrive_cluster(mapa_shared(smem_u32(&acc_empty[b]), 0));
             }
-            const int col0 = (first + j * G) * TP_BN + hc * TP_COLS;   // first reference of this warp
+            // first reference of this warp
+            const int col0 = (a.tile_base + a.tiles.tile(u0 + j)) * TP_BN + hc * TP_COLS;
             const int valid = a.N - col0;
 #pragma unroll
             for (int c = 0; c < TP_CHUNKS; ++c) {
@@ -535,12 +536,12 @@ __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld,
 
 // The translation c applied to both sets before the BF16 expansion (squared
 // distances do not change, but the expansion's error bound scales with the
-// norms): the mean of the 256-point tiles 0, stride, 2 stride, ... (n_tiles
-// of them), one block per dimension, a fixed-order reduction.  c = 0 in
-// [d, d_pad).
+// norms): the mean of the 256-point tiles of units 0, step, 2 step, ... of
+// a tile pattern (n_used of them), one block per dimension, a fixed-order
+// reduction.  c = 0 in [d, d_pad).
 __global__ void __launch_bounds__(256)
-    tc_center_kernel(const float *__restrict__ x, int n, long long ld, int d, int tile_stride,
-                     int n_tiles, float *__restrict__ center) {
+    tc_center_kernel(const float *__restrict__ x, int n, long long ld, int d, TileRuns tiles,
+                     int step, int n_used, float *__restrict__ center) {
     __shared__ float part[256];
     __shared__ int cnt[256];
     const int dd = blockIdx.x;
@@ -550,8 +551,8 @@ __global__ void __launch_bounds__(256)
     if (dd < d) {
         const float *row = x + (size_t)dd * ld;
 #pragma unroll 4
-        for (int t = 0; t < n_tiles; ++t) {
-            const long long p = ((long long)t * tile_stride) * TP_BN + threadIdx.x;
+        for (int t = 0; t < n_used; ++t) {
+            const long long p = (long long)tiles.tile(t * step) * TP_BN + threadIdx.x;
             if (p < n) {
                 s4[t & 3] += row[p];
                 ++c;
@@ -574,20 +575,20 @@ __global__ void __launch_bounds__(256)
 // Reference-set prep in one pass over the input: point-major BF16 and FP32
 // copies (zero-padded to d_pad; the BF16 one of x - center, the FP32 one of
 // x itself) plus the norm-step row and the largest squared norm of
-// x - center, for the 256-point tiles tile0 + i * tile_stride (eight
-// blocks per tile).  A block owns 32 points and walks the dimensions in
+// x - center, for the 256-point tiles tile0 + tiles.tile(u) (eight blocks
+// per tile).  A block owns 32 points and walks the dimensions in
 // 32 x 32 tiles through shared memory (coalesced on both sides); one thread
 // per point accumulates the squared norm in increasing d with FP32 fma, the
 // order tc_norms_kernel uses.
 __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long ld, int d,
-                                   int d_pad, int tile0, int tile_stride,
+                                   int d_pad, int tile0, TileRuns tiles,
                                    const float *__restrict__ center,
                                    __nv_bfloat16 *__restrict__ xb, float *__restrict__ xt,
                                    __nv_bfloat16 *__restrict__ parts,
                                    unsigned *__restrict__ max_bits) {
     __shared__ float tile[32][33];
     __shared__ float cs[32];   // the chunk's translation
-    const int p0 = (tile0 + (int)(blockIdx.x >> 3) * tile_stride) * TP_BN + (blockIdx.x & 7) * 32;
+    const int p0 = (tile0 + tiles.tile((int)(blockIdx.x >> 3))) * TP_BN + (blockIdx.x & 7) * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     float s = 0.f;
     for (int d0 = 0; d0 < d_pad; d0 += 32) {
@@ -913,7 +914,7 @@ bool encode_norm_rows(CUtensorMap *m, const void *base, int rows) {
                      (uint64_t)TC_NK, TC_NK, TC_BM, CU_TENSOR_MAP_SWIZZLE_32B);
 }
 
-// Candidate lists: first scan cmax = 4 * KS * stride1 (<= 1280 for k <=
+// Candidate lists: first scan cmax = 4 * KS * stride (<= 1280 for k <=
 // 128); the second scan of the queries whose list overflowed reuses the
 // whole list buffer, up to kTcCmaxRetry entries per query.  The re-rank
 // kernel's shared memory (keys padded to a power of two) is capped at
@@ -922,8 +923,9 @@ constexpr int kTcCmaxRetry = 8192;
 constexpr size_t kRerankSmem = 200 * 1024;
 
 struct TcPlan {
-    int d_pad, kb, qtiles, stride1, cmax;
+    int d_pad, kb, qtiles, cmax;
     int n_tiles2, splits1;   // 256-point tiles; pass-1 splits over CTA pairs
+    TileRuns sample;         // pass-1 tiles
 };
 
 // Splits that fill whole waves of one CTA per SM for `tiles` tiles per
@@ -949,15 +951,20 @@ TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
     p.d_pad = (d + 63) / 64 * 64;
     p.kb = p.d_pad / 64;
     p.qtiles = (Q + TC_QT - 1) / TC_QT;
-    // the sample must hold about 2.5k points below T_q: KS * stride >= 2.5k
-    p.stride1 = std::max(16, (5 * k + 2 * TC_KS - 1) / (2 * TC_KS));
-    p.cmax = 4 * TC_KS * p.stride1;
+    // pass 1 samples one tile in `stride`: the sample must hold about 2.5k
+    // points below T_q, KS * stride >= 2.5k
+    const int stride = std::max(16, (5 * k + 2 * TC_KS - 1) / (2 * TC_KS));
+    p.cmax = 4 * TC_KS * stride;
     p.n_tiles2 = (N + TP_BN - 1) / TP_BN;
-    // pass 1 (CTA pairs) scans every stride1-th 256-point tile; coarser
-    // splits amortise each pair's set-up (query tile load, TMEM allocation,
-    // pipeline fill)
-    p.splits1 = choose_splits(p.qtiles, (p.n_tiles2 + p.stride1 - 1) / p.stride1, 16, 8.0,
-                              std::max(1, num_sms / 2));
+    // in runs of up to 16 consecutive tiles (one every stride tiles when
+    // the set is small), at least 32 runs across the set
+    const int run = std::max(1, std::min(16, p.n_tiles2 / (32 * stride)));
+    p.sample.run = run;
+    p.sample.period = run * stride;
+    p.sample.units = p.sample.count_below(p.n_tiles2);
+    // coarser pass-1 splits amortise each pair's set-up (query tile load,
+    // TMEM allocation, pipeline fill)
+    p.splits1 = choose_splits(p.qtiles, p.sample.units, 16, 8.0, std::max(1, num_sms / 2));
     return p;
 }
 
@@ -1004,25 +1011,29 @@ int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, i
                    cudaStream_t st) {
     if (cudaMemsetAsync(v.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess) return kErrCuda;
     const int n_tiles = (N + TP_BN - 1) / TP_BN;
-    const int rc = tc_center_from_tiles(v, ref, N, ldr, d, kCenterStride, st);
-    return rc != kOk ? rc : tc_prepare_ref_tiles(v, ref, N, ldr, d, 0, n_tiles, 1, st);
+    const int rc = tc_center_from_tiles(v, ref, N, ldr, d, contiguous_tiles(n_tiles),
+                                        kCenterStride, st);
+    return rc != kOk ? rc
+                     : tc_prepare_ref_tiles(v, ref, N, ldr, d, 0, contiguous_tiles(n_tiles), st);
 }
 
 int tc_center_from_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
-                         int tile_stride, cudaStream_t st) {
+                         const TileRuns &tiles, int step, cudaStream_t st) {
+    if (step < 1 || tiles.run < 1 || tiles.period < tiles.run) return kErrInvalid;
     const int d_pad = (d + 63) / 64 * 64;
-    const int n_sample = ((N + TP_BN - 1) / TP_BN + tile_stride - 1) / tile_stride;
-    tc_center_kernel<<<d_pad, 256, 0, st>>>(ref, N, ldr, d, tile_stride, n_sample, v.center);
+    const int n_used = (tiles.units + step - 1) / step;
+    tc_center_kernel<<<d_pad, 256, 0, st>>>(ref, N, ldr, d, tiles, step, n_used, v.center);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
 int tc_prepare_ref_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
-                         int tile0, int n_tiles, int tile_stride, cudaStream_t st) {
-    if (n_tiles <= 0) return kOk;
+                         int tile0, const TileRuns &tiles, cudaStream_t st) {
+    if (tiles.units <= 0) return kOk;
+    if (tiles.run < 1 || tiles.period < tiles.run) return kErrInvalid;
     const int d_pad = (d + 63) / 64 * 64;
-    tc_prep_ref_kernel<<<n_tiles * 8, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, tile0,
-                                                            tile_stride, v.center, v.refB, v.refT,
-                                                            v.refN, v.rmax_bits);
+    tc_prep_ref_kernel<<<tiles.units * 8, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, tile0,
+                                                                tiles, v.center, v.refB, v.refT,
+                                                                v.refN, v.rmax_bits);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
@@ -1057,9 +1068,8 @@ int emit_scan(const TcRun &r, cudaStream_t st, const __nv_bfloat16 *qB, int Q, c
     a.Q = Q;
     a.kb_count = r.kb;
     a.tile_base = tb;
-    a.n_tiles = te - tb;
+    a.tiles = contiguous_tiles(te - tb);
     a.n_splits = choose_splits(qtiles, te - tb, 8, 2.0, std::max(1, P.num_sms / 2));
-    a.tile_stride = 1;
     a.thr = thr;
     a.p1 = nullptr;
     a.cand = r.cand;
@@ -1107,8 +1117,8 @@ int read_count(const int *dev, int *host_pinned, cudaStream_t st, int &out) {
 
 }  // namespace
 
-int tc_sample_stride(int N, int Q, int d, int k, int num_sms) {
-    return plan_tc(N, Q, d, k, num_sms).stride1;
+TileRuns tc_sample_runs(int N, int Q, int d, int k, int num_sms) {
+    return plan_tc(N, Q, d, k, num_sms).sample;
 }
 
 int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun &r) {
@@ -1121,7 +1131,7 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     r.qtiles = p.qtiles;
     r.n_tiles2 = p.n_tiles2;
     r.splits1 = p.splits1;
-    r.stride1 = p.stride1;
+    r.sample = p.sample;
     r.cmax = p.cmax;
     Carve cv{static_cast<unsigned char *>(P.scratch), 0, P.scratch_bytes};
     r.qB = cv.take<__nv_bfloat16>((size_t)p.qtiles * TC_QT * p.d_pad);
@@ -1173,9 +1183,8 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
     a.Q = P.Q;
     a.kb_count = r.kb;
     a.tile_base = 0;
-    a.n_tiles = r.n_tiles2;
+    a.tiles = r.sample;
     a.n_splits = r.splits1;
-    a.tile_stride = r.stride1;
     a.thr = nullptr;
     a.p1 = r.p1;
     a.cand = r.cand;
