@@ -236,7 +236,7 @@ KNN_DI bool consume_ref_tile(f32x2_t (&acc)[QPW][4], const float *stages, uint64
         }
         const float *qs = stages + (size_t)s * C::STAGE_FLOATS + warp * 2 * QPW;
         const float *rs = stages + (size_t)s * C::STAGE_FLOATS + C::Q_FLOATS + lane * 4;
-#pragma unroll 4
+#pragma unroll
         for (int dd = 0; dd < EX_BD; ++dd) {
             // 16-byte loads straight into packed pairs (x, y), (z, w)
             const ulonglong2 ra = *reinterpret_cast<const ulonglong2 *>(rs + dd * EX_BR);

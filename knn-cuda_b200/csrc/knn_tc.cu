@@ -591,14 +591,24 @@ __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long
     const int p0 = (tile0 + tiles.tile((int)(blockIdx.x >> 3))) * TP_BN + (blockIdx.x & 7) * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     float s = 0.f;
+    // the next chunk's values are loaded into registers while this chunk
+    // is processed
+    float nx[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int dd = ty + 8 * i, p = p0 + tx;
+        nx[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
+    }
     for (int d0 = 0; d0 < d_pad; d0 += 32) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int dd = d0 + ty + 8 * i, p = p0 + tx;
-            tile[ty + 8 * i][tx] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
-        }
+        for (int i = 0; i < 4; ++i) tile[ty + 8 * i][tx] = nx[i];
         if (ty == 1) cs[tx] = d0 + tx < d ? center[d0 + tx] : 0.f;
         __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int dd = d0 + 32 + ty + 8 * i, p = p0 + tx;
+            nx[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
+        }
         if (ty == 0) {
             const int dm = min(32, d - d0);
             for (int dd = 0; dd < dm; ++dd) {
@@ -689,13 +699,15 @@ KNN_DI void warp_bitonic_sort(unsigned long long *keys, int P, int lane) {
 // distance of that prefix is the k-th of all candidates.
 //
 // The prefix is handled 32 candidates at a time, one per lane: the warp
-// copies the 32 candidate rows of the FP32 point-major copy, 64 dimensions
-// at a time, into a padded shared tile with asynchronous 16-byte copies
-// (cp.async, two rows per instruction, coalesced), double-buffered so the
-// next chunk is in flight while each lane runs its candidate's FMA chain in
-// increasing d -- the fused exact kernel's arithmetic and order, so
-// distances are identical.  The (distance, index) keys are bitonic-sorted by
-// the warp.
+// copies the 32 candidate rows of the FP32 point-major copy, TC_RR_DCH
+// dimensions at a time, into a padded shared tile with asynchronous 16-byte
+// copies (cp.async, several rows per instruction, coalesced), through a ring
+// of TC_RR_NBUF buffers so the next chunks are in flight while each lane
+// runs its candidate's FMA chain in increasing d -- the fused exact kernel's
+// arithmetic and order, so distances are identical.  The (distance, index)
+// keys are bitonic-sorted by the warp.  One warp per block: the gather is
+// latency-bound, and single-warp blocks let the SM hold as many warps as
+// its shared memory allows (about 14 at d = 256).
 //
 // An uncertified query is appended to fail_list and retry[q] receives a
 // threshold for a second scan: when it had at least k candidates, their k-th
@@ -705,15 +717,16 @@ KNN_DI void warp_bitonic_sort(unsigned long long *keys, int P, int lane) {
 // the threshold is widened by 8 E; an overflowing list keeps its threshold
 // for a second scan with a longer list (final_pass = 0) or gets NaN (exact
 // kernel).
-constexpr int TC_RR_WARPS = 4;
-constexpr int TC_RR_DCH = 64;                 // dimensions per staged chunk
+constexpr int TC_RR_WARPS = 1;
+constexpr int TC_RR_DCH = 32;                 // dimensions per staged chunk
+constexpr int TC_RR_NBUF = 2;                 // staging buffers per warp (ring)
 // padded row (floats): 16-byte aligned, and 16-byte reads of one row per lane
 // fall in distinct bank groups for every 8 consecutive lanes
 constexpr int TC_RR_STRIDE = TC_RR_DCH + 4;
 constexpr int TC_RR_BUF = 32 * TC_RR_STRIDE;  // floats per staging buffer
 
 __host__ __device__ inline size_t tc_rr_warp_bytes(int d_pad, int cpow) {
-    return (size_t)d_pad * 4 + 2 * TC_RR_BUF * 4 + (size_t)cpow * 8;
+    return (size_t)d_pad * 4 + TC_RR_NBUF * TC_RR_BUF * 4 + (size_t)cpow * 8;
 }
 
 KNN_DI void cp_async16(void *smem_dst, const void *gmem_src) {
@@ -722,7 +735,10 @@ KNN_DI void cp_async16(void *smem_dst, const void *gmem_src) {
                  : "memory");
 }
 KNN_DI void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-KNN_DI void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+template <int N>
+KNN_DI void cp_async_wait_n() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __global__ void __launch_bounds__(TC_RR_WARPS * 32)
     tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
@@ -740,7 +756,7 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
     unsigned char *mine = rsm + (size_t)warp * tc_rr_warp_bytes(d_pad, cpow);
     float *qv = reinterpret_cast<float *>(mine);
     float *rows = qv + d_pad;   // two staging buffers
-    unsigned long long *keys = reinterpret_cast<unsigned long long *>(rows + 2 * TC_RR_BUF);
+    unsigned long long *keys = reinterpret_cast<unsigned long long *>(rows + TC_RR_NBUF * TC_RR_BUF);
 
     const int c = count[q];
     if (lane == 0) atomicAdd(cand_total, (unsigned long long)c);
@@ -783,41 +799,45 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
         }
         n_s = max(cnt, k);   // keys are sorted, so the kept ones are a prefix
     }
-    // steps s = (group, chunk); the copy of step s + 1 overlaps step s
+    // steps s = (group, chunk); the copies of steps s + 1 .. s + NBUF - 1
+    // overlap step s
     {
         const int nch = d_pad / TC_RR_DCH;
         const int total = ((n_s + 31) / 32) * nch;
+        constexpr int CPL = TC_RR_DCH / 4;   // 16-byte copies per row and chunk
+        constexpr int RPI = 32 / CPL;        // rows per copy instruction
         auto issue = [&](int buf, int rr, int ch) {
             float *dstb = rows + buf * TC_RR_BUF;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const int row = 2 * i + (lane >> 4);
+            for (int i = 0; i < 32 / RPI; ++i) {
+                const int row = RPI * i + lane / CPL;
                 const int r = __shfl_sync(0xffffffffu, rr, row);
                 if (r >= 0)
-                    cp_async16(dstb + row * TC_RR_STRIDE + (lane & 15) * 4,
-                               refT + (size_t)r * d_pad + ch + (lane & 15) * 4);
+                    cp_async16(dstb + row * TC_RR_STRIDE + (lane % CPL) * 4,
+                               refT + (size_t)r * d_pad + ch + (lane % CPL) * 4);
             }
         };
-        int r_cur = lane < n_s ? (int)(uint32_t)keys[lane] : -1;
-        int r_nxt = r_cur;
-        issue(0, r_cur, 0);
-        cp_async_commit();
+        auto row_of = [&](int grp) {
+            const int t = grp * 32 + lane;
+            return t < n_s ? (int)(uint32_t)keys[t] : -1;
+        };
+#pragma unroll
+        for (int s = 0; s < TC_RR_NBUF - 1; ++s) {
+            if (s < total) issue(s, row_of(s / nch), (s % nch) * TC_RR_DCH);
+            cp_async_commit();
+        }
         float acc = 0.f;
+        int r_cur = -1;
         for (int s = 0; s < total; ++s) {
             const int g = s / nch, ch = s - g * nch;
-            if (s + 1 < total) {
-                const int s1 = s + 1, g1 = s1 / nch, ch1 = s1 - g1 * nch;
-                if (ch1 == 0) {
-                    const int t1 = g1 * 32 + lane;
-                    r_nxt = t1 < n_s ? (int)(uint32_t)keys[t1] : -1;
-                }
-                issue(s1 & 1, r_nxt, ch1 * TC_RR_DCH);
-            }
+            if (ch == 0) r_cur = row_of(g);
+            const int s1 = s + TC_RR_NBUF - 1;
+            if (s1 < total) issue(s1 % TC_RR_NBUF, row_of(s1 / nch), (s1 % nch) * TC_RR_DCH);
             cp_async_commit();
-            cp_async_wait_prev();   // step s's copies have landed
+            cp_async_wait_n<TC_RR_NBUF - 1>();   // step s's copies have landed
             __syncwarp();
-            const float4 *myrow =
-                reinterpret_cast<const float4 *>(rows + (s & 1) * TC_RR_BUF + lane * TC_RR_STRIDE);
+            const float4 *myrow = reinterpret_cast<const float4 *>(
+                rows + (s % TC_RR_NBUF) * TC_RR_BUF + lane * TC_RR_STRIDE);
             const float4 *qc = reinterpret_cast<const float4 *>(qv + ch * TC_RR_DCH);
 #pragma unroll
             for (int j = 0; j < TC_RR_DCH / 4; ++j) {
@@ -831,12 +851,11 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
                 t0 = __fsub_rn(rv.w, qq4.w);
                 acc = __fmaf_rn(t0, t0, acc);
             }
-            __syncwarp();   // buffer s & 1 is refilled by step s + 1's prefetch
+            __syncwarp();   // this buffer is refilled NBUF - 1 steps later
             if (ch == nch - 1) {
                 const int t = g * 32 + lane;
                 if (t < n_s) keys[t] = make_key(acc, (uint32_t)r_cur);
                 acc = 0.f;
-                r_cur = r_nxt;
             }
         }
     }
