@@ -81,6 +81,7 @@ struct BatchCfg {
     using C = ExCfg<QPW, KCAP>;
     static constexpr size_t ITEM_OFFSET = C::BAR_OFFSET + 2 * EX_STAGES * 8 + 64;
     static constexpr size_t SMEM = 1024 + ITEM_OFFSET + 2 * sizeof(ItemInfo) + 4 * 8 + 64;
+    static_assert(SMEM <= 232448, "shared memory per CTA");
 };
 
 template <int QPW, int KCAP>

@@ -7,7 +7,7 @@
 //   * A CTA owns BQ queries (one query tile) and one contiguous slice
 //     ("split") of the reference set.  Reference tiles of 256 points x 16
 //     dimensions and the matching 16 x BQ query slab are brought into shared
-//     memory by TMA (one producer warp, a 3-stage mbarrier ring).
+//     memory by TMA (one producer warp, a 4-stage mbarrier ring).
 //   * 16 consumer warps; warp w owns QPW queries, lane l owns the 8
 //     reference points {4l..4l+3, 128+4l..128+4l+3} of each tile, so every
 //     lane accumulates a QPW x 8 block of squared distances in registers as

@@ -14,7 +14,7 @@ constexpr int EX_WARPS = 16;     // consumer warps
 constexpr int EX_QPW = 4;        // queries per warp for k <= 128
 constexpr int EX_QPW_K256 = 2;   // queries per warp for 128 < k <= 256
 constexpr int EX_THREADS = (EX_WARPS + 1) * 32;
-constexpr int EX_STAGES = 3;
+constexpr int EX_STAGES = 4;
 
 template <int QPW, int KCAP>
 struct ExCfg {
@@ -30,6 +30,7 @@ struct ExCfg {
     static constexpr size_t BAR_OFFSET = (size_t)EX_STAGES * STAGE_BYTES + LIST_BYTES;
     static constexpr size_t SMEM = 1024 + BAR_OFFSET + 2 * EX_STAGES * 8 + 16;
     static_assert(STAGE_BYTES % 1024 == 0, "stage alignment");
+    static_assert(SMEM <= 232448, "shared memory per CTA");
     static_assert(KCAP % 32 == 0 && (KCAP & (KCAP - 1)) == 0, "KCAP power of two >= 32");
 };
 
