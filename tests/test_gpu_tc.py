@@ -177,11 +177,13 @@ def test_overflowing_lists_rescanned_with_longer_lists(knncuda, gpu):
 
 @pytest.mark.parametrize("n,dim,k", [(262144, 64, 20),     # tile-aligned, 8 whole chunks
                                      (299108, 96, 100),    # ragged last sample tile and chunk
+                                     (262244, 48, 20),     # last sample run: one ragged tile
                                      (1 << 20, 256, 100)])  # the headline shape
 def test_cublas_host_streamed_from_pinned_memory(knncuda, gpu, n, dim, k):
     """knn_cublas from page-locked host buffers on a large set streams the
-    reference set in (sample tiles first, then chunks, each scanned once it
-    has landed); the answer equals knn_cuda_global's bit for bit."""
+    reference set in (the threshold sample's runs of tiles first, then
+    chunks without them, each scanned once it has landed); the answer equals
+    knn_cuda_global's bit for bit."""
     import torch
 
     rng = np.random.default_rng(n + dim)
