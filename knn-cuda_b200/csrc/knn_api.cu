@@ -292,7 +292,8 @@ int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_h
         if (cudaStreamWaitEvent(st, ws.copied[1 + c], 0) != cudaSuccess) return kErrCuda;
         if (bound[c] >= bound[c + 1]) continue;
         if ((rc = for_each_gap(sample, bound[c], bound[c + 1], prep_tiles)) != kOk ||
-            (rc = tc_run_pass2(run, bound[c], bound[c + 1], st)) != kOk)
+            (rc = tc_run_pass2(run, bound[c], bound[c + 1], st)) != kOk ||
+            (rc = tc_run_rerank_piece(run, st)) != kOk)
             return rc;
     }
     return tc_run_finish(run, st, ws.tc_stats);

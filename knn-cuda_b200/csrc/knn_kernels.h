@@ -178,6 +178,12 @@ struct TcRun {
     unsigned long long *cand_total, *cand;
     unsigned char *xs;
     size_t xcap;
+    // incremental re-rank (tc_run_rerank_piece): running k smallest exact
+    // keys per query and list entries consumed, in the exact-fallback
+    // scratch (idle until certification)
+    bool pieces;
+    unsigned long long *run_keys;
+    int *done;
 };
 int tc_tile_points();   // points per tile of the staged API (256)
 TileRuns tc_sample_runs(int N, int Q, int d, int k, int num_sms);
@@ -195,6 +201,11 @@ inline TileRuns contiguous_tiles(int n) { return TileRuns{1, 1, n}; }
 int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun &run);
 int tc_run_pass1(TcRun &run, cudaStream_t st);
 int tc_run_pass2(TcRun &run, int tile_begin, int tile_end, cudaStream_t st);
+// Exact re-rank of the candidates found since the last call, merged into
+// running per-query lists; when it has run after the last tc_run_pass2,
+// tc_run_finish only certifies (and handles the second chance).  Optional:
+// without it tc_run_finish re-ranks all candidates at once.
+int tc_run_rerank_piece(TcRun &run, cudaStream_t st);
 int tc_run_finish(TcRun &run, cudaStream_t st, int *host_stats);
 
 // Queues the tensor-core k-NN.  Synchronises once to learn how many queries

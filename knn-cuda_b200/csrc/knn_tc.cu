@@ -46,6 +46,7 @@
 #include <algorithm>
 #include <cstdio>
 
+#include "knn_exact_core.cuh"
 #include "knn_kernels.h"
 #include "knn_tc.cuh"
 
@@ -740,6 +741,117 @@ KNN_DI void cp_async_wait_n() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// A candidate list that cannot be re-ranked -- more entries than it holds
+// (overflow) or fewer than k: the query joins fail_list with the threshold
+// of a second scan.  Too few candidates mean the threshold was low, so it is
+// widened by 8 E; an overflowing list is scanned again with the same
+// threshold and a longer list, and overflowing that too (final_pass) it
+// goes to the exact kernel (NaN).  Warp-uniform; true if rejected.
+KNN_DI bool rr_reject_list(int c, int cmax, int k, int q, float qq, float r2, float T, int d_pad,
+                           int final_pass, int *fail_list, int *n_fail, float *retry, int lane) {
+    if (c <= cmax && c >= k) return false;
+    if (lane == 0) {
+        fail_list[atomicAdd(n_fail, 1)] = q;
+        retry[q] = c < k ? T + 8.f * tc_error_bound(qq, r2, T, d_pad)
+                         : (final_pass ? __int_as_float(0x7fc00000) : T);
+    }
+    return true;
+}
+
+// Exact FP32 distances of the candidates keys[0..n) (point index in the low
+// 32 bits), in place: keys[t] = (distance, index).  One warp, 32 candidates
+// at a time, one per lane: the rows of the FP32 point-major copy are staged
+// TC_RR_DCH dimensions at a time through the TC_RR_NBUF buffers `rows`
+// (steps s = (group, chunk); the copies of steps s + 1 .. s + NBUF - 1
+// overlap step s), and each lane runs its candidate's FMA chain against the
+// query qv (d_pad floats) in increasing d.
+KNN_DI void rr_exact_distances(unsigned long long *keys, int n, const float *__restrict__ refT,
+                               int d_pad, const float *qv, float *rows, int lane) {
+    const int nch = d_pad / TC_RR_DCH;
+    const int total = ((n + 31) / 32) * nch;
+    constexpr int CPL = TC_RR_DCH / 4;   // 16-byte copies per row and chunk
+    constexpr int RPI = 32 / CPL;        // rows per copy instruction
+    auto issue = [&](int buf, int rr, int ch) {
+        float *dstb = rows + buf * TC_RR_BUF;
+#pragma unroll
+        for (int i = 0; i < 32 / RPI; ++i) {
+            const int row = RPI * i + lane / CPL;
+            const int r = __shfl_sync(0xffffffffu, rr, row);
+            if (r >= 0)
+                cp_async16(dstb + row * TC_RR_STRIDE + (lane % CPL) * 4,
+                           refT + (size_t)r * d_pad + ch + (lane % CPL) * 4);
+        }
+    };
+    auto row_of = [&](int grp) {
+        const int t = grp * 32 + lane;
+        return t < n ? (int)(uint32_t)keys[t] : -1;
+    };
+#pragma unroll
+    for (int s = 0; s < TC_RR_NBUF - 1; ++s) {
+        if (s < total) issue(s, row_of(s / nch), (s % nch) * TC_RR_DCH);
+        cp_async_commit();
+    }
+    float acc = 0.f;
+    int r_cur = -1;
+    for (int s = 0; s < total; ++s) {
+        const int g = s / nch, ch = s - g * nch;
+        if (ch == 0) r_cur = row_of(g);
+        const int s1 = s + TC_RR_NBUF - 1;
+        if (s1 < total) issue(s1 % TC_RR_NBUF, row_of(s1 / nch), (s1 % nch) * TC_RR_DCH);
+        cp_async_commit();
+        cp_async_wait_n<TC_RR_NBUF - 1>();   // step s's copies have landed
+        __syncwarp();
+        const float4 *myrow = reinterpret_cast<const float4 *>(
+            rows + (s % TC_RR_NBUF) * TC_RR_BUF + lane * TC_RR_STRIDE);
+        const float4 *qc = reinterpret_cast<const float4 *>(qv + ch * TC_RR_DCH);
+#pragma unroll
+        for (int j = 0; j < TC_RR_DCH / 4; ++j) {
+            const float4 rv = myrow[j], qq4 = qc[j];
+            float t0 = __fsub_rn(rv.x, qq4.x);
+            acc = __fmaf_rn(t0, t0, acc);
+            t0 = __fsub_rn(rv.y, qq4.y);
+            acc = __fmaf_rn(t0, t0, acc);
+            t0 = __fsub_rn(rv.z, qq4.z);
+            acc = __fmaf_rn(t0, t0, acc);
+            t0 = __fsub_rn(rv.w, qq4.w);
+            acc = __fmaf_rn(t0, t0, acc);
+        }
+        __syncwarp();   // this buffer is refilled NBUF - 1 steps later
+        if (ch == nch - 1) {
+            const int t = g * 32 + lane;
+            if (t < n) keys[t] = make_key(acc, (uint32_t)r_cur);
+            acc = 0.f;
+        }
+    }
+}
+
+// Certification from a query's k smallest exact keys (sorted; keys[k - 1]
+// the k-th): certified, the query's sqrt distances and indices are written;
+// otherwise it joins fail_list with the threshold of a second scan that
+// certifies (see tc_rerank_kernel).  Warp-uniform.
+KNN_DI void rr_certify(const unsigned long long *keys, int q, float qq, float r2, float T,
+                       int d_pad, int k, float *__restrict__ out_dist, int *__restrict__ out_idx,
+                       long long ld_out, int *fail_list, int *n_fail, float *retry, int lane) {
+    int failed = 0;
+    if (lane == 0) {
+        const float dk = key_dist2(keys[k - 1]);
+        const float E = tc_error_bound(qq, r2, T, d_pad);
+        const float dkg = dk * (1.f + (float)d_pad * 2.384185791015625e-07f);
+        failed = !(dkg + E < T + qq);
+        if (failed) {
+            fail_list[atomicAdd(n_fail, 1)] = q;
+            const float T2 = dkg - qq;
+            retry[q] = T2 + 2.5f * tc_error_bound(qq, r2, T2, d_pad);
+        }
+    }
+    if (__shfl_sync(0xffffffffu, failed, 0)) return;
+    for (int j = lane; j < k; j += 32) {
+        const unsigned long long key = keys[j];
+        out_dist[(size_t)j * ld_out + q] = sqrtf(key_dist2(key));
+        out_idx[(size_t)j * ld_out + q] = key_index(key);
+    }
+}
+
 __global__ void __launch_bounds__(TC_RR_WARPS * 32)
     tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
                      const float *__restrict__ qry, long long ldq, const float *__restrict__ qn,
@@ -763,18 +875,9 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
     const float qq = qn[q];
     const float r2 = __uint_as_float(*rmax_bits);
     const float T = thr[q];
-    if (c > cmax || c < k) {
-        if (lane == 0) {
-            fail_list[atomicAdd(n_fail, 1)] = q;
-            // too few candidates: the threshold was low; widen it by 8 E.
-            // An overflowing list is scanned again with the same threshold
-            // and a longer list; overflowing that too, it goes to the exact
-            // kernel (NaN).
-            retry[q] = c < k ? T + 8.f * tc_error_bound(qq, r2, T, d_pad)
-                             : (final_pass ? __int_as_float(0x7fc00000) : T);
-        }
+    if (rr_reject_list(c, cmax, k, q, qq, r2, T, d_pad, final_pass, fail_list, n_fail, retry,
+                       lane))
         return;
-    }
     // candidates sorted by (a, index)
     const unsigned long long *cq = cand + (size_t)q * cmax;
     int P = 32;
@@ -799,89 +902,82 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
         }
         n_s = max(cnt, k);   // keys are sorted, so the kept ones are a prefix
     }
-    // steps s = (group, chunk); the copies of steps s + 1 .. s + NBUF - 1
-    // overlap step s
-    {
-        const int nch = d_pad / TC_RR_DCH;
-        const int total = ((n_s + 31) / 32) * nch;
-        constexpr int CPL = TC_RR_DCH / 4;   // 16-byte copies per row and chunk
-        constexpr int RPI = 32 / CPL;        // rows per copy instruction
-        auto issue = [&](int buf, int rr, int ch) {
-            float *dstb = rows + buf * TC_RR_BUF;
-#pragma unroll
-            for (int i = 0; i < 32 / RPI; ++i) {
-                const int row = RPI * i + lane / CPL;
-                const int r = __shfl_sync(0xffffffffu, rr, row);
-                if (r >= 0)
-                    cp_async16(dstb + row * TC_RR_STRIDE + (lane % CPL) * 4,
-                               refT + (size_t)r * d_pad + ch + (lane % CPL) * 4);
-            }
-        };
-        auto row_of = [&](int grp) {
-            const int t = grp * 32 + lane;
-            return t < n_s ? (int)(uint32_t)keys[t] : -1;
-        };
-#pragma unroll
-        for (int s = 0; s < TC_RR_NBUF - 1; ++s) {
-            if (s < total) issue(s, row_of(s / nch), (s % nch) * TC_RR_DCH);
-            cp_async_commit();
-        }
-        float acc = 0.f;
-        int r_cur = -1;
-        for (int s = 0; s < total; ++s) {
-            const int g = s / nch, ch = s - g * nch;
-            if (ch == 0) r_cur = row_of(g);
-            const int s1 = s + TC_RR_NBUF - 1;
-            if (s1 < total) issue(s1 % TC_RR_NBUF, row_of(s1 / nch), (s1 % nch) * TC_RR_DCH);
-            cp_async_commit();
-            cp_async_wait_n<TC_RR_NBUF - 1>();   // step s's copies have landed
-            __syncwarp();
-            const float4 *myrow = reinterpret_cast<const float4 *>(
-                rows + (s % TC_RR_NBUF) * TC_RR_BUF + lane * TC_RR_STRIDE);
-            const float4 *qc = reinterpret_cast<const float4 *>(qv + ch * TC_RR_DCH);
-#pragma unroll
-            for (int j = 0; j < TC_RR_DCH / 4; ++j) {
-                const float4 rv = myrow[j], qq4 = qc[j];
-                float t0 = __fsub_rn(rv.x, qq4.x);
-                acc = __fmaf_rn(t0, t0, acc);
-                t0 = __fsub_rn(rv.y, qq4.y);
-                acc = __fmaf_rn(t0, t0, acc);
-                t0 = __fsub_rn(rv.z, qq4.z);
-                acc = __fmaf_rn(t0, t0, acc);
-                t0 = __fsub_rn(rv.w, qq4.w);
-                acc = __fmaf_rn(t0, t0, acc);
-            }
-            __syncwarp();   // this buffer is refilled NBUF - 1 steps later
-            if (ch == nch - 1) {
-                const int t = g * 32 + lane;
-                if (t < n_s) keys[t] = make_key(acc, (uint32_t)r_cur);
-                acc = 0.f;
-            }
-        }
-    }
+    rr_exact_distances(keys, n_s, refT, d_pad, qv, rows, lane);
     int P2 = 32;
     while (P2 < n_s) P2 <<= 1;
     for (int t = n_s + lane; t < P2; t += 32) keys[t] = kKeyInf;
     __syncwarp();
     warp_bitonic_sort(keys, P2, lane);
-    int failed = 0;
-    if (lane == 0) {
-        const float dk = key_dist2(keys[k - 1]);
-        const float E = tc_error_bound(qq, r2, T, d_pad);
-        const float dkg = dk * (1.f + (float)d_pad * 2.384185791015625e-07f);
-        failed = !(dkg + E < T + qq);
-        if (failed) {
-            fail_list[atomicAdd(n_fail, 1)] = q;
-            const float T2 = dkg - qq;
-            retry[q] = T2 + 2.5f * tc_error_bound(qq, r2, T2, d_pad);
-        }
+    rr_certify(keys, q, qq, r2, T, d_pad, k, out_dist, out_idx, ld_out, fail_list, n_fail, retry,
+               lane);
+}
+
+// Incremental re-rank for a reference set that arrives in pieces (the
+// streamed host entry).  After each piece's scan, the candidates a query
+// gained since the last call (list entries done[q] .. min(count, cmax)) get
+// their exact FP32 distances and are merged into its running k smallest
+// keys run[q][0..k) (a sort of the new keys, then every key placed at its
+// index plus its rank in the other array).  Nothing is pruned -- the k-th a
+// is not known yet -- so about twice the rows of tc_rerank_kernel are
+// gathered, while the rest of the set is still being copied in.  After the
+// last piece run[q] holds the k smallest exact keys of all candidates: the
+// certification and the output are those of tc_rerank_kernel.  One warp
+// (block) per query.
+template <int KCAP>
+__global__ void __launch_bounds__(32)
+    tc_rerank_piece_kernel(const float *__restrict__ refT, int d, int d_pad,
+                           const float *__restrict__ qry, long long ldq,
+                           const unsigned long long *__restrict__ cand,
+                           const int *__restrict__ count, int cmax, int k,
+                           unsigned long long *__restrict__ run, int *__restrict__ done) {
+    extern __shared__ unsigned char rsm[];
+    const int q = blockIdx.x, lane = threadIdx.x;
+    const int c = min(count[q], cmax);
+    const int s0 = done[q];
+    if (s0 >= c) return;
+    float *qv = reinterpret_cast<float *>(rsm);
+    float *rows = qv + d_pad;
+    unsigned long long *L = reinterpret_cast<unsigned long long *>(rows + TC_RR_NBUF * TC_RR_BUF);
+    unsigned long long *C = L + KCAP;   // warp_merge's candidate slots (EX_CB)
+    for (int dd = lane; dd < d_pad; dd += 32) qv[dd] = dd < d ? qry[(size_t)dd * ldq + q] : 0.f;
+    for (int t = lane; t < KCAP; t += 32) L[t] = t < k ? run[(size_t)q * k + t] : kKeyInf;
+    __syncwarp();
+    const unsigned long long *cq = cand + (size_t)q * cmax;
+    for (int b0 = s0; b0 < c; b0 += EX_CB) {
+        const int n = min(EX_CB, c - b0);
+        for (int t = lane; t < n; t += 32) C[t] = cq[b0 + t];
+        __syncwarp();
+        rr_exact_distances(C, n, refT, d_pad, qv, rows, lane);
+        __syncwarp();
+        warp_merge<KCAP>(L, n, k, lane);
     }
-    if (__shfl_sync(0xffffffffu, failed, 0)) return;
-    for (int j = lane; j < k; j += 32) {
-        const unsigned long long key = keys[j];
-        out_dist[(size_t)j * ld_out + q] = sqrtf(key_dist2(key));
-        out_idx[(size_t)j * ld_out + q] = key_index(key);
-    }
+    for (int t = lane; t < k; t += 32) run[(size_t)q * k + t] = L[t];
+    if (lane == 0) done[q] = c;
+}
+
+// Certification after the last piece: tc_rerank_kernel's first-pass checks
+// on the running k smallest keys of tc_rerank_piece_kernel.  One warp per
+// query.
+__global__ void tc_certify_pieces_kernel(const int *__restrict__ count, int cmax,
+                                         const float *__restrict__ qn,
+                                         const unsigned *__restrict__ rmax_bits,
+                                         const float *__restrict__ thr,
+                                         const unsigned long long *__restrict__ run, int Q, int k,
+                                         int d_pad, float *__restrict__ out_dist,
+                                         int *__restrict__ out_idx, long long ld_out,
+                                         int *__restrict__ fail_list, int *__restrict__ n_fail,
+                                         float *__restrict__ retry,
+                                         unsigned long long *__restrict__ cand_total) {
+    const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (q >= Q) return;
+    const int c = count[q];
+    if (lane == 0) atomicAdd(cand_total, (unsigned long long)c);
+    const float qq = qn[q];
+    const float r2 = __uint_as_float(*rmax_bits);
+    const float T = thr[q];
+    if (rr_reject_list(c, cmax, k, q, qq, r2, T, d_pad, 0, fail_list, n_fail, retry, lane)) return;
+    rr_certify(run + (size_t)q * k, q, qq, r2, T, d_pad, k, out_dist, out_idx, ld_out, fail_list,
+               n_fail, retry, lane);
 }
 
 // Fallback plumbing: gather the uncertified queries into a dense d x m set
@@ -1171,6 +1267,9 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     r.xs = cv.take<unsigned char>(0);
     if (cv.used > P.scratch_bytes) return kErrScratch;
     r.xcap = P.scratch_bytes - cv.used;
+    r.pieces = false;
+    r.run_keys = nullptr;
+    r.done = nullptr;
 
     // queries: norms + BF16 K-major copy of -2 q
     tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, R.center, r.qn,
@@ -1231,14 +1330,58 @@ int tc_run_pass2(TcRun &r, int tile_begin, int tile_end, cudaStream_t st) {
     return rc;
 }
 
+int tc_run_rerank_piece(TcRun &r, cudaStream_t st) {
+    const TcProblem &P = r.P;
+    if (!r.pieces) {
+        // the running lists take the exact-fallback scratch, which nothing
+        // uses before the certification; without room the full re-rank
+        // runs in tc_run_finish instead
+        Carve cv{r.xs, 0, r.xcap};
+        unsigned long long *keys = cv.take<unsigned long long>((size_t)P.Q * P.k);
+        int *done = cv.take<int>(P.Q);
+        if (cv.used > r.xcap) return kOk;
+        if (cudaMemsetAsync(keys, 0xff, (size_t)P.Q * P.k * 8, st) != cudaSuccess ||
+            cudaMemsetAsync(done, 0, (size_t)P.Q * 4, st) != cudaSuccess)
+            return kErrCuda;
+        r.run_keys = keys;
+        r.done = done;
+        r.pieces = true;
+    }
+    const int kcap = P.k <= 32 ? 32 : (P.k <= 64 ? 64 : 128);
+    const size_t smem = (size_t)r.d_pad * 4 + (size_t)TC_RR_NBUF * TC_RR_BUF * 4 +
+                        (size_t)(kcap + EX_CB) * 8;   // < 48 KB for d_pad <= 256
+    auto go = [&](auto kern) {
+        kern<<<P.Q, 32, smem, st>>>(r.R.refT, P.d, r.d_pad, P.qry, P.ldq, r.cand, r.count, r.cmax,
+                                    P.k, r.run_keys, r.done);
+    };
+    if (kcap == 32)
+        go(tc_rerank_piece_kernel<32>);
+    else if (kcap == 64)
+        go(tc_rerank_piece_kernel<64>);
+    else
+        go(tc_rerank_piece_kernel<128>);
+    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
+}
+
 int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     const TcProblem &P = r.P;
     PhaseTimer *tm = P.timer;
     int *host_tmp = host_stats + 2;
     host_stats[0] = host_stats[1] = 0;
     host_stats[4] = host_stats[5] = 0;
-    int rc = rerank(r, st, P.Q, r.cmax, P.qry, P.ldq, r.qn, r.thr, P.out_dist, P.out_idx,
+    int rc = kOk;
+    if (r.pieces) {
+        // every candidate was re-ranked piece by piece: certify
+        if (cudaMemsetAsync(r.nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
+        constexpr int W = 4;
+        tc_certify_pieces_kernel<<<(P.Q + W - 1) / W, W * 32, 0, st>>>(
+            r.count, r.cmax, r.qn, r.R.rmax_bits, r.thr, r.run_keys, P.Q, P.k, r.d_pad,
+            P.out_dist, P.out_idx, P.ld_out, r.fail, r.nfail, r.retry, r.cand_total);
+        if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    } else {
+        rc = rerank(r, st, P.Q, r.cmax, P.qry, P.ldq, r.qn, r.thr, P.out_dist, P.out_idx,
                     P.ld_out, r.fail, false);
+    }
     if (rc != kOk) return rc;
     if (tm) tm->mark(st, kPhaseTcRerank);
     int nf = 0;
