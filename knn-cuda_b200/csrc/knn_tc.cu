@@ -17,7 +17,8 @@
 //             FP32 point-major copy of the reference set (for re-ranking),
 //             the reference norm parts, FP32 query norms and the largest
 //             reference norm.
-//   pass 1    tensor scan of a strided 1/G sample of the reference tiles; each
+//   pass 1    tensor scan of a 1/G sample of the reference tiles (runs of
+//             consecutive tiles, one run every G runs' worth); each
 //             epilogue thread keeps the KS smallest a of its query row in
 //             registers -> threshold T_q (KS-th smallest over the sample;
 //             over the full set about KS*G points lie below it).
@@ -32,6 +33,9 @@
 //             exact top-k was emitted, and the output is bit-identical to
 //             the exact kernel's.  Uncertified queries (sample too small, list
 //             overflow) are scanned again or recomputed by the exact kernel.
+//             When the set streams in from the host in pieces, the re-rank
+//             runs piece by piece into running top-k lists and only the
+//             certification waits for the last piece.
 //
 // Error bound (u = 2^-8, BF16 unit roundoff; K = d_pad + 16 accumulated
 // terms): |bf16(r).bf16(q) - r.q| <= (2u + u^2) sum|r_i q_i|, and the FP32
