@@ -71,15 +71,19 @@ KNNB200_API int knnb200_knn_device(const float *ref, int ref_nb, long long ref_l
  * allowed where they call from.  It has no counterpart in the reference
  * (whose functions allocate and free every buffer per call).  Inputs and
  * outputs are caller-owned device memory as for knnb200_knn_device; the
- * per-split scratch is a static 64 MiB device array inside this library,
- * held on every GPU that loads it until exit.  Shapes needing more scratch
- * than that (splits * query_nb * k * 8 bytes, splits as reported by
- * knnb200_plan_splits) are rejected with KNNB200_ESCRATCH.  The first call
- * on a device looks up the array's device address (make that first call
- * before any stream capture).  All calls share the array and its status
- * word: calls that overlap on the GPU race and must be serialised by the
- * caller.  Returns after the results are written (KNNB200_OK, or
- * KNNB200_ETIMEOUT if a kernel wait gave up). */
+ * scratch is a static 64 MiB device array inside this library, held on
+ * every GPU that loads it until exit.  A call needs the exact path's whole
+ * scratch there: the duplicated query copy (dim * round_up(query_nb, 32) * 8
+ * bytes), 256 bytes, and the per-split lists (splits * query_nb * k * 8
+ * bytes when the reference set is split; query_nb * 8 more for k > 256).
+ * knnb200_scratch_bytes(..., KNNB200_METHOD_GLOBAL) gives the exact figure;
+ * shapes needing more than 64 MiB are rejected with KNNB200_ESCRATCH.  The
+ * first call on a device looks up the array's device address (make that
+ * first call before any stream capture).  All calls share the array and its
+ * status word: calls that overlap on the GPU race and must be serialised by
+ * the caller.  The call synchronises `stream` (it reads the status word back
+ * into host memory) and returns after the results are written (KNNB200_OK,
+ * or KNNB200_ETIMEOUT if a kernel wait gave up). */
 KNNB200_API int knnb200_knn_device_noalloc(const float *ref, int ref_nb, long long ref_ld,
                                            const float *query, int query_nb,
                                            long long query_ld, int dim, int k, float *knn_dist,

@@ -13,9 +13,19 @@
 // Limits and sharing:
 //   * the static area is 64 MiB of device memory, held on every GPU that
 //     loads this library until the process exits;
-//   * a call needs splits * query_nb * k * 8 bytes of it (splits as chosen
-//     by the kernel's planner; knnb200_plan_splits reports it), and a call
-//     needing more is rejected with KNNB200_ESCRATCH before anything runs;
+//   * a call needs the exact path's whole scratch in it: the query set
+//     duplicated into (q, q) pairs (dim * round_up(query_nb, 32) * 8 bytes),
+//     256 bytes of alignment and, when the planner splits the reference set,
+//     splits * query_nb * k * 8 bytes of per-split lists (for k > 256 also
+//     query_nb * 8 bytes of lower-bound keys).  knnb200_scratch_bytes(...,
+//     KNNB200_METHOD_GLOBAL) gives the exact figure; a call needing more
+//     than the static area is rejected with KNNB200_ESCRATCH before anything
+//     runs;
+//   * the first call on a device looks up the area's device address
+//     (cudaGetSymbolAddress, with that device current); make that first
+//     call before any stream capture.  Every call waits for its own work
+//     on `stream` (it reads the kernel's status word back) before it
+//     returns;
 //   * every call uses the same area and the same status word, and the area
 //     keeps whatever the previous call left in it: each call overwrites the
 //     lists it reads and clears the status word itself, but two calls whose
@@ -41,8 +51,8 @@ static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocSc
 static __device__ int g_noalloc_status;
 
 struct NoAllocDevice {
-    std::once_flag once;
-    cudaError_t err = cudaSuccess;
+    std::mutex mu;
+    bool ready = false;
     void *scratch = nullptr;
     int *status = nullptr;
     int num_sms = 0;
@@ -50,18 +60,29 @@ struct NoAllocDevice {
 
 NoAllocDevice g_dev[kNoAllocMaxDevices];
 
-// Runs once per device, with that device current.
-NoAllocDevice *set_up(int dev) {
+// Looks up the device addresses once per device, with that device current.
+// Only a successful lookup is kept: after a failure (reported to the caller)
+// the next call on that device tries again.
+cudaError_t set_up(int dev, NoAllocDevice *&out) {
     NoAllocDevice *d = &g_dev[dev];
-    std::call_once(d->once, [d, dev]() {
-        d->err = cudaGetSymbolAddress(&d->scratch, g_noalloc_scratch);
-        if (d->err == cudaSuccess)
-            d->err = cudaGetSymbolAddress(reinterpret_cast<void **>(&d->status),
-                                          g_noalloc_status);
-        if (d->err == cudaSuccess)
-            d->err = cudaDeviceGetAttribute(&d->num_sms, cudaDevAttrMultiProcessorCount, dev);
-    });
-    return d;
+    std::lock_guard<std::mutex> lock(d->mu);
+    if (!d->ready) {
+        void *scratch = nullptr, *status = nullptr;
+        int sms = 0;
+        cudaError_t e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+        if (e == cudaSuccess) e = cudaGetSymbolAddress(&status, g_noalloc_status);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return e;
+        }
+        d->scratch = scratch;
+        d->status = static_cast<int *>(status);
+        d->num_sms = sms;
+        d->ready = true;
+    }
+    out = d;
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -86,10 +107,11 @@ extern "C" KNNB200_API int knnb200_knn_device_noalloc(const float *ref, int ref_
         return KNNB200_ENODEV;
     }
     if (cudaGetDevice(&dev) != cudaSuccess || dev >= kNoAllocMaxDevices) return KNNB200_ECUDA;
-    NoAllocDevice *d = set_up(dev);
-    if (d->err != cudaSuccess) {
+    NoAllocDevice *d = nullptr;
+    const cudaError_t se = set_up(dev, d);
+    if (se != cudaSuccess) {
         std::printf("ERROR: knnb200_knn_device_noalloc: cannot locate the static scratch (%s)\n",
-                    cudaGetErrorString(d->err));
+                    cudaGetErrorString(se));
         return KNNB200_ECUDA;
     }
     const size_t need = exact_scratch_bytes(ref_nb, query_nb, dim, k, d->num_sms);
