@@ -74,8 +74,9 @@ KNNB200_API int knnb200_knn_device(const float *ref, int ref_nb, long long ref_l
  * scratch is a static 64 MiB device array inside this library, held on
  * every GPU that loads it until exit.  A call needs the exact path's whole
  * scratch there: the duplicated query copy (dim * round_up(query_nb, 32) * 8
- * bytes), 256 bytes, and the per-split lists (splits * query_nb * k * 8
- * bytes when the reference set is split; query_nb * 8 more for k > 256).
+ * bytes), 256 bytes, and the per-split lists (splits * query_nb *
+ * min(k, 256) * 8 bytes when the reference set is split; query_nb * 8 more
+ * for k > 256).
  * knnb200_scratch_bytes(..., KNNB200_METHOD_GLOBAL) gives the exact figure;
  * shapes needing more than 64 MiB are rejected with KNNB200_ESCRATCH.  The
  * first call on a device looks up the array's device address (make that
@@ -191,6 +192,23 @@ KNNB200_API size_t knnb200_scratch_bytes(int ref_nb, int query_nb, int dim, int 
 /* Number of reference splits the exact kernel uses for this shape. */
 KNNB200_API int knnb200_plan_splits(int ref_nb, int query_nb, int dim, int k);
 
+/* Memory admission of the host and device entry points (the reference's
+ * legacy code split the queries by free memory,
+ * legacy/KNN.CUDA.with.indexes/knn_cuda_with_indexes.cu:348-349, :406-444):
+ * a call whose buffers for all query_nb queries do not fit in the device's
+ * free memory (plus what the library's workspace already holds) runs its
+ * queries in chunks that do, with the same results.  knnb200_set_memory_cap
+ * lowers the memory the library assumes it may use to `bytes` (0 = no cap;
+ * a host-side setting, used to test the chunked path); knnb200_last_query_chunks
+ * returns the number of chunks of the last host or device call. */
+KNNB200_API void knnb200_set_memory_cap(size_t bytes);
+KNNB200_API int knnb200_last_query_chunks(void);
+/* Device bytes the library estimates for one call of this shape run as one
+ * chunk: host != 0 for the host entry points (reference and query copies,
+ * outputs, scratch), 0 for knnb200_knn_device (scratch only). */
+KNNB200_API size_t knnb200_call_bytes(int ref_nb, int query_nb, int dim, int k, int method,
+                                      int host);
+
 /* Free the current device's workspace (the next call re-allocates). */
 KNNB200_API void knnb200_release_workspace(void);
 
@@ -218,6 +236,21 @@ KNNB200_API int knnb200_selftest_wait_timeout(long long limit_ns, void *stream);
  * exact kernel (*exact).  All 0 when the call ran the exact kernel only.
  * Any pointer may be NULL. */
 KNNB200_API void knnb200_last_tc_stats(long long *candidates, int *second_scan, int *exact);
+
+/* Test-only check of the tensor path's error bound (no counterpart in the
+ * reference, whose knn_cublas has no bound).  While enabled, every
+ * knn_cublas-method call on the current device that runs the tensor path
+ * records, over all candidates its exact re-rank sees, the largest
+ * |a + ||q||^2 - D| / E_q: a the candidate's BF16-expansion value, D its
+ * exact FP32 squared distance, E_q the bound the certification assumes
+ * for the query.  A ratio below 1 is what the certification needs; the
+ * test asserts a margin.  The check runs a separate instantiation of the
+ * re-rank kernel; off by default (enable = 0 turns it off). */
+KNNB200_API int knnb200_set_bound_check(int enable);
+/* Waits for the current device's work stream and returns the ratio and the
+ * number of candidates checked by the last such call (KNNB200_EINVAL if
+ * the check was never enabled). */
+KNNB200_API int knnb200_last_bound_check(double *max_ratio, long long *checked);
 
 /* Per-phase device timing of the calls on the current device (CUDA events on
  * the launching stream between the kernels of a call).  Off by default. */

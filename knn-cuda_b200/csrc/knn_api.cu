@@ -10,6 +10,7 @@
 // ref_nb x query_nb FP32 distance matrix -- this runtime keeps a per-device
 // workspace (grow-only device buffers, one stream, one status word) guarded
 // by a mutex, so calls are thread-safe and no distance matrix exists.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -104,6 +105,8 @@ struct Workspace {
     cudaEvent_t last_done = nullptr;   // orders device-resident calls on this device
     Buffer ref, qry, dist, idx, scratch, status;
     Buffer tcref;                      // prepared reference set of the tensor-core path
+    Buffer bound;                      // re-rank bound check (test-only, off by default)
+    bool bound_check = false;
     PhaseTimer timer;                  // optional per-phase device timing
     int *status_host = nullptr;        // pinned status word for the host path
     int *tc_stats = nullptr;           // pinned: [0] second-scan queries, [1] exact fallbacks
@@ -155,7 +158,10 @@ size_t scratch_for(int method, int N, int Q, int d, int k, int num_sms) {
 // knn_cublas runs the tensor-core expansion path when the shape qualifies
 // (it synchronises the stream once, to recompute uncertified queries);
 // everything else runs the fused exact kernel.
-int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st) {
+// ref_prepared: the tensor-core view of this reference set is already in
+// ws.tcref (a later query chunk of the same call).
+int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st,
+            bool ref_prepared = false) {
     for (int i = 0; i < 8; ++i) ws.tc_stats[i] = 0;
     if (!exact_supported_k(p0.k)) return kErrUnsupported;
     ExactProblem p = p0;
@@ -164,7 +170,7 @@ int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st) 
     if (!use_tc(method, p.N, p.Q, p.d, p.k)) return launch_exact(p, st);
     if (!ws.tcref.ensure(tc_ref_bytes(p.N, p.d))) return kErrNoMemory;
     const TcRefView rv = tc_carve_ref(ws.tcref.ptr, p.N, p.d);
-    int rc = tc_prepare_ref(rv, p.ref, p.N, p.ldr, p.d, st);
+    int rc = ref_prepared ? kOk : tc_prepare_ref(rv, p.ref, p.N, p.ldr, p.d, st);
     if (rc != kOk) return rc;
     ws.timer.mark(st, kPhaseTcPrepRef);
     TcProblem t;
@@ -184,6 +190,10 @@ int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st) 
     t.status = p.status;
     t.num_sms = p.num_sms;
     t.timer = &ws.timer;
+    if (ws.bound_check) {
+        if (cudaMemsetAsync(ws.bound.ptr, 0, 16, st) != cudaSuccess) return kErrCuda;
+        t.bound_stat = static_cast<unsigned *>(ws.bound.ptr);
+    }
     return launch_tc(t, rv, st, ws.tc_stats);
 }
 
@@ -330,6 +340,58 @@ const char *method_name(int method) {
     }
 }
 
+// Query chunking by free memory (the legacy code's split of the query set
+// by cuMemGetInfo, legacy/KNN.CUDA.with.indexes/knn_cuda_with_indexes.cu:
+// 348-349, :406-444).  The memory a call may use is the device's free memory
+// plus what this workspace already holds (its buffers are reallocated as
+// needed), less a margin, and at most g_mem_cap when that is set (a host-side
+// cap for tests).  Buffer::ensure over-allocates by 1/8, which the
+// estimate includes.
+size_t g_mem_cap = 0;
+int g_last_chunks = 0;   // query chunks of the last host / device call
+constexpr size_t kMemMargin = 64u << 20;
+
+size_t grown(size_t b) { return b ? b + b / 8 + 256 : 0; }
+
+size_t usable_memory(const Workspace &ws) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        free_b = 0;
+    }
+    const size_t held = ws.ref.bytes + ws.qry.bytes + ws.dist.bytes + ws.idx.bytes +
+                        ws.scratch.bytes + ws.tcref.bytes;
+    size_t avail = free_b + held;
+    avail = avail > kMemMargin ? avail - kMemMargin : 0;
+    return g_mem_cap ? std::min(avail, g_mem_cap) : avail;
+}
+
+// Largest query chunk (all of Q when it fits, else a multiple of 256) whose
+// memory, per_chunk(qc) on top of `fixed`, fits the usable memory; 0 when
+// not even one query fits.
+template <class F>
+int plan_query_chunk(const Workspace &ws, int Q, size_t fixed, F per_chunk) {
+    const size_t avail = usable_memory(ws);
+    auto fits = [&](int qc) { return fixed + per_chunk(qc) <= avail; };
+    if (fits(Q)) return Q;
+    int lo = 0, hi = Q;   // fits(lo) (or lo == 0), !fits(hi)
+    while (hi - lo > 1) {
+        const int mid = lo + (hi - lo) / 2;
+        if (fits(mid)) lo = mid;
+        else hi = mid;
+    }
+    if (lo >= 256) lo = lo / 256 * 256;
+    return lo;
+}
+
+// Device bytes of one query chunk of the host entry: query copy, outputs,
+// scratch.
+size_t host_chunk_bytes(int method, int N, int qc, int d, int k, int num_sms) {
+    return grown((size_t)d * round_up(qc, 64) * sizeof(float)) +
+           2 * grown((size_t)k * qc * sizeof(float)) +
+           grown(scratch_for(method, N, qc, d, k, num_sms));
+}
+
 // The body shared by the three host entry points.
 bool host_entry(int method, const float *ref, int ref_nb, const float *query, int query_nb,
                 int dim, int k, float *knn_dist, int *knn_index) {
@@ -341,11 +403,6 @@ bool host_entry(int method, const float *ref, int ref_nb, const float *query, in
         std::printf("ERROR: %s: invalid sizes (ref_nb=%d query_nb=%d dim=%d k=%d; "
                     "need >= 1 and k <= ref_nb)\n",
                     method_name(method), ref_nb, query_nb, dim, k);
-        return false;
-    }
-    if (!exact_supported_k(k)) {
-        std::printf("ERROR: %s: k=%d exceeds the supported maximum of 256\n",
-                    method_name(method), k);
         return false;
     }
     Workspace *ws = nullptr;
@@ -366,9 +423,21 @@ bool host_entry(int method, const float *ref, int ref_nb, const float *query, in
         cudaGetLastError();
         return false;
     }
-    const long long ldr = round_up(ref_nb, 64), ldq = round_up(query_nb, 64);
-    const size_t out_elems = (size_t)k * query_nb;
-    const size_t scratch = scratch_for(method, ref_nb, query_nb, dim, k, ws->num_sms);
+    const long long ldr = round_up(ref_nb, 64);
+    const bool tc = use_tc(method, ref_nb, query_nb, dim, k);
+    const size_t fixed = grown((size_t)dim * ldr * sizeof(float)) +
+                         (tc ? grown(tc_ref_bytes(ref_nb, dim)) : 0);
+    const int qc = plan_query_chunk(*ws, query_nb, fixed, [&](int c) {
+        return host_chunk_bytes(method, ref_nb, c, dim, k, ws->num_sms);
+    });
+    if (qc < 1) {
+        std::printf("ERROR: Memory allocation error\n");
+        return false;
+    }
+    g_last_chunks = (query_nb + qc - 1) / qc;
+    const long long ldq = round_up(qc, 64);
+    const size_t out_elems = (size_t)k * qc;
+    const size_t scratch = scratch_for(method, ref_nb, qc, dim, k, ws->num_sms);
     if (!ws->ref.ensure((size_t)dim * ldr * sizeof(float)) ||
         !ws->qry.ensure((size_t)dim * ldq * sizeof(float)) ||
         !ws->dist.ensure(out_elems * sizeof(float)) ||
@@ -379,52 +448,74 @@ bool host_entry(int method, const float *ref, int ref_nb, const float *query, in
     cudaStream_t st = ws->stream;
     float *ref_d = static_cast<float *>(ws->ref.ptr);
     float *qry_d = static_cast<float *>(ws->qry.ptr);
-    const bool streamed = use_tc(method, ref_nb, query_nb, dim, k) &&
-                          ref_nb >= kStreamMinPoints && host_pinned(ref);
+    // the streamed reference copy serves a call that runs as one chunk
+    const bool streamed = tc && qc == query_nb && ref_nb >= kStreamMinPoints && host_pinned(ref);
     cudaError_t e0 = streamed ? cudaSuccess
                               : cudaMemcpy2DAsync(ref_d, ldr * sizeof(float), ref,
                                                   ref_nb * sizeof(float), ref_nb * sizeof(float),
                                                   dim, cudaMemcpyHostToDevice, st);
-    cudaError_t e1 = cudaMemcpy2DAsync(qry_d, ldq * sizeof(float), query,
-                                       query_nb * sizeof(float), query_nb * sizeof(float), dim,
-                                       cudaMemcpyHostToDevice, st);
     cudaError_t e2 = cudaMemsetAsync(ws->status.ptr, 0, sizeof(int), st);
-    if (e0 != cudaSuccess || e1 != cudaSuccess || e2 != cudaSuccess) {
+    if (e0 != cudaSuccess || e2 != cudaSuccess) {
         std::printf("ERROR: Unable to copy data from host to device\n");
         cudaGetLastError();
         return false;
     }
-    ExactProblem p;
-    p.ref = ref_d;
-    p.N = ref_nb;
-    p.ldr = ldr;
-    p.qry = qry_d;
-    p.Q = query_nb;
-    p.ldq = ldq;
-    p.d = dim;
-    p.k = k;
-    p.out_dist = static_cast<float *>(ws->dist.ptr);
-    p.out_idx = static_cast<int *>(ws->idx.ptr);
-    p.ld_out = query_nb;
-    p.scratch = ws->scratch.ptr;
-    p.scratch_bytes = ws->scratch.bytes;
-    p.status = static_cast<int *>(ws->status.ptr);
-    p.num_sms = ws->num_sms;
-    p.force_splits = 0;
-    rc = streamed ? enqueue_tc_streamed(*ws, p, ref, st) : enqueue(*ws, p, method, st);
-    if (rc != kOk) {
-        std::printf("ERROR: Unable to execute kernel (%s)\n", knnb200_status_string(rc));
-        cudaGetLastError();
-        return false;
+    long long stats[3] = {0, 0, 0};   // second scan, exact, candidates over the chunks
+    for (int q0 = 0; q0 < query_nb; q0 += qc) {
+        const int n = std::min(qc, query_nb - q0);
+        if (cudaMemcpy2DAsync(qry_d, ldq * sizeof(float), query + q0, query_nb * sizeof(float),
+                              n * sizeof(float), dim, cudaMemcpyHostToDevice,
+                              st) != cudaSuccess) {
+            std::printf("ERROR: Unable to copy data from host to device\n");
+            cudaGetLastError();
+            return false;
+        }
+        ExactProblem p;
+        p.ref = ref_d;
+        p.N = ref_nb;
+        p.ldr = ldr;
+        p.qry = qry_d;
+        p.Q = n;
+        p.ldq = ldq;
+        p.d = dim;
+        p.k = k;
+        p.out_dist = static_cast<float *>(ws->dist.ptr);
+        p.out_idx = static_cast<int *>(ws->idx.ptr);
+        p.ld_out = n;
+        p.scratch = ws->scratch.ptr;
+        p.scratch_bytes = ws->scratch.bytes;
+        p.status = static_cast<int *>(ws->status.ptr);
+        p.num_sms = ws->num_sms;
+        p.force_splits = 0;
+        rc = streamed ? enqueue_tc_streamed(*ws, p, ref, st)
+                      : enqueue(*ws, p, method, st, /*ref_prepared=*/q0 > 0);
+        if (rc != kOk) {
+            std::printf("ERROR: Unable to execute kernel (%s)\n", knnb200_status_string(rc));
+            cudaGetLastError();
+            return false;
+        }
+        stats[0] += ws->tc_stats[0];
+        stats[1] += ws->tc_stats[1];
+        stats[2] += *reinterpret_cast<const long long *>(ws->tc_stats + 4);
+        e0 = cudaMemcpy2DAsync(knn_dist + q0, query_nb * sizeof(float), p.out_dist,
+                               n * sizeof(float), n * sizeof(float), k, cudaMemcpyDeviceToHost,
+                               st);
+        cudaError_t e1 = cudaMemcpy2DAsync(knn_index + q0, query_nb * sizeof(int), p.out_idx,
+                                           n * sizeof(int), n * sizeof(int), k,
+                                           cudaMemcpyDeviceToHost, st);
+        if (e0 != cudaSuccess || e1 != cudaSuccess) {
+            std::printf("ERROR: Unable to copy data from device to host (%s)\n",
+                        cudaGetErrorString(cudaGetLastError()));
+            return false;
+        }
     }
-    e0 = cudaMemcpyAsync(knn_dist, p.out_dist, out_elems * sizeof(float), cudaMemcpyDeviceToHost,
-                         st);
-    e1 = cudaMemcpyAsync(knn_index, p.out_idx, out_elems * sizeof(int), cudaMemcpyDeviceToHost,
-                         st);
+    ws->tc_stats[0] = (int)stats[0];
+    ws->tc_stats[1] = (int)stats[1];
+    *reinterpret_cast<long long *>(ws->tc_stats + 4) = stats[2];
     e2 = cudaMemcpyAsync(ws->status_host, ws->status.ptr, sizeof(int), cudaMemcpyDeviceToHost,
                          st);
     cudaError_t e3 = cudaStreamSynchronize(st);
-    if (e0 != cudaSuccess || e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+    if (e2 != cudaSuccess || e3 != cudaSuccess) {
         std::printf("ERROR: Unable to copy data from device to host (%s)\n",
                     cudaGetErrorString(e3 != cudaSuccess ? e3 : cudaGetLastError()));
         cudaGetLastError();
@@ -501,32 +592,74 @@ int knnb200_knn_device(const float *ref, int ref_nb, long long ref_ld, const flo
     int dev = 0;
     cudaGetDevice(&dev);
     if (!ws->setup(dev)) return KNNB200_ECUDA;
-    if (!ws->scratch.ensure(scratch_for(method, ref_nb, query_nb, dim, k, ws->num_sms)))
+    // inputs and outputs are the caller's: only the scratch (and the tensor
+    // path's prepared reference set) grow with the call; queries that do not
+    // fit in one go run in chunks (column offsets into the caller's arrays)
+    const bool tc = use_tc(method, ref_nb, query_nb, dim, k);
+    const int qc = plan_query_chunk(*ws, query_nb, tc ? grown(tc_ref_bytes(ref_nb, dim)) : 0,
+                                    [&](int c) {
+                                        return grown(scratch_for(method, ref_nb, c, dim, k,
+                                                                 ws->num_sms));
+                                    });
+    if (qc < 1) return KNNB200_ENOMEM;
+    g_last_chunks = (query_nb + qc - 1) / qc;
+    if (!ws->scratch.ensure(scratch_for(method, ref_nb, qc, dim, k, ws->num_sms)))
         return KNNB200_ENOMEM;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // Calls on one device share the workspace scratch: order them.
     if (cudaStreamWaitEvent(st, ws->last_done, 0) != cudaSuccess) return KNNB200_ECUDA;
     if (cudaMemsetAsync(ws->status.ptr, 0, sizeof(int), st) != cudaSuccess) return KNNB200_ECUDA;
-    ExactProblem p;
-    p.ref = ref;
-    p.N = ref_nb;
-    p.ldr = ref_ld;
-    p.qry = query;
-    p.Q = query_nb;
-    p.ldq = query_ld;
-    p.d = dim;
-    p.k = k;
-    p.out_dist = knn_dist;
-    p.out_idx = knn_index;
-    p.ld_out = out_ld;
-    p.scratch = ws->scratch.ptr;
-    p.scratch_bytes = ws->scratch.bytes;
-    p.status = static_cast<int *>(ws->status.ptr);
-    p.num_sms = ws->num_sms;
-    p.force_splits = 0;
-    rc = enqueue(*ws, p, method, st);
+    long long stats[3] = {0, 0, 0};
+    for (int q0 = 0; q0 < query_nb && rc == kOk; q0 += qc) {
+        ExactProblem p;
+        p.ref = ref;
+        p.N = ref_nb;
+        p.ldr = ref_ld;
+        p.qry = query + q0;
+        p.Q = std::min(qc, query_nb - q0);
+        p.ldq = query_ld;
+        p.d = dim;
+        p.k = k;
+        p.out_dist = knn_dist + q0;
+        p.out_idx = knn_index + q0;
+        p.ld_out = out_ld;
+        p.scratch = ws->scratch.ptr;
+        p.scratch_bytes = ws->scratch.bytes;
+        p.status = static_cast<int *>(ws->status.ptr);
+        p.num_sms = ws->num_sms;
+        p.force_splits = 0;
+        rc = enqueue(*ws, p, method, st, /*ref_prepared=*/q0 > 0);
+        stats[0] += ws->tc_stats[0];
+        stats[1] += ws->tc_stats[1];
+        stats[2] += *reinterpret_cast<const long long *>(ws->tc_stats + 4);
+    }
+    ws->tc_stats[0] = (int)stats[0];
+    ws->tc_stats[1] = (int)stats[1];
+    *reinterpret_cast<long long *>(ws->tc_stats + 4) = stats[2];
     if (cudaEventRecord(ws->last_done, st) != cudaSuccess && rc == kOk) rc = kErrCuda;
     return rc;
+}
+
+void knnb200_set_memory_cap(size_t bytes) {
+    Workspace *ws = nullptr;
+    if (current_workspace(ws) != kOk) return;
+    std::lock_guard<std::mutex> lock(ws->mu);
+    g_mem_cap = bytes;
+}
+
+int knnb200_last_query_chunks(void) { return g_last_chunks; }
+
+size_t knnb200_call_bytes(int ref_nb, int query_nb, int dim, int k, int method, int host) {
+    if (!valid_sizes(ref_nb, query_nb, dim, k)) return 0;
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    const bool tc = use_tc(method, ref_nb, query_nb, dim, k);
+    const size_t tcb = tc ? grown(tc_ref_bytes(ref_nb, dim)) : 0;
+    if (!host) return tcb + grown(scratch_for(method, ref_nb, query_nb, dim, k, sms));
+    return grown((size_t)dim * round_up(ref_nb, 64) * sizeof(float)) + tcb +
+           host_chunk_bytes(method, ref_nb, query_nb, dim, k, sms);
 }
 
 int knnb200_sync_status(void *stream) {
@@ -630,6 +763,41 @@ void knnb200_last_tc_stats(long long *candidates, int *second_scan, int *exact) 
     if (candidates) *candidates = *reinterpret_cast<const long long *>(ws->tc_stats + 4);
     if (second_scan) *second_scan = ws->tc_stats[0];
     if (exact) *exact = ws->tc_stats[1];
+}
+
+int knnb200_set_bound_check(int enable) {
+    Workspace *ws = nullptr;
+    int rc = current_workspace(ws);
+    if (rc != kOk) return rc;
+    std::lock_guard<std::mutex> lock(ws->mu);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!ws->setup(dev)) return KNNB200_ECUDA;
+    if (enable) {
+        if (!ws->bound.ensure(16)) return KNNB200_ENOMEM;
+        if (cudaMemset(ws->bound.ptr, 0, 16) != cudaSuccess) return KNNB200_ECUDA;
+    }
+    ws->bound_check = enable != 0;
+    return KNNB200_OK;
+}
+
+int knnb200_last_bound_check(double *max_ratio, long long *checked) {
+    if (max_ratio) *max_ratio = 0.0;
+    if (checked) *checked = 0;
+    Workspace *ws = nullptr;
+    int rc = current_workspace(ws);
+    if (rc != kOk) return rc;
+    std::lock_guard<std::mutex> lock(ws->mu);
+    if (!ws->init || !ws->bound.ptr) return KNNB200_EINVAL;
+    unsigned v[4] = {0, 0, 0, 0};
+    if (cudaStreamSynchronize(ws->stream) != cudaSuccess ||
+        cudaMemcpy(v, ws->bound.ptr, 16, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return KNNB200_ECUDA;
+    float r;
+    std::memcpy(&r, &v[0], 4);
+    if (max_ratio) *max_ratio = r;
+    if (checked) *checked = (long long)v[2] | ((long long)v[3] << 32);
+    return KNNB200_OK;
 }
 
 const char *knnb200_version(void) { return "knnb200 0.1.0 (sm_100a)"; }

@@ -27,6 +27,13 @@
 //   * With one split the kernel writes sqrt(distance) and the index straight
 //     into the k x query_nb output; with several splits it writes each
 //     split's sorted keys to scratch and knn_merge_splits_kernel merges them.
+//   * k > 256 (the reference's insertion sort has no limit on k,
+//     code/knncuda.cu:143-189) runs in passes over the whole set: pass p
+//     keeps the 256 smallest keys at or above a per-query lower bound (one
+//     more than the last key of pass p - 1) and writes output rows
+//     256 p .. 256 p + 255.  Keys are unique, so the passes together return
+//     exactly the k smallest keys in order, with the same distances and tie
+//     order as a single pass.
 #include <algorithm>
 #include <cstdio>
 
@@ -35,7 +42,7 @@
 
 namespace knnb200 {
 
-template <int QPW, int KCAP>
+template <int QPW, int KCAP, bool LB>
 __global__ void __launch_bounds__(EX_THREADS, 1)
     knn_exact_kernel(const __grid_constant__ CUtensorMap tm_ref,
                      const __grid_constant__ CUtensorMap tm_qry, ExactArgs a) {
@@ -101,6 +108,12 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
     for (int i = lane; i < QPW * C::REGION; i += 32) wl[i] = kKeyInf;
     __syncwarp();
     uint32_t nb = 0;   // candidate buffer fills
+    unsigned long long lbk[QPW];
+#pragma unroll
+    for (int i = 0; i < QPW; ++i) {
+        const int q = qtile * C::BQ + warp * QPW + i;
+        lbk[i] = (LB && q < a.Q) ? a.lb[q] : 0ull;
+    }
 
     int it = 0;
     for (int rt = t0; rt < t1; ++rt) {
@@ -108,7 +121,7 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
         if (!consume_ref_tile<QPW, KCAP>(acc, stages, full, empty, abort_flag, it, a.n_dchunks,
                                          warp, lane, a.status))
             break;
-        select_tile<QPW, KCAP>(wl, nb, acc, rt, a.N, a.k, lane);
+        select_tile<QPW, KCAP, LB>(wl, nb, acc, rt, a.N, a.k, lane, lbk);
     }
     flush_all<QPW, KCAP>(wl, nb, a.k, lane);
 
@@ -123,8 +136,9 @@ __global__ void __launch_bounds__(EX_THREADS, 1)
             const int j = e / C::BQ, qi = e - j * C::BQ, q = q0 + qi;
             if (q < a.Q) {
                 const unsigned long long key = lists[(size_t)qi * C::REGION + j];
-                a.out_dist[(size_t)j * a.ld_out + q] = sqrtf(key_dist2(key));
-                a.out_idx[(size_t)j * a.ld_out + q] = key_index(key);
+                a.out_dist[(size_t)(a.row0 + j) * a.ld_out + q] = sqrtf(key_dist2(key));
+                a.out_idx[(size_t)(a.row0 + j) * a.ld_out + q] = key_index(key);
+                if (a.lb_out && j == a.k - 1) a.lb_out[q] = key + 1;
             }
         }
     } else {
@@ -154,7 +168,8 @@ __global__ void dup_queries_kernel(const float *__restrict__ src, int Q, long lo
 // An element's output position is the sum of its ranks in every list.
 __global__ void knn_merge_splits_kernel(const unsigned long long *__restrict__ part, int S,
                                         int Q, int k, float *__restrict__ out_dist,
-                                        int *__restrict__ out_idx, long long ld_out) {
+                                        int *__restrict__ out_idx, long long ld_out, int row0,
+                                        unsigned long long *__restrict__ lb_out) {
     extern __shared__ unsigned long long msm[];
     const int wpb = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -173,8 +188,9 @@ __global__ void knn_merge_splits_kernel(const unsigned long long *__restrict__ p
         for (int u = 0; u < S && pos < k; ++u)
             if (u != t) pos += rank_sorted(L + (size_t)u * k, k, x);
         if (pos < k) {
-            out_dist[(size_t)pos * ld_out + q] = sqrtf(key_dist2(x));
-            out_idx[(size_t)pos * ld_out + q] = key_index(x);
+            out_dist[(size_t)(row0 + pos) * ld_out + q] = sqrtf(key_dist2(x));
+            out_idx[(size_t)(row0 + pos) * ld_out + q] = key_index(x);
+            if (lb_out && pos == k - 1) lb_out[q] = x + 1;
         }
     }
 }
@@ -200,12 +216,17 @@ void shape_of(ExactShape &s) {
     s.smem = C::SMEM;
 }
 
-bool choose_shape(int N, int Q, int d, int k, int num_sms, ExactShape &s) {
+// Ranks selected by one pass of the kernel: k <= 256 in one pass, larger k
+// in passes of 256 (the last one may be shorter).
+constexpr int kPassRanks = 256;
+
+bool choose_shape(int N, int Q, int d, int k_all, int num_sms, ExactShape &s) {
+    if (k_all < 1) return false;
+    const int k = std::min(k_all, kPassRanks);
     if (k <= 32) shape_of<EX_QPW, 32>(s);
     else if (k <= 64) shape_of<EX_QPW, 64>(s);
     else if (k <= 128) shape_of<EX_QPW, 128>(s);
-    else if (k <= 256) shape_of<EX_QPW_K256, 256>(s);
-    else return false;
+    else shape_of<EX_QPW_K256, 256>(s);
     s.n_rtiles = (N + EX_BR - 1) / EX_BR;
     s.n_dchunks = (d + EX_BD - 1) / EX_BD;
     const int qtiles = (Q + s.bq - 1) / s.bq;
@@ -234,11 +255,11 @@ bool choose_shape(int N, int Q, int d, int k, int num_sms, ExactShape &s) {
     return true;
 }
 
-template <int QPW, int KCAP>
+template <int QPW, int KCAP, bool LB = false>
 cudaError_t launch_t(const CUtensorMap &mr, const CUtensorMap &mq, const ExactArgs &a,
                      int qtiles, cudaStream_t st) {
     using C = ExCfg<QPW, KCAP>;
-    auto kern = knn_exact_kernel<QPW, KCAP>;
+    auto kern = knn_exact_kernel<QPW, KCAP, LB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)C::SMEM);
     if (e != cudaSuccess) return e;
@@ -253,7 +274,8 @@ cudaError_t launch_t(const CUtensorMap &mr, const CUtensorMap &mq, const ExactAr
 static long long qdup_pitch2(int Q) { return ((long long)Q + 31) / 32 * 32; }
 
 int launch_split_merge(const unsigned long long *part, int S, int Q, int k, float *out_dist,
-                       int *out_idx, long long ld_out, cudaStream_t st) {
+                       int *out_idx, long long ld_out, cudaStream_t st, int row0,
+                       unsigned long long *lb_out) {
     const size_t per_warp = (size_t)S * k * 8;
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (160u * 1024u) / per_warp));
     const size_t smem = per_warp * wpb;
@@ -263,21 +285,34 @@ int launch_split_merge(const unsigned long long *part, int S, int Q, int k, floa
     if (cudaFuncSetAttribute(knn_merge_splits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kMergeSmemMax) != cudaSuccess)
         return kErrLaunch;
-    knn_merge_splits_kernel<<<(Q + wpb - 1) / wpb, wpb * 32, smem, st>>>(part, S, Q, k, out_dist,
-                                                                       out_idx, ld_out);
+    knn_merge_splits_kernel<<<(Q + wpb - 1) / wpb, wpb * 32, smem, st>>>(
+        part, S, Q, k, out_dist, out_idx, ld_out, row0, lb_out);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
+}
+
+// Scratch of the exact path: the (q, q)-duplicated queries, 256 bytes of
+// alignment, the per-split key lists of one pass when the reference set is
+// split, and for k > 256 the per-query lower-bound keys of the passes.
+static size_t exact_need(const ExactShape &s, int Q, int d, int k, size_t *part_off,
+                         size_t *lb_off) {
+    const int kp = std::min(k, kPassRanks);
+    const size_t dup = (size_t)d * qdup_pitch2(Q) * sizeof(float2);
+    const size_t off = (dup + 255) & ~size_t(255);
+    const size_t part = s.splits > 1 ? (size_t)s.splits * Q * kp * 8 : 0;
+    const size_t lb = k > kPassRanks ? (size_t)Q * 8 : 0;
+    if (part_off) *part_off = off;
+    if (lb_off) *lb_off = off + part;
+    return std::max(dup + 256, off) + part + lb;
 }
 
 size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     if (lowdim_applies(N, Q, d, k)) return lowdim_scratch_bytes(N, Q, d, k, num_sms);
     ExactShape s;
     if (!choose_shape(N, Q, d, k, num_sms, s)) return 0;
-    const size_t dup = (size_t)d * qdup_pitch2(Q) * sizeof(float2);
-    const size_t part = s.splits > 1 ? (size_t)s.splits * Q * k * sizeof(unsigned long long) : 0;
-    return dup + 256 + part;
+    return exact_need(s, Q, d, k, nullptr, nullptr);
 }
 
-bool exact_supported_k(int k) { return k >= 1 && k <= 256; }
+bool exact_supported_k(int k) { return k >= 1; }
 
 int launch_exact(const ExactProblem &p, cudaStream_t st) {
     if (lowdim_applies(p.N, p.Q, p.d, p.k)) return launch_lowdim(p, st);
@@ -285,12 +320,12 @@ int launch_exact(const ExactProblem &p, cudaStream_t st) {
     if (!choose_shape(p.N, p.Q, p.d, p.k, p.num_sms, s)) return kErrUnsupported;
     if (p.force_splits > 0) s.splits = std::min(p.force_splits, std::min(s.n_rtiles, 256));
     const long long ld2 = qdup_pitch2(p.Q);
-    const size_t dup = (size_t)p.d * ld2 * sizeof(float2);
-    const size_t need = dup + 256 + (s.splits > 1 ? (size_t)s.splits * p.Q * p.k * 8 : 0);
-    if (need > p.scratch_bytes) return kErrScratch;
+    size_t part_off = 0, lb_off = 0;
+    if (exact_need(s, p.Q, p.d, p.k, &part_off, &lb_off) > p.scratch_bytes) return kErrScratch;
     float2 *qdup = static_cast<float2 *>(p.scratch);
-    unsigned long long *part = reinterpret_cast<unsigned long long *>(
-        static_cast<unsigned char *>(p.scratch) + ((dup + 255) & ~size_t(255)));
+    unsigned char *sb = static_cast<unsigned char *>(p.scratch);
+    unsigned long long *part = reinterpret_cast<unsigned long long *>(sb + part_off);
+    unsigned long long *lb = reinterpret_cast<unsigned long long *>(sb + lb_off);
     dup_queries_kernel<<<dim3((p.Q + 255) / 256, p.d), 256, 0, st>>>(p.qry, p.Q, p.ldq, p.d, qdup,
                                                                    ld2);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
@@ -306,7 +341,6 @@ int launch_exact(const ExactProblem &p, cudaStream_t st) {
     a.N = p.N;
     a.Q = p.Q;
     a.d = p.d;
-    a.k = p.k;
     a.n_rtiles = s.n_rtiles;
     a.n_splits = s.splits;
     a.n_dchunks = s.n_dchunks;
@@ -315,22 +349,36 @@ int launch_exact(const ExactProblem &p, cudaStream_t st) {
     a.ld_out = p.ld_out;
     a.part = part;
     a.status = p.status;
+    a.lb = lb;
     const int qtiles = (p.Q + s.bq - 1) / s.bq;
-
-    cudaError_t e;
-    switch (s.kcap) {
-        case 32: e = launch_t<EX_QPW, 32>(mr, mq, a, qtiles, st); break;
-        case 64: e = launch_t<EX_QPW, 64>(mr, mq, a, qtiles, st); break;
-        case 128: e = launch_t<EX_QPW, 128>(mr, mq, a, qtiles, st); break;
-        default: e = launch_t<EX_QPW_K256, 256>(mr, mq, a, qtiles, st); break;
-    }
-    if (e != cudaSuccess) return kErrLaunch;
-    if (p.timer) p.timer->mark(st, kPhaseExactMain);
-    if (s.splits > 1) {
-        const int rc = launch_split_merge(a.part, s.splits, p.Q, p.k, p.out_dist, p.out_idx,
-                                          p.ld_out, st);
-        if (rc != kOk) return rc;
-        if (p.timer) p.timer->mark(st, kPhaseExactMerge);
+    const bool multi = p.k > kPassRanks;
+    // ranks [row0, row0 + a.k) per pass
+    for (int row0 = 0; row0 < p.k; row0 += kPassRanks) {
+        a.k = std::min(kPassRanks, p.k - row0);
+        a.row0 = row0;
+        a.lb_out = (multi && row0 + a.k < p.k) ? lb : nullptr;
+        cudaError_t e;
+        if (multi) {
+            // pass 0 has no lower bound; every later pass starts above the
+            // last key of the one before
+            e = row0 == 0 ? launch_t<EX_QPW_K256, 256, false>(mr, mq, a, qtiles, st)
+                          : launch_t<EX_QPW_K256, 256, true>(mr, mq, a, qtiles, st);
+        } else {
+            switch (s.kcap) {
+                case 32: e = launch_t<EX_QPW, 32>(mr, mq, a, qtiles, st); break;
+                case 64: e = launch_t<EX_QPW, 64>(mr, mq, a, qtiles, st); break;
+                case 128: e = launch_t<EX_QPW, 128>(mr, mq, a, qtiles, st); break;
+                default: e = launch_t<EX_QPW_K256, 256>(mr, mq, a, qtiles, st); break;
+            }
+        }
+        if (e != cudaSuccess) return kErrLaunch;
+        if (p.timer) p.timer->mark(st, kPhaseExactMain);
+        if (s.splits > 1) {
+            const int rc = launch_split_merge(a.part, s.splits, p.Q, a.k, p.out_dist, p.out_idx,
+                                              p.ld_out, st, row0, a.lb_out);
+            if (rc != kOk) return rc;
+            if (p.timer) p.timer->mark(st, kPhaseExactMerge);
+        }
     }
     return kOk;
 }

@@ -155,9 +155,11 @@ KNN_DI void flush_all(unsigned long long *wl, uint32_t &nb, int k, int lane) {
 // grows geometrically as the list tightens) instead of one per half tile
 // that holds any survivor.  nb packs the warp-uniform buffer fills.
 // d2(i, j) gives the squared distance of query i to the lane's j-th point.
-template <int QPW, int KCAP, typename D2>
-KNN_DI void select_half(unsigned long long *wl, uint32_t &nb, D2 d2, uint32_t rbase, int N,
-                        int k, int lane) {
+// With LB, only keys >= lb[i] are selected: pass p of a k > 256 problem keeps
+// the 256 smallest keys above the ones earlier passes returned.
+template <int QPW, int KCAP, bool LB, typename D2>
+KNN_DI void select_half_lb(unsigned long long *wl, uint32_t &nb, D2 d2, uint32_t rbase, int N,
+                           int k, int lane, const unsigned long long (&lb)[QPW]) {
     constexpr int REGION = KCAP + EX_CB;
     unsigned long long tau[QPW];
 #pragma unroll
@@ -170,7 +172,9 @@ KNN_DI void select_half(unsigned long long *wl, uint32_t &nb, D2 d2, uint32_t rb
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const uint32_t idx = rbase + j;
-            const bool p = (idx < (uint32_t)N) && make_key(d2(i, j), idx) < tau[i];
+            const unsigned long long key = make_key(d2(i, j), idx);
+            bool p = (idx < (uint32_t)N) && key < tau[i];
+            if (LB) p = p && key >= lb[i];
             pm[i] |= (p ? 1u : 0u) << j;
             any |= p;
         }
@@ -205,6 +209,13 @@ KNN_DI void select_half(unsigned long long *wl, uint32_t &nb, D2 d2, uint32_t rb
         nb = nbuf_set(nb, i, c);
     }
     __syncwarp();
+}
+
+template <int QPW, int KCAP, typename D2>
+KNN_DI void select_half(unsigned long long *wl, uint32_t &nb, D2 d2, uint32_t rbase, int N,
+                        int k, int lane) {
+    const unsigned long long none[QPW] = {};
+    select_half_lb<QPW, KCAP, false>(wl, nb, d2, rbase, N, k, lane, none);
 }
 
 
@@ -261,20 +272,26 @@ KNN_DI bool consume_ref_tile(f32x2_t (&acc)[QPW][4], const float *stages, uint64
 }
 
 // Select both halves of a consumed tile (reference points rt*256 + ...).
-template <int QPW, int KCAP>
+template <int QPW, int KCAP, bool LB = false>
 KNN_DI void select_tile(unsigned long long *wl, uint32_t &nb, f32x2_t (&acc)[QPW][4], int rt,
-                        int N, int k, int lane) {
+                        int N, int k, int lane, const unsigned long long (&lb)[QPW]) {
     const uint32_t rb0 = (uint32_t)rt * EX_BR + lane * 4;
-    select_half<QPW, KCAP>(
+    select_half_lb<QPW, KCAP, LB>(
         wl, nb,
         [&](int i, int j) { return (j & 1) ? f2_hi(acc[i][j >> 1]) : f2_lo(acc[i][j >> 1]); },
-        rb0, N, k, lane);
-    select_half<QPW, KCAP>(
+        rb0, N, k, lane, lb);
+    select_half_lb<QPW, KCAP, LB>(
         wl, nb,
         [&](int i, int j) {
             return (j & 1) ? f2_hi(acc[i][2 + (j >> 1)]) : f2_lo(acc[i][2 + (j >> 1)]);
         },
-        rb0 + 128, N, k, lane);
+        rb0 + 128, N, k, lane, lb);
+}
+template <int QPW, int KCAP>
+KNN_DI void select_tile(unsigned long long *wl, uint32_t &nb, f32x2_t (&acc)[QPW][4], int rt,
+                        int N, int k, int lane) {
+    const unsigned long long none[QPW] = {};
+    select_tile<QPW, KCAP, false>(wl, nb, acc, rt, N, k, lane, none);
 }
 
 // Number of elements of sorted A[0..n) below x.

@@ -68,6 +68,12 @@ struct ExactArgs {
     long long ld_out;
     unsigned long long *part;   // [n_splits][Q][k] keys when n_splits > 1
     int *status;                // device status word (DeviceStatus)
+    // k > 256 runs in passes of up to 256 ranks: pass p selects keys >= lb[q]
+    // (LB kernels only), writes output rows row0 .. row0 + k - 1 and, when
+    // lb_out is set, lb_out[q] = (its k-th key) + 1 for the next pass
+    const unsigned long long *lb;
+    unsigned long long *lb_out;
+    int row0;
 };
 
 // One exact k-NN problem on device-resident, dim x n row-major inputs.
@@ -107,9 +113,11 @@ bool lowdim_applies(int N, int Q, int d, int k);
 size_t lowdim_scratch_bytes(int N, int Q, int d, int k, int num_sms);
 int lowdim_plan_splits(int N, int Q, int d, int k, int num_sms);
 int launch_lowdim(const ExactProblem &p, cudaStream_t st);
-// Merge per-split sorted key lists [S][Q][k] into the k x Q output.
+// Merge per-split sorted key lists [S][Q][k] into rows row0 .. row0 + k - 1
+// of the output; with lb_out, lb_out[q] = (k-th merged key) + 1.
 int launch_split_merge(const unsigned long long *part, int S, int Q, int k, float *out_dist,
-                       int *out_idx, long long ld_out, cudaStream_t st);
+                       int *out_idx, long long ld_out, cudaStream_t st, int row0 = 0,
+                       unsigned long long *lb_out = nullptr);
 size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms);
 int exact_plan_splits(int N, int Q, int d, int k, int num_sms);
 int launch_exact(const ExactProblem &p, cudaStream_t st);
@@ -139,6 +147,10 @@ struct TcProblem {
     int *status;
     int num_sms;
     PhaseTimer *timer = nullptr;
+    // test-only bound check of the re-rank (nullptr = off): [0] max over
+    // re-ranked candidates of |a + ||q||^2 - D| / E_q (float bits), [2..3]
+    // candidates checked (64-bit)
+    unsigned *bound_stat = nullptr;
 };
 
 // A sample of the 256-point tiles: `run` consecutive tiles out of every

@@ -16,8 +16,8 @@
 //   * a call needs the exact path's whole scratch in it: the query set
 //     duplicated into (q, q) pairs (dim * round_up(query_nb, 32) * 8 bytes),
 //     256 bytes of alignment and, when the planner splits the reference set,
-//     splits * query_nb * k * 8 bytes of per-split lists (for k > 256 also
-//     query_nb * 8 bytes of lower-bound keys).  knnb200_scratch_bytes(...,
+//     splits * query_nb * min(k, 256) * 8 bytes of per-split lists (for
+//     k > 256 also query_nb * 8 bytes of lower-bound keys).  knnb200_scratch_bytes(...,
 //     KNNB200_METHOD_GLOBAL) gives the exact figure; a call needing more
 //     than the static area is rejected with KNNB200_ESCRATCH before anything
 //     runs;

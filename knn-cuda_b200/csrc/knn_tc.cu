@@ -769,8 +769,21 @@ KNN_DI bool rr_reject_list(int c, int cmax, int k, int q, float qq, float r2, fl
 // (steps s = (group, chunk); the copies of steps s + 1 .. s + NBUF - 1
 // overlap step s), and each lane runs its candidate's FMA chain against the
 // query qv (d_pad floats) in increasing d.
+//
+// Bound check (STAT, a test-only instantiation): before a key is replaced,
+// its entry still holds the BF16-expansion value a of that candidate; the
+// lane records |a + ||q||^2 - D| / E_q (D the exact FP32 distance, qq =
+// ||q||^2, E_q = e_q) as float bits in stat[0] (atomic max) and counts the
+// candidates checked in the 64-bit counter at stat + 2.
+struct BoundStat {
+    float qq, e_q;
+    unsigned *stat;
+};
+
+template <bool STAT = false>
 KNN_DI void rr_exact_distances(unsigned long long *keys, int n, const float *__restrict__ refT,
-                               int d_pad, const float *qv, float *rows, int lane) {
+                               int d_pad, const float *qv, float *rows, int lane,
+                               BoundStat bs = BoundStat{0.f, 0.f, nullptr}) {
     const int nch = d_pad / TC_RR_DCH;
     const int total = ((n + 31) / 32) * nch;
     constexpr int CPL = TC_RR_DCH / 4;   // 16-byte copies per row and chunk
@@ -823,6 +836,12 @@ KNN_DI void rr_exact_distances(unsigned long long *keys, int n, const float *__r
         __syncwarp();   // this buffer is refilled NBUF - 1 steps later
         if (ch == nch - 1) {
             const int t = g * 32 + lane;
+            if (STAT && t < n) {
+                const float a = ord_float((uint32_t)(keys[t] >> 32));
+                const float ratio = fabsf(a + bs.qq - acc) / bs.e_q;
+                atomicMax(bs.stat, __float_as_uint(ratio));
+                atomicAdd(reinterpret_cast<unsigned long long *>(bs.stat + 2), 1ull);
+            }
             if (t < n) keys[t] = make_key(acc, (uint32_t)r_cur);
             acc = 0.f;
         }
@@ -856,6 +875,7 @@ KNN_DI void rr_certify(const unsigned long long *keys, int q, float qq, float r2
     }
 }
 
+template <bool STAT>
 __global__ void __launch_bounds__(TC_RR_WARPS * 32)
     tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
                      const float *__restrict__ qry, long long ldq, const float *__restrict__ qn,
@@ -864,7 +884,8 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
                      int cmax, int cpow, int Q, int k, float *__restrict__ out_dist,
                      int *__restrict__ out_idx, long long ld_out, int *__restrict__ fail_list,
                      int *__restrict__ n_fail, float *__restrict__ retry,
-                     unsigned long long *__restrict__ cand_total, int final_pass) {
+                     unsigned long long *__restrict__ cand_total, int final_pass,
+                     unsigned *__restrict__ bound_stat) {
     extern __shared__ unsigned char rsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -906,7 +927,8 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
         }
         n_s = max(cnt, k);   // keys are sorted, so the kept ones are a prefix
     }
-    rr_exact_distances(keys, n_s, refT, d_pad, qv, rows, lane);
+    rr_exact_distances<STAT>(keys, n_s, refT, d_pad, qv, rows, lane,
+                             BoundStat{qq, tc_error_bound(qq, r2, T, d_pad), bound_stat});
     int P2 = 32;
     while (P2 < n_s) P2 <<= 1;
     for (int t = n_s + lane; t < P2; t += 32) keys[t] = kKeyInf;
@@ -1214,14 +1236,16 @@ int rerank(const TcRun &r, cudaStream_t st, int Q, int cmax, const float *qry, l
     const size_t rsmem = (size_t)warps * tc_rr_warp_bytes(r.d_pad, cpow);
     // one fixed limit for every launch, so that calls from several host
     // threads never lower it under each other
+    // the bound statistic runs in its own instantiation, only when asked for
+    auto kern = P.bound_stat ? tc_rerank_kernel<true> : tc_rerank_kernel<false>;
     if (rsmem > kRerankSmem ||
-        cudaFuncSetAttribute(tc_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kRerankSmem) != cudaSuccess)
         return kErrLaunch;
-    tc_rerank_kernel<<<(Q + warps - 1) / warps, warps * 32, rsmem, st>>>(
+    kern<<<(Q + warps - 1) / warps, warps * 32, rsmem, st>>>(
         r.R.refT, P.d, r.d_pad, qry, ldq, qn, r.R.rmax_bits, thr, r.cand, r.count, cmax, cpow,
         Q, P.k, out_dist, out_idx, ld_out, fail, r.nfail, r.retry, r.cand_total,
-        final_pass ? 1 : 0);
+        final_pass ? 1 : 0, P.bound_stat);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 

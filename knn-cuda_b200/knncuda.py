@@ -51,6 +51,8 @@ C_SYMBOLS = (
     "knnb200_batched_plan_create", "knnb200_batched_run", "knnb200_batched_status",
     "knnb200_batched_items", "knnb200_batched_plan_destroy", "knnb200_batched_graph_create",
     "knnb200_graph_launch", "knnb200_graph_destroy", "knnb200_batched_autotune",
+    "knnb200_set_bound_check", "knnb200_last_bound_check", "knnb200_set_memory_cap",
+    "knnb200_last_query_chunks", "knnb200_call_bytes",
 )
 
 
@@ -156,6 +158,17 @@ def lib():
         L.knnb200_batched_autotune.restype = ctypes.c_int
         L.knnb200_batched_autotune.argtypes = [PP, ctypes.c_int, vp, ctypes.POINTER(ctypes.c_int),
                                                ctypes.POINTER(ctypes.c_float)]
+        L.knnb200_set_bound_check.restype = ctypes.c_int
+        L.knnb200_set_bound_check.argtypes = [ctypes.c_int]
+        L.knnb200_last_bound_check.restype = ctypes.c_int
+        L.knnb200_last_bound_check.argtypes = [ctypes.POINTER(ctypes.c_double),
+                                               ctypes.POINTER(ctypes.c_longlong)]
+        L.knnb200_set_memory_cap.restype = None
+        L.knnb200_set_memory_cap.argtypes = [ctypes.c_size_t]
+        L.knnb200_last_query_chunks.restype = ctypes.c_int
+        L.knnb200_last_query_chunks.argtypes = []
+        L.knnb200_call_bytes.restype = ctypes.c_size_t
+        L.knnb200_call_bytes.argtypes = [ctypes.c_int] * 6
         L.knnb200_version.restype = ctypes.c_char_p
         L.knnb200_version.argtypes = []
         _lib = L
@@ -497,6 +510,38 @@ def last_tc_stats() -> dict:
     c, a, b = ctypes.c_longlong(0), ctypes.c_int(0), ctypes.c_int(0)
     lib().knnb200_last_tc_stats(ctypes.byref(c), ctypes.byref(a), ctypes.byref(b))
     return {"candidates": c.value, "second_scan": a.value, "exact": b.value}
+
+
+def set_bound_check(enable: bool) -> None:
+    """Turn the test-only check of the tensor path's error bound on or off."""
+    rc = lib().knnb200_set_bound_check(1 if enable else 0)
+    if rc != 0:
+        raise RuntimeError(f"knnb200_set_bound_check failed: {status_string(rc)}")
+
+
+def last_bound_check() -> tuple:
+    """(max |a + |q|^2 - D| / E_q, candidates checked) of the last tensor-path
+    call made while the check was on."""
+    r, n = ctypes.c_double(0), ctypes.c_longlong(0)
+    rc = lib().knnb200_last_bound_check(ctypes.byref(r), ctypes.byref(n))
+    if rc != 0:
+        raise RuntimeError(f"knnb200_last_bound_check failed: {status_string(rc)}")
+    return r.value, n.value
+
+
+def set_memory_cap(nbytes: int) -> None:
+    """Cap the device memory the library assumes it may use (0 = no cap)."""
+    lib().knnb200_set_memory_cap(int(nbytes))
+
+
+def call_bytes(ref_nb, query_nb, dim, k, method="global", host=True) -> int:
+    """The library's device-memory estimate for one call of this shape."""
+    return lib().knnb200_call_bytes(ref_nb, query_nb, dim, k, METHODS[method], 1 if host else 0)
+
+
+def last_query_chunks() -> int:
+    """Query chunks the last host or device call ran in."""
+    return lib().knnb200_last_query_chunks()
 
 
 def last_fallback_counts() -> tuple:

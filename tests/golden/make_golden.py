@@ -6,7 +6,7 @@ oracle/_ref/libknnref_c.so), on small seeded inputs and stores inputs and
 outputs in tests/golden/*.npz.  The fixtures pin the oracle restatement
 (bit-identical outputs) and serve as parity targets for the CUDA path.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [name ...]
 """
 from __future__ import annotations
 
@@ -61,13 +61,21 @@ def cases():
     rng = np.random.default_rng(18)
     out["single_query"] = (rng.random((64, 700), dtype=np.float32),
                            rng.random((64, 1), dtype=np.float32), 1, "Q=1, k=1")
+    # k well above 256: the reference's insertion sort has no limit on k
+    rng = np.random.default_rng(19)
+    out["large_k"] = (10 * rng.random((8, 2000), dtype=np.float32),
+                      10 * rng.random((8, 24), dtype=np.float32), 1000,
+                      "k=1000 of 2000 points, 10*U[0,1)")
     return out
 
 
-def main():
+def main(names=None):
+    """Write every fixture, or only those named on the command line."""
     if not oracle.ref_available():
         raise SystemExit("oracle/_ref/libknnref_c.so missing: run make -C oracle ref")
     for name, (ref, query, k, note) in cases().items():
+        if names and name not in names:
+            continue
         ref = np.ascontiguousarray(ref, dtype=np.float32)
         query = np.ascontiguousarray(query, dtype=np.float32)
         dist, idx = oracle.ref_knn_c(ref, query, k)
@@ -78,4 +86,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

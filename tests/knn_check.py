@@ -82,3 +82,39 @@ def recall_at_k(idx, i64):
 
 def max_rel_err(dist, d64):
     return float(np.max(np.abs(dist.astype(np.float64) - d64) / np.maximum(np.abs(d64), ABS_FLOOR)))
+
+
+def check_exact_sampled_torch(torch, ref_d, qry_d, dist, idx, sample, rel=REL_TOL):
+    """check_exact on sampled queries of a large problem, with the FP64 brute
+    force computed by torch on the device that holds ref_d (dim x n) and
+    qry_d (dim x Q).  dist / idx: (k, Q) tensors or arrays.  Returns
+    (recall@k, max relative distance error) over the sample."""
+    dist = torch.as_tensor(dist, device=ref_d.device)
+    idx = torch.as_tensor(idx, device=ref_d.device).long()
+    k = idx.shape[0]
+    r64 = ref_d.double()
+    hits, worst = 0, 0.0
+    for q in sample:
+        d2 = ((r64 - qry_d[:, q].double()[:, None]) ** 2).sum(0)
+        top = torch.topk(d2, k, largest=False)           # ascending (sorted=True)
+        truth_d = torch.sqrt(top.values)
+        mine_i = idx[:, q]
+        mine_d = dist[:, q].double()
+        exact_mine = torch.sqrt(d2[mine_i])
+        tol = torch.clamp(rel * exact_mine, min=ABS_FLOOR)
+        assert bool(((mine_d - exact_mine).abs() <= tol).all()), f"query {q}: distance/index mismatch"
+        assert bool((mine_d[1:] >= mine_d[:-1]).all()), f"query {q}: not ascending"
+        assert torch.unique(mine_i).numel() == k, f"query {q}: repeated index"
+        tol2 = torch.clamp(rel * truth_d, min=ABS_FLOOR)
+        assert bool(((mine_d - truth_d).abs() <= tol2).all()), f"query {q}: rank distances off FP64"
+        a, b = set(mine_i.tolist()), set(top.indices.tolist())
+        hits += len(a & b)
+        if a != b:
+            kth = float(truth_d[-1])
+            band = max(rel * kth, ABS_FLOOR)
+            for j in (a - b) | (b - a):
+                assert abs(float(torch.sqrt(d2[j])) - kth) <= band, (
+                    f"query {q}: index sets differ beyond boundary ties")
+        worst = max(worst, float(((mine_d - exact_mine).abs() /
+                                  torch.clamp(exact_mine, min=ABS_FLOOR)).max()))
+    return hits / (k * len(sample)), worst

@@ -122,3 +122,10 @@ def test_scratch_and_split_plan_are_consistent(knncuda):
         b = knncuda.scratch_bytes(n, q, d, k)
         dup = d * ((q + 31) // 32 * 32) * 8
         assert b == dup + 256 + (s * q * k * 8 if s > 1 else 0)
+    # k > 256 runs in passes of 256 ranks: per-split lists of one pass plus
+    # one lower-bound key per query
+    for n, q, d, k in [(20000, 40, 64, 1000), (200000, 8, 16, 600), (3000, 30, 8, 3000)]:
+        s = knncuda.plan_splits(n, q, d, k)
+        b = knncuda.scratch_bytes(n, q, d, k)
+        dup = d * ((q + 31) // 32 * 32) * 8
+        assert b == dup + 256 + (s * q * 256 * 8 if s > 1 else 0) + q * 8

@@ -73,6 +73,57 @@ def test_random_cases(knncuda, oracle, gpu, method, case):
     check_exact(d, i, ref, query, d64, i64)
 
 
+LARGE_K_CASES = [
+    # (seed, ref_nb, query_nb, dim, k): k > 256 runs in passes of 256 ranks
+    (51, 5000, 60, 32, 257),        # one rank beyond a single pass
+    (52, 20000, 40, 64, 1000),
+    (53, 9000, 20, 16, 4096),       # 16 passes
+    (54, 3000, 30, 8, 3000),        # k == ref_nb
+    (55, 200000, 8, 16, 600),       # few queries: split reference set + merge per pass
+    (56, 700, 33, 3, 513),          # d = 3 (beyond the low-d kernel's k)
+]
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("case", LARGE_K_CASES,
+                         ids=[f"n{c[1]}q{c[2]}d{c[3]}k{c[4]}" for c in LARGE_K_CASES])
+def test_large_k(knncuda, oracle, gpu, method, case):
+    """k > 256: the reference accepts any k <= ref_nb (its insertion sort has
+    no cap, code/knncuda.cu:143-189, code/test.cpp:85-114).  Judged by the
+    reference criterion against knn_c and exactly against FP64."""
+    seed, n, q, dim, k = case
+    rng = np.random.default_rng(seed)
+    ref = rng.random((dim, n), dtype=np.float32)
+    query = rng.random((dim, q), dtype=np.float32)
+    d, i = knncuda.knn(ref, query, k, method)
+    gt_d, gt_i = oracle.knn_c(ref, query, k, threads=THREADS)
+    ok, dacc, iacc = oracle.reference_criterion(d, i, gt_d, gt_i)
+    assert ok, (dacc, iacc)
+    d64, i64 = oracle.knn_f64(ref, query, k, threads=THREADS)
+    check_exact(d, i, ref, query, d64, i64)
+
+
+def test_large_k_device_entry_and_pass_boundaries(knncuda, gpu):
+    """The device entry at k = 700 equals the host entry bit for bit, and the
+    ranks on both sides of each 256-rank pass boundary are in order with no
+    index repeated."""
+    import torch
+
+    rng = np.random.default_rng(57)
+    dim, n, q, k = 48, 30000, 200, 700
+    ref = rng.random((dim, n), dtype=np.float32)
+    query = rng.random((dim, q), dtype=np.float32)
+    hd, hi = knncuda.knn(ref, query, k)
+    d, i = knncuda.knn_device(torch.from_numpy(ref).to(gpu), torch.from_numpy(query).to(gpu), k)
+    assert knncuda.sync_status() == 0
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), hd.view(np.uint32))
+    assert np.array_equal(i.cpu().numpy(), hi)
+    for b in (255, 511):
+        assert np.all(hd[b] <= hd[b + 1])
+    s = np.sort(hi, axis=0)
+    assert np.all(np.diff(s, axis=0) != 0)
+
+
 def test_duplicate_points_tie_order(knncuda, oracle, gpu):
     # every reference point repeated 4 times, far more ties than k
     rng = np.random.default_rng(21)
