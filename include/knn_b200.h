@@ -38,6 +38,9 @@ extern "C" {
 #define KNNB200_METHOD_GLOBAL 0   /* fused exact FP32 direct form (knn_cuda_global) */
 #define KNNB200_METHOD_TEXTURE 1  /* same kernel as GLOBAL (knn_cuda_texture) */
 #define KNNB200_METHOD_CUBLAS 2   /* expansion method (knn_cublas) */
+#define KNNB200_METHOD_FP8 3      /* expansion method with an FP8 (e4m3) candidate scan; same
+                                     exact results; as CUBLAS where the FP8 scan does not apply
+                                     (d > 1024) */
 
 /* C-linkage aliases of the three drop-in entry points of knncuda.h.
  * Replace knn_cuda_global / knn_cuda_texture / knn_cublas,
@@ -182,6 +185,32 @@ KNNB200_API void knnb200_graph_destroy(void *graph_exec);
 KNNB200_API int knnb200_batched_autotune(const knnb200_problem *problems, int count,
                                          void *stream, int *best_item_stages, float *best_ms);
 
+/* Plan configuration: the work-item size in pipeline stages (<= 0: 256),
+ * the queries per consumer warp of the persistent kernel (its query tile is
+ * 16 x that: 4 -> 64-query tiles, 2 -> 32-query tiles for small query
+ * counts; 0: 4, or 2 when some k > 128), and whether problems with dim <= 4
+ * and k <= 16 run the low-dimension kernel in launches of their own
+ * (queued by knnb200_batched_run) instead of the persistent launch. */
+typedef struct knnb200_batched_config {
+    int item_stages;
+    int queries_per_warp;
+    int lowdim_kernel;
+} knnb200_batched_config;
+KNNB200_API int knnb200_batched_plan_create_config(const knnb200_problem *problems, int count,
+                                                   const knnb200_batched_config *config,
+                                                   knnb200_batched_plan **out);
+/* The configuration a plan was built with and the number of problems it
+ * routes to the low-dimension kernel. */
+KNNB200_API int knnb200_batched_plan_config(const knnb200_batched_plan *plan,
+                                            knnb200_batched_config *config,
+                                            int *lowdim_problems);
+/* Autotuner over the whole configuration: the work-item size with the
+ * default tile, then both tile shapes with and without low-d routing at
+ * that size; returns the fastest configuration and its ms per run. */
+KNNB200_API int knnb200_batched_autotune_config(const knnb200_problem *problems, int count,
+                                                void *stream, knnb200_batched_config *best,
+                                                float *best_ms);
+
 /* Synchronise `stream` and return the status of the last device-resident
  * call on the current device (KNNB200_OK or KNNB200_ETIMEOUT / ECUDA). */
 KNNB200_API int knnb200_sync_status(void *stream);
@@ -247,10 +276,17 @@ KNNB200_API void knnb200_last_tc_stats(long long *candidates, int *second_scan, 
  * test asserts a margin.  The check runs a separate instantiation of the
  * re-rank kernel; off by default (enable = 0 turns it off). */
 KNNB200_API int knnb200_set_bound_check(int enable);
-/* Waits for the current device's work stream and returns the ratio and the
+/* Waits for the current device (cudaDeviceSynchronize) and returns the ratio and the
  * number of candidates checked by the last such call (KNNB200_EINVAL if
  * the check was never enabled). */
 KNNB200_API int knnb200_last_bound_check(double *max_ratio, long long *checked);
+
+/* Scan kinds of the last knn_cublas- or FP8-method call on the current
+ * device: *first = the kind of its candidate scan over the whole set,
+ * *second = the kind of the second scan of uncertified queries; 0 BF16,
+ * 1 split BF16 (hi + lo parts), 2 FP8 e4m3, -1 none (exact kernel only, or
+ * no second scan).  Either pointer may be NULL. */
+KNNB200_API void knnb200_last_tc_kinds(int *first, int *second);
 
 /* Per-phase device timing of the calls on the current device (CUDA events on
  * the launching stream between the kernels of a call).  Off by default. */

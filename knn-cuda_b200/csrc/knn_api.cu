@@ -105,6 +105,7 @@ struct Workspace {
     cudaEvent_t last_done = nullptr;   // orders device-resident calls on this device
     Buffer ref, qry, dist, idx, scratch, status;
     Buffer tcref;                      // prepared reference set of the tensor-core path
+    TcRefState tc_state;               // its host-side state
     Buffer bound;                      // re-rank bound check (test-only, off by default)
     bool bound_check = false;
     PhaseTimer timer;                  // optional per-phase device timing
@@ -146,7 +147,8 @@ bool valid_sizes(int ref_nb, int query_nb, int dim, int k) {
 }
 
 bool use_tc(int method, int N, int Q, int d, int k) {
-    return method == KNNB200_METHOD_CUBLAS && tc_supported(N, Q, d, k);
+    return (method == KNNB200_METHOD_CUBLAS || method == KNNB200_METHOD_FP8) &&
+           tc_supported(N, Q, d, k);
 }
 
 size_t scratch_for(int method, int N, int Q, int d, int k, int num_sms) {
@@ -163,14 +165,17 @@ size_t scratch_for(int method, int N, int Q, int d, int k, int num_sms) {
 int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st,
             bool ref_prepared = false) {
     for (int i = 0; i < 8; ++i) ws.tc_stats[i] = 0;
+    ws.tc_stats[6] = ws.tc_stats[7] = -1;
     if (!exact_supported_k(p0.k)) return kErrUnsupported;
     ExactProblem p = p0;
     p.timer = &ws.timer;
     ws.timer.begin(st);
     if (!use_tc(method, p.N, p.Q, p.d, p.k)) return launch_exact(p, st);
     if (!ws.tcref.ensure(tc_ref_bytes(p.N, p.d))) return kErrNoMemory;
-    const TcRefView rv = tc_carve_ref(ws.tcref.ptr, p.N, p.d);
-    int rc = ref_prepared ? kOk : tc_prepare_ref(rv, p.ref, p.N, p.ldr, p.d, st);
+    // a later chunk of the same call keeps the view (and its prepared copies)
+    TcRefView v = tc_carve_ref(ws.tcref.ptr, p.N, p.d, ref_prepared ? nullptr : &ws.tc_state);
+    v.state = &ws.tc_state;
+    int rc = ref_prepared ? kOk : tc_prepare_ref(v, p.ref, p.N, p.ldr, p.d, st);
     if (rc != kOk) return rc;
     ws.timer.mark(st, kPhaseTcPrepRef);
     TcProblem t;
@@ -190,11 +195,12 @@ int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st,
     t.status = p.status;
     t.num_sms = p.num_sms;
     t.timer = &ws.timer;
+    t.request = (method == KNNB200_METHOD_FP8 && tc_fp8_supported(p.d)) ? kTcReqFp8 : kTcReqBf16;
     if (ws.bound_check) {
         if (cudaMemsetAsync(ws.bound.ptr, 0, 16, st) != cudaSuccess) return kErrCuda;
         t.bound_stat = static_cast<unsigned *>(ws.bound.ptr);
     }
-    return launch_tc(t, rv, st, ws.tc_stats);
+    return launch_tc(t, v, st, ws.tc_stats);
 }
 
 // Calls fn(g0, g1) for each maximal range of tiles [g0, g1) of [tb, te)
@@ -226,9 +232,10 @@ int for_each_gap(const TileRuns &s, int tb, int te, F fn) {
 int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_host,
                         cudaStream_t st) {
     for (int i = 0; i < 8; ++i) ws.tc_stats[i] = 0;
+    ws.tc_stats[6] = ws.tc_stats[7] = -1;
     ws.timer.begin(st);
     if (!ws.tcref.ensure(tc_ref_bytes(p.N, p.d))) return kErrNoMemory;
-    const TcRefView rv = tc_carve_ref(ws.tcref.ptr, p.N, p.d);
+    const TcRefView rv = tc_carve_ref(ws.tcref.ptr, p.N, p.d, &ws.tc_state);
     float *ref_d = const_cast<float *>(p.ref);
     const int T = tc_tile_points();
     const int n_tiles = (p.N + T - 1) / T;
@@ -284,10 +291,12 @@ int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_h
     t.status = p.status;
     t.num_sms = p.num_sms;
     t.timer = nullptr;
+    t.host_tmp = ws.tc_stats + 2;
+    t.adaptive = false;   // pass 2 starts before the whole set has arrived
     // the translation comes from every fourth sample tile; the query prep
     // (in tc_run_begin) needs it
     if (cudaStreamWaitEvent(st, ws.copied[0], 0) != cudaSuccess ||
-        cudaMemsetAsync(rv.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess)
+        cudaMemsetAsync(rv.rmax_bits, 0, 3 * 256, st) != cudaSuccess)
         return kErrCuda;
     if ((rc = tc_center_from_tiles(rv, p.ref, p.N, p.ldr, p.d, sample, 4, st)) != kOk) return rc;
     TcRun run;
@@ -579,7 +588,7 @@ int knnb200_knn_device(const float *ref, int ref_nb, long long ref_ld, const flo
                        float *knn_dist, int *knn_index, long long out_ld, void *stream) {
     if (!ref || !query || !knn_dist || !knn_index) return KNNB200_EINVAL;
     if (!valid_sizes(ref_nb, query_nb, dim, k)) return KNNB200_EINVAL;
-    if (method < KNNB200_METHOD_GLOBAL || method > KNNB200_METHOD_CUBLAS) return KNNB200_EINVAL;
+    if (method < KNNB200_METHOD_GLOBAL || method > KNNB200_METHOD_FP8) return KNNB200_EINVAL;
     if (ref_ld < ref_nb || query_ld < query_nb || out_ld < query_nb) return KNNB200_EINVAL;
     if (ref_ld % 4 || query_ld % 4) return KNNB200_EINVAL;
     if ((reinterpret_cast<uintptr_t>(ref) | reinterpret_cast<uintptr_t>(query)) & 15)
@@ -790,7 +799,8 @@ int knnb200_last_bound_check(double *max_ratio, long long *checked) {
     std::lock_guard<std::mutex> lock(ws->mu);
     if (!ws->init || !ws->bound.ptr) return KNNB200_EINVAL;
     unsigned v[4] = {0, 0, 0, 0};
-    if (cudaStreamSynchronize(ws->stream) != cudaSuccess ||
+    // the call may have run on any stream (device entry): wait for all
+    if (cudaDeviceSynchronize() != cudaSuccess ||
         cudaMemcpy(v, ws->bound.ptr, 16, cudaMemcpyDeviceToHost) != cudaSuccess)
         return KNNB200_ECUDA;
     float r;
@@ -798,6 +808,16 @@ int knnb200_last_bound_check(double *max_ratio, long long *checked) {
     if (max_ratio) *max_ratio = r;
     if (checked) *checked = (long long)v[2] | ((long long)v[3] << 32);
     return KNNB200_OK;
+}
+
+void knnb200_last_tc_kinds(int *first, int *second) {
+    if (first) *first = -1;
+    if (second) *second = -1;
+    Workspace *ws = nullptr;
+    if (current_workspace(ws) != kOk || !ws->init) return;
+    std::lock_guard<std::mutex> lock(ws->mu);
+    if (first) *first = ws->tc_stats[6];
+    if (second) *second = ws->tc_stats[7];
 }
 
 const char *knnb200_version(void) { return "knnb200 0.1.0 (sm_100a)"; }

@@ -302,8 +302,9 @@ long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
 struct knnb200_batched_plan {
     int device = 0, num_sms = 148;
-    int kcap = 32, qpw = 4;
-    int count = 0, n_rows = 0, n_split_probs = 0;
+    int kcap = 32, qpw = 4, item_stages = 256;
+    int count = 0, n_rows = 0, n_split_probs = 0;   // count: problems of the persistent launch
+    std::vector<ExactProblem> lowdim;                // problems routed to the low-d kernel
     long long n_items = 0, n_tasks = 0;
     int merge_wpb = 1, slab_keys = 0;
     DevMem tables;      // BatchProb[count] | CUtensorMap[2*count] | counter, status | mlist
@@ -344,13 +345,14 @@ int validate(const knnb200_problem &q) {
 
 extern "C" {
 
-int knnb200_batched_plan_create(const knnb200_problem *in, int count, int item_stages,
-                                knnb200_batched_plan **out) {
+int knnb200_batched_plan_create_config(const knnb200_problem *all, int n_all,
+                                       const knnb200_batched_config *cfg,
+                                       knnb200_batched_plan **out) {
     if (!out) return KNNB200_EINVAL;
     *out = nullptr;
-    if (!in || count < 1) return KNNB200_EINVAL;
-    for (int i = 0; i < count; ++i) {
-        const int rc = validate(in[i]);
+    if (!all || n_all < 1) return KNNB200_EINVAL;
+    for (int i = 0; i < n_all; ++i) {
+        const int rc = validate(all[i]);
         if (rc != KNNB200_OK) return rc;
     }
     int ndev = 0;
@@ -358,14 +360,30 @@ int knnb200_batched_plan_create(const knnb200_problem *in, int count, int item_s
         cudaGetLastError();
         return KNNB200_ENODEV;
     }
-    if (item_stages <= 0) item_stages = 256;
+    const int item_stages = cfg && cfg->item_stages > 0 ? cfg->item_stages : 256;
+    const int want_qpw = cfg ? cfg->queries_per_warp : 0;
+    if (want_qpw != 0 && want_qpw != 2 && want_qpw != 4) return KNNB200_EINVAL;
+    const bool route_lowdim = cfg && cfg->lowdim_kernel;
     knnb200_batched_plan *pl = new knnb200_batched_plan();
     cudaGetDevice(&pl->device);
     cudaDeviceGetAttribute(&pl->num_sms, cudaDevAttrMultiProcessorCount, pl->device);
+    pl->item_stages = item_stages;
+    // problem classes: d <= 4, k <= 16 to the low-d kernel (when asked),
+    // the rest to the persistent launch
+    std::vector<knnb200_problem> persist;
+    std::vector<int> low_idx;
+    for (int i = 0; i < n_all; ++i) {
+        if (route_lowdim && lowdim_applies(all[i].ref_nb, all[i].query_nb, all[i].dim, all[i].k))
+            low_idx.push_back(i);
+        else
+            persist.push_back(all[i]);
+    }
+    const knnb200_problem *in = persist.data();
+    const int count = (int)persist.size();
     int kmax = 1;
     for (int i = 0; i < count; ++i) kmax = std::max(kmax, in[i].k);
     pl->kcap = kmax <= 32 ? 32 : kmax <= 64 ? 64 : kmax <= 128 ? 128 : 256;
-    pl->qpw = pl->kcap == 256 ? EX_QPW_K256 : EX_QPW;
+    pl->qpw = pl->kcap == 256 ? EX_QPW_K256 : (want_qpw ? want_qpw : EX_QPW);
     const int bq = pl->qpw * EX_WARPS;
 
     // records, cut into items of about `item_stages` pipeline stages
@@ -399,15 +417,23 @@ int knnb200_batched_plan_create(const knnb200_problem *in, int count, int item_s
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
 
-    // scratch: duplicated queries + per-split lists
+    // scratch: duplicated queries + per-split lists; then the low-d
+    // problems' split lists
     size_t sbytes = 0;
-    std::vector<size_t> dup_off(count), part_off(count);
+    std::vector<size_t> dup_off(count), part_off(count), low_off(low_idx.size());
     for (int i = 0; i < count; ++i) {
         BatchProb &P = recs[i];
         dup_off[i] = sbytes;
         sbytes += round_up((long long)P.d * P.ld2 * sizeof(float2), 256);
         part_off[i] = sbytes;
         if (P.n_splits > 1) sbytes += round_up((long long)P.n_splits * P.Q * P.k * 8, 256);
+    }
+    for (size_t j = 0; j < low_idx.size(); ++j) {
+        const knnb200_problem &q = all[low_idx[j]];
+        low_off[j] = sbytes;
+        sbytes += round_up((long long)lowdim_scratch_bytes(q.ref_nb, q.query_nb, q.dim, q.k,
+                                                           pl->num_sms),
+                           256);
     }
     const size_t tbytes = round_up((long long)count * sizeof(BatchProb), 64) +
                           (size_t)2 * count * sizeof(CUtensorMap) + 64 + (size_t)count * 4 + 256;
@@ -453,6 +479,28 @@ int knnb200_batched_plan_create(const knnb200_problem *in, int count, int item_s
         }
         table[r] = P;
     }
+    for (size_t j = 0; j < low_idx.size(); ++j) {
+        const knnb200_problem &q = all[low_idx[j]];
+        ExactProblem e;
+        e.ref = q.ref;
+        e.N = q.ref_nb;
+        e.ldr = q.ref_ld;
+        e.qry = q.query;
+        e.Q = q.query_nb;
+        e.ldq = q.query_ld;
+        e.d = q.dim;
+        e.k = q.k;
+        e.out_dist = q.knn_dist;
+        e.out_idx = q.knn_index;
+        e.ld_out = q.out_ld;
+        e.scratch = sb + low_off[j];
+        e.scratch_bytes = (j + 1 < low_idx.size() ? low_off[j + 1] : sbytes) - low_off[j];
+        e.status = pl->status;
+        e.num_sms = pl->num_sms;
+        e.force_splits = 0;
+        e.timer = nullptr;
+        pl->lowdim.push_back(e);
+    }
     pl->count = count;
     pl->n_split_probs = (int)mlist.size();
     pl->n_items = item;
@@ -462,10 +510,11 @@ int knnb200_batched_plan_create(const knnb200_problem *in, int count, int item_s
     pl->merge_wpb = max_slab ? (int)std::max<size_t>(
                                    1, std::min<size_t>(8, kBatchMergeSmemMax / (8ull * max_slab)))
                              : 1;
-    if (cudaMemcpy(pl->probs, table.data(), count * sizeof(BatchProb), cudaMemcpyHostToDevice) !=
-            cudaSuccess ||
-        cudaMemcpy(pl->maps, maps.data(), 2 * count * sizeof(CUtensorMap),
-                   cudaMemcpyHostToDevice) != cudaSuccess ||
+    if ((count > 0 &&
+         (cudaMemcpy(pl->probs, table.data(), count * sizeof(BatchProb),
+                     cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMemcpy(pl->maps, maps.data(), 2 * count * sizeof(CUtensorMap),
+                     cudaMemcpyHostToDevice) != cudaSuccess)) ||
         (!mlist.empty() && cudaMemcpy(pl->mlist, mlist.data(), mlist.size() * sizeof(int),
                                       cudaMemcpyHostToDevice) != cudaSuccess)) {
         delete pl;
@@ -475,19 +524,51 @@ int knnb200_batched_plan_create(const knnb200_problem *in, int count, int item_s
     return KNNB200_OK;
 }
 
+int knnb200_batched_plan_create(const knnb200_problem *in, int count, int item_stages,
+                                knnb200_batched_plan **out) {
+    const knnb200_batched_config c{item_stages, 0, 0};
+    return knnb200_batched_plan_create_config(in, count, &c, out);
+}
+
+int knnb200_batched_plan_config(const knnb200_batched_plan *pl, knnb200_batched_config *cfg,
+                                int *lowdim_problems) {
+    if (!pl) return KNNB200_EINVAL;
+    if (cfg) {
+        cfg->item_stages = pl->item_stages;
+        cfg->queries_per_warp = pl->qpw;
+        cfg->lowdim_kernel = pl->lowdim.empty() ? 0 : 1;
+    }
+    if (lowdim_problems) *lowdim_problems = (int)pl->lowdim.size();
+    return KNNB200_OK;
+}
+
 int knnb200_batched_run(knnb200_batched_plan *pl, void *stream) {
     if (!pl) return KNNB200_EINVAL;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // queue counter and status word (the first 64 bytes after the maps)
     if (cudaMemsetAsync(pl->counter, 0, 64, st) != cudaSuccess) return KNNB200_ECUDA;
+    // low-d problems: one launch each (plus a split merge), no waits, so the
+    // plan stays capturable
+    for (const ExactProblem &e : pl->lowdim)
+        if (launch_lowdim(e, st) != kOk) return KNNB200_ELAUNCH;
+    if (pl->count == 0) return KNNB200_OK;
     batched_dup_kernel<<<pl->n_rows, 256, 0, st>>>(pl->probs, pl->count, pl->n_rows);
     if (cudaGetLastError() != cudaSuccess) return KNNB200_ELAUNCH;
     cudaError_t e;
-    switch (pl->kcap) {
-        case 32: e = launch_batched_t<EX_QPW, 32>(pl, st); break;
-        case 64: e = launch_batched_t<EX_QPW, 64>(pl, st); break;
-        case 128: e = launch_batched_t<EX_QPW, 128>(pl, st); break;
-        default: e = launch_batched_t<EX_QPW_K256, 256>(pl, st); break;
+    if (pl->kcap == 256) {
+        e = launch_batched_t<EX_QPW_K256, 256>(pl, st);
+    } else if (pl->qpw == 2) {
+        switch (pl->kcap) {
+            case 32: e = launch_batched_t<2, 32>(pl, st); break;
+            case 64: e = launch_batched_t<2, 64>(pl, st); break;
+            default: e = launch_batched_t<2, 128>(pl, st); break;
+        }
+    } else {
+        switch (pl->kcap) {
+            case 32: e = launch_batched_t<EX_QPW, 32>(pl, st); break;
+            case 64: e = launch_batched_t<EX_QPW, 64>(pl, st); break;
+            default: e = launch_batched_t<EX_QPW, 128>(pl, st); break;
+        }
     }
     if (e != cudaSuccess) return KNNB200_ELAUNCH;
     if (pl->n_tasks > 0) {
@@ -558,6 +639,70 @@ void knnb200_graph_destroy(void *graph_exec) {
     if (graph_exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph_exec));
 }
 
+// Times one plan configuration: a warm-up run, then three.
+static int time_config(const knnb200_problem *in, int count, const knnb200_batched_config &c,
+                       cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1, float *ms_out) {
+    knnb200_batched_plan *pl = nullptr;
+    int rc = knnb200_batched_plan_create_config(in, count, &c, &pl);
+    if (rc != KNNB200_OK) return rc;
+    float ms = 0.f;
+    rc = knnb200_batched_run(pl, st);   // warm-up
+    if (rc == KNNB200_OK) {
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 3 && rc == KNNB200_OK; ++r) rc = knnb200_batched_run(pl, st);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = KNNB200_ECUDA;
+        cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (rc == KNNB200_OK) rc = knnb200_batched_status(pl, st);
+    knnb200_batched_plan_destroy(pl);
+    *ms_out = ms / 3;
+    return rc;
+}
+
+int knnb200_batched_autotune_config(const knnb200_problem *in, int count, void *stream,
+                                    knnb200_batched_config *best_cfg, float *best_ms) {
+    if (!in || count < 1 || !best_cfg) return KNNB200_EINVAL;
+    static const int stage_cands[] = {32, 64, 128, 256, 512, 1024, 2048};
+    static const int qpw_cands[] = {4, 2};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    knnb200_batched_config bc{256, 4, 0};
+    int rc = KNNB200_OK;
+    // work-item size first (with the default tile shape), then the tile
+    // shape and the low-d routing at the best size
+    for (int c : stage_cands) {
+        const knnb200_batched_config cfg{c, 4, 0};
+        float ms = 0.f;
+        if ((rc = time_config(in, count, cfg, st, e0, e1, &ms)) != KNNB200_OK) break;
+        if (ms < best) {
+            best = ms;
+            bc = cfg;
+        }
+    }
+    for (int qpw : qpw_cands) {
+        for (int low = 0; low < 2 && rc == KNNB200_OK; ++low) {
+            const knnb200_batched_config cfg{bc.item_stages, qpw, low};
+            if (qpw == bc.queries_per_warp && low == bc.lowdim_kernel) continue;
+            float ms = 0.f;
+            if ((rc = time_config(in, count, cfg, st, e0, e1, &ms)) != KNNB200_OK) break;
+            if (ms < best) {
+                best = ms;
+                bc = cfg;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != KNNB200_OK) return rc;
+    *best_cfg = bc;
+    if (best_ms) *best_ms = best;
+    return KNNB200_OK;
+}
+
 int knnb200_batched_autotune(const knnb200_problem *in, int count, void *stream,
                              int *best_item_stages, float *best_ms) {
     if (!in || count < 1 || !best_item_stages) return KNNB200_EINVAL;
@@ -569,23 +714,12 @@ int knnb200_batched_autotune(const knnb200_problem *in, int count, void *stream,
     float best = 1e30f;
     int bestc = 256, rc = KNNB200_OK;
     for (int c : cands) {
-        knnb200_batched_plan *pl = nullptr;
-        rc = knnb200_batched_plan_create(in, count, c, &pl);
-        if (rc != KNNB200_OK) break;
         float ms = 0.f;
-        rc = knnb200_batched_run(pl, stream);   // warm-up
-        if (rc == KNNB200_OK) {
-            cudaEventRecord(e0, st);
-            for (int r = 0; r < 3 && rc == KNNB200_OK; ++r) rc = knnb200_batched_run(pl, stream);
-            cudaEventRecord(e1, st);
-            if (cudaEventSynchronize(e1) != cudaSuccess) rc = KNNB200_ECUDA;
-            cudaEventElapsedTime(&ms, e0, e1);
-        }
-        if (rc == KNNB200_OK) rc = knnb200_batched_status(pl, stream);
-        knnb200_batched_plan_destroy(pl);
-        if (rc != KNNB200_OK) break;
-        if (ms / 3 < best) {
-            best = ms / 3;
+        if ((rc = time_config(in, count, knnb200_batched_config{c, 0, 0}, st, e0, e1, &ms)) !=
+            KNNB200_OK)
+            break;
+        if (ms < best) {
+            best = ms;
             bestc = c;
         }
     }

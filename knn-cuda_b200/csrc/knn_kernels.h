@@ -122,13 +122,35 @@ size_t exact_scratch_bytes(int N, int Q, int d, int k, int num_sms);
 int exact_plan_splits(int N, int Q, int d, int k, int num_sms);
 int launch_exact(const ExactProblem &p, cudaStream_t st);
 
+// Host-side state of a prepared reference set: which of the optional
+// copies exist, and the FP8 scales (known once the set's largest |r - c|
+// and ||r - c||^2 have been read back).
+struct TcRefState {
+    bool lo_ready = false;   // refBlo holds the split-BF16 lo parts
+    bool f8_ready = false;   // ref8 / refN8 hold the FP8 copy
+    float s_r = 0.f, kappa = 0.f, resid8 = 0.f;   // FP8 scale, norm-step unit, norm residual
+    float absmax_r = 0.f, r2max = 0.f;            // read back with the FP8 prep
+};
+
 // Prepared reference set of the tensor-core path (see knn_tc.cu).
 struct TcRefView {
-    __nv_bfloat16 *refB;    // [N][d_pad] BF16, K-major
+    __nv_bfloat16 *refB;    // [N][d_pad] BF16 of r - c, K-major
     float *refT;            // [N][d_pad] FP32 point-major (re-rank gathers)
     __nv_bfloat16 *refN;    // [N][16] squared norm as three BF16 parts, then zeros
     unsigned *rmax_bits;    // largest squared norm of ref - center (float bits)
-    float *center;          // [d_pad] translation of both sets before the BF16 expansion
+    unsigned *absmax_bits;  // largest |r - c| of any coordinate (float bits)
+    unsigned *resid8_bits;  // FP8 norm-split residual (float bits)
+    float *center;          // [d_pad] translation of both sets before the expansion
+    __nv_bfloat16 *refBlo;  // [N][d_pad] split-BF16 lo parts (prepared when first needed)
+    unsigned char *ref8;    // [N][d_pad8] FP8 e4m3 of s_r (r - c) (prepared when first needed)
+    unsigned char *refN8;   // [N][32] FP8 norm-step parts
+    TcRefState *state;      // host-side flags and scales
+};
+
+// First-scan kind requested of the tensor path.
+enum TcRequest : int {
+    kTcReqBf16 = 0,   // BF16 scan; split BF16 when BF16 is predicted to overflow
+    kTcReqFp8 = 1,    // FP8 e4m3 scan
 };
 
 struct TcProblem {
@@ -151,6 +173,11 @@ struct TcProblem {
     // re-ranked candidates of |a + ||q||^2 - D| / E_q (float bits), [2..3]
     // candidates checked (64-bit)
     unsigned *bound_stat = nullptr;
+    int request = kTcReqBf16;
+    int *host_tmp = nullptr;   // pinned, >= 2 ints: read-backs inside the run
+    // the first scan's kind may switch to split BF16 after the threshold
+    // pass (not with a reference set still streaming in)
+    bool adaptive = true;
 };
 
 // A sample of the 256-point tiles: `run` consecutive tiles out of every
@@ -167,9 +194,11 @@ struct TileRuns {
 };
 
 bool tc_supported(int N, int Q, int d, int k);
+bool tc_fp8_supported(int d);
 size_t tc_ref_bytes(int N, int d);
 size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms);
-TcRefView tc_carve_ref(void *mem, int N, int d);
+// Carves the view out of `mem` (tc_ref_bytes); a non-null `state` is reset.
+TcRefView tc_carve_ref(void *mem, int N, int d, TcRefState *state);
 int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, int d,
                    cudaStream_t st);
 // Staged form of launch_tc, for callers that stream the reference set in:
@@ -182,11 +211,14 @@ struct TcRun {
     TcProblem P;
     TcRefView R;
     TileRuns sample;
-    int d_pad, kb, qtiles, n_tiles2, splits1, cmax;
+    int d_pad, d_pad8, qtiles, n_tiles2, splits1, cmax;
+    int kind;               // kind of the first scan's pass 2 (TcKind in knn_tc.cu)
+    float s_q, scale;       // FP8: query scale, accumulator units per a unit (s_q s_r)
     long long ldf;
-    __nv_bfloat16 *qB;
-    float *qn, *thr, *retry, *p1, *qsub, *sd;
-    int *count, *fail, *fail2, *nfail, *si;
+    __nv_bfloat16 *qB, *qBlo;
+    unsigned char *q8;
+    float *qn, *thr, *thr_raw, *retry, *retry_f, *p1, *qsub, *sd;
+    int *count, *fail, *fail2, *nfail, *si, *nwide;
     unsigned long long *cand_total, *cand;
     unsigned char *xs;
     size_t xcap;
@@ -220,12 +252,19 @@ int tc_run_pass2(TcRun &run, int tile_begin, int tile_end, cudaStream_t st);
 int tc_run_rerank_piece(TcRun &run, cudaStream_t st);
 int tc_run_finish(TcRun &run, cudaStream_t st, int *host_stats);
 
+// Prepares the optional copies of a prepared set (split-BF16 lo parts, the
+// FP8 copy) now rather than on first use; synchronises `st`.  host_tmp:
+// pinned, >= 2 ints.  For sets shared by several streams.
+int tc_prepare_extras(const TcRefView &v, int N, int d, cudaStream_t st, int *host_tmp);
+
 // Queues the tensor-core k-NN.  Synchronises once to learn how many queries
 // failed certification; those get a second scan with thresholds that
 // certify, and queries whose candidate list overflowed are recomputed by the
 // exact kernel.  host_stats (pinned, 8 ints, 8-byte aligned): [0] queries
-// given the second scan, [1] queries recomputed by the exact kernel, [2]
-// scratch, [4..5] total first-scan candidates (64-bit).
+// given the second scan, [1] queries recomputed by the exact kernel, [2..3]
+// scratch, [4..5] total first-scan candidates (64-bit), [6] kind of the
+// first scan's pass 2, [7] kind of the second scan (-1: none); kinds are
+// 0 BF16, 1 split BF16, 2 FP8.
 int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_stats);
 
 }  // namespace knnb200

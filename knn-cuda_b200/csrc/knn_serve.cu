@@ -103,6 +103,7 @@ struct knnb200_refset {
     DevBuf ref;          // [d][ldr] FP32
     DevBuf tcmem;        // prepared tensor-core view
     TcRefView tc{};
+    TcRefState tc_state;
     bool has_tc = false;
     std::mutex mu;       // guards `slot` for knnb200_refset_knn
     Slot slot;
@@ -111,7 +112,8 @@ struct knnb200_refset {
 namespace {
 
 bool use_tc_for(const knnb200_refset *rs, int method, int Q, int k) {
-    return method == KNNB200_METHOD_CUBLAS && rs->has_tc && tc_supported(rs->N, Q, rs->d, k);
+    return (method == KNNB200_METHOD_CUBLAS || method == KNNB200_METHOD_FP8) && rs->has_tc &&
+           tc_supported(rs->N, Q, rs->d, k);
 }
 
 size_t scratch_need(const knnb200_refset *rs, int method, int Q, int k) {
@@ -144,6 +146,8 @@ int run_refset(knnb200_refset *rs, Slot &slot, const float *query, int Q, long l
         t.status = static_cast<int *>(slot.status.ptr);
         t.num_sms = rs->num_sms;
         t.timer = nullptr;
+        t.request = (method == KNNB200_METHOD_FP8 && tc_fp8_supported(rs->d)) ? kTcReqFp8
+                                                                             : kTcReqBf16;
         return launch_tc(t, rs->tc, st, slot.host_stats);
     }
     ExactProblem p;
@@ -215,9 +219,11 @@ int knnb200_refset_create(const float *ref, int ref_nb, long long ref_ld, int di
         if (!rs->tcmem.ensure(tc_ref_bytes(ref_nb, dim))) {
             rc = KNNB200_ENOMEM;
         } else {
-            rs->tc = tc_carve_ref(rs->tcmem.ptr, ref_nb, dim);
+            rs->tc = tc_carve_ref(rs->tcmem.ptr, ref_nb, dim, &rs->tc_state);
+            // every copy prepared now: the server's slots share the set
             if (tc_prepare_ref(rs->tc, static_cast<const float *>(rs->ref.ptr), ref_nb, rs->ldr,
-                               dim, st) != kOk)
+                               dim, st) != kOk ||
+                tc_prepare_extras(rs->tc, ref_nb, dim, st, rs->slot.host_stats + 2) != kOk)
                 rc = KNNB200_ELAUNCH;
             else
                 rs->has_tc = true;
@@ -256,7 +262,7 @@ int knnb200_refset_knn(knnb200_refset *rs, const float *query, int query_nb, lon
     if (query_nb < 1 || k < 1 || k > rs->N || query_ld < query_nb || out_ld < query_nb)
         return KNNB200_EINVAL;
     if (query_ld % 4 || (reinterpret_cast<uintptr_t>(query) & 15)) return KNNB200_EINVAL;
-    if (method < KNNB200_METHOD_GLOBAL || method > KNNB200_METHOD_CUBLAS) return KNNB200_EINVAL;
+    if (method < KNNB200_METHOD_GLOBAL || method > KNNB200_METHOD_FP8) return KNNB200_EINVAL;
     std::lock_guard<std::mutex> lock(rs->mu);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // scratch of the refset's own slot: order this call after its previous one
@@ -428,7 +434,7 @@ int knnb200_server_create(knnb200_refset *rs, int slots, size_t memory_budget_by
     if (!out) return KNNB200_EINVAL;
     *out = nullptr;
     if (!rs || slots < 1 || slots > 16 || max_batch_queries < 1) return KNNB200_EINVAL;
-    if (method < KNNB200_METHOD_GLOBAL || method > KNNB200_METHOD_CUBLAS) return KNNB200_EINVAL;
+    if (method < KNNB200_METHOD_GLOBAL || method > KNNB200_METHOD_FP8) return KNNB200_EINVAL;
     knnb200_server *s = new knnb200_server();
     s->rs = rs;
     s->method = method;

@@ -46,9 +46,12 @@
 // 2^-16 + g, E_q = 2 eps ||q|| max||r|| + g (max||r||^2 + ||q||^2) + 2^-20
 // (|T_q| + ||q||^2) covers all of them and the roundings of ||q||^2 and T_q.
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
+#include <cstring>
 
 #include "knn_exact_core.cuh"
 #include "knn_kernels.h"
@@ -59,10 +62,7 @@ namespace knnb200 {
 constexpr int TC_BM = 128;            // rows (queries) per CTA of a pair, points per CTA half-tile
 constexpr int TC_QT = 2 * TC_BM;      // queries per CTA pair
 constexpr int TC_BK = 64;             // K block: 64 bf16 = 128 B (one swizzle row)
-constexpr int TC_KBMAX = 4;           // d_pad <= 256
-constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;   // 16 KB (A or B K-block tile of one CTA)
 constexpr int TC_NK = 16;             // norm step: K = 16 (h, m, l, 13 zeros)
-constexpr int TC_NORM_BYTES = TC_BM * TC_NK * 2;   // 4 KB norm tile (32-byte swizzle)
 constexpr int TC_KS = 16;             // pass-1 per-row list length
 constexpr uint32_t TC_TMEM_COLS = 512;   // 2 accumulator buffers x 256 columns
 constexpr int kCenterStride = 64;     // the translation is the mean of every 64th tile
@@ -155,48 +155,94 @@ constexpr int TP_COLS = TP_BN / (TP_EPI_WARPS / 4);   // columns per epilogue wa
 constexpr int TP_CHUNKS = TP_COLS / 32;
 constexpr int TP_THREADS = 32 * (2 + TP_EPI_WARPS);   // warp 0 TMA, warp 1 MMA, epilogue
 constexpr int TP_LISTS = TP_EPI_WARPS / 4;             // pass-1 lists per query and split
-constexpr int TP_STAGES = 8;
 constexpr int TP_NSLOTS = 4;
-constexpr uint32_t TP_IDESC = umma_idesc_bf16(2 * TC_BM, TP_BN);
 
-constexpr size_t TP_OFF_A = 0;
-constexpr size_t TP_OFF_ONES = (size_t)TC_KBMAX * TC_TILE_BYTES;                // 64 KB
-constexpr size_t TP_OFF_B = TP_OFF_ONES + (size_t)TC_BM * TC_NK * 2;            // +4 KB
-constexpr size_t TP_OFF_N = TP_OFF_B + (size_t)TP_STAGES * TC_TILE_BYTES;        // +128 KB
-constexpr size_t TP_OFF_BAR = TP_OFF_N + (size_t)TP_NSLOTS * TC_NORM_BYTES;      // +16 KB
-constexpr int TP_NBARS = 1 + 2 * TP_STAGES + 2 * TP_NSLOTS + 2 + 2 + 1;
+// Operand kinds of the scan.  Every kind keeps the same epilogue: the
+// accumulator holds a (scaled for FP8) and the threshold test is the same.
+enum TcKind : int {
+    kTcBf16 = 0,     // BF16 operands (kind::f16): one MMA per 16-element K step
+    kTcBf16x3 = 1,   // split BF16: hi + lo parts of both sets, hi.hi + lo.hi + hi.lo
+    kTcFp8 = 2,      // FP8 e4m3 operands (kind::f8f6f4), power-of-two scales
+};
+
+// Shared memory: a region of TP_REGION_TILES operand tiles (128 rows x
+// 128 bytes, 16 KB each) holds the resident query tiles (A) followed by the
+// reference ring (B), or -- when A does not fit, d_pad > 512 in BF16 -- a
+// ring whose stages carry an A tile and a B tile each; then the ones tile,
+// the norm-step ring and the barriers.
+constexpr int TP_TILE_BYTES = TC_BM * 128;            // 16 KB
+constexpr int TP_REGION_TILES = 12;
+constexpr int TP_MAX_RESIDENT_A = 8;                   // leaves >= 4 ring stages
+constexpr int TP_MAX_STAGES = TP_REGION_TILES - 1;
+constexpr int TP_NORM_BYTES = TC_BM * 32;              // 4 KB: 32-byte norm-step rows
+constexpr size_t TP_OFF_REGION = 0;
+constexpr size_t TP_OFF_ONES = (size_t)TP_REGION_TILES * TP_TILE_BYTES;   // 192 KB
+constexpr size_t TP_OFF_N = TP_OFF_ONES + TP_NORM_BYTES;                   // +4 KB
+constexpr size_t TP_OFF_BAR = TP_OFF_N + (size_t)TP_NSLOTS * TP_NORM_BYTES;  // +16 KB
+constexpr int TP_NBARS = 1 + 2 * TP_MAX_STAGES + 2 * TP_NSLOTS + 2 + 2 + 1;
 constexpr size_t TP_SMEM = 1024 + TP_OFF_BAR + TP_NBARS * 8 + 16;
 static_assert(TP_SMEM <= 232448, "pair scan kernel shared memory");
+static_assert(TP_OFF_N % 1024 == 0 && TP_OFF_ONES % 1024 == 0, "tile alignment");
 
 struct TpArgs {
-    int N, Q, kb_count;
+    int N, Q;
+    int kb;                 // K blocks per operand row (128 bytes each)
+    int ka;                 // resident A tiles (0: A streamed with B)
+    int stages;             // ring stages
+    int items;              // ring items per reference tile
     int tile_base, n_splits;
     TileRuns tiles;         // scan tiles tile_base + tiles.tile(u), u < tiles.units
     const float *thr;       // emit pass: [Q] thresholds (a units)
-    float *p1;              // sample pass: [TP_LISTS n_splits][Q][TC_KS] (per column range)
-    unsigned long long *cand;   // [Q][cmax] (a, index) entries
+    float thr_scale;        // accumulator units per a unit (FP8: s_q s_r; else 1)
+    uint32_t ones_word;     // four bytes of the ones tile (1.0 BF16 x2, or the FP8 c1 x4)
+    float *p1;              // sample pass: [TP_LISTS n_splits][Q][TC_KS] (accumulator units)
+    unsigned long long *cand;   // [Q][cmax] (accumulator bits, index) entries
     int *count;             // [Q]
     int cmax;
     int *status;
 };
 
-template <int MODE>   // 0: threshold sample pass, 1: emit pass
+// Norm step and one ring item's MMAs for each kind, issued by the even
+// CTA's MMA thread.  K steps advance the descriptors by 32 bytes (2 in
+// 16-byte units) for every kind: 16 BF16 or 32 FP8 elements.
+template <int KIND>
+KNN_DI void tp_mma_norm(uint32_t acc, uint64_t odesc, uint64_t ndesc) {
+    if (KIND == kTcFp8)
+        umma_f8_pair(acc, odesc, ndesc, umma_idesc_e4m3(2 * TC_BM, TP_BN), 0u);
+    else
+        umma_bf16_pair(acc, odesc, ndesc, umma_idesc_bf16(2 * TC_BM, TP_BN), 0u);
+}
+template <int KIND>
+KNN_DI void tp_mma_block(uint32_t acc, uint64_t adesc, uint64_t bdesc) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (KIND == kTcFp8)
+            umma_f8_pair(acc, adesc + (uint64_t)(2 * k), bdesc + (uint64_t)(2 * k),
+                         umma_idesc_e4m3(2 * TC_BM, TP_BN), 1u);
+        else
+            umma_bf16_pair(acc, adesc + (uint64_t)(2 * k), bdesc + (uint64_t)(2 * k),
+                           umma_idesc_bf16(2 * TC_BM, TP_BN), 1u);
+    }
+}
+
+template <int MODE, int KIND>   // MODE 0: threshold sample pass, 1: emit pass
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
     knn_tc_pair_scan_kernel(const __grid_constant__ CUtensorMap tmA,
+                            const __grid_constant__ CUtensorMap tmA2,
                             const __grid_constant__ CUtensorMap tmB,
+                            const __grid_constant__ CUtensorMap tmB2,
                             const __grid_constant__ CUtensorMap tmN, TpArgs a) {
     extern __shared__ unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char *sA = base + TP_OFF_A;
+    unsigned char *sR = base + TP_OFF_REGION;
     unsigned char *sOnes = base + TP_OFF_ONES;
-    unsigned char *sB = base + TP_OFF_B;
     unsigned char *sN = base + TP_OFF_N;
     uint64_t *bars = reinterpret_cast<uint64_t *>(base + TP_OFF_BAR);
     uint64_t *a_full = bars;
     uint64_t *b_full = bars + 1;
-    uint64_t *b_empty = b_full + TP_STAGES;
-    uint64_t *n_full = b_empty + TP_STAGES;
+    uint64_t *b_empty = b_full + TP_MAX_STAGES;
+    uint64_t *n_full = b_empty + TP_MAX_STAGES;
     uint64_t *n_empty = n_full + TP_NSLOTS;
     uint64_t *acc_full = n_empty + TP_NSLOTS;
     uint64_t *acc_empty = acc_full + 2;
@@ -208,17 +254,22 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
     const uint32_t rank = cluster_ctarank();
     const bool lead = rank == 0;
     const int qpair = blockIdx.x >> 1, split = blockIdx.y;
-    const int KB = a.kb_count;
+    const int KB = a.kb, KA = a.ka, NST = a.stages, ITEMS = a.items;
+    const bool streamed = KA == 0;
+    const int stage_tiles = streamed ? 2 : 1;
+    const uint32_t stage_bytes = (uint32_t)(stage_tiles * TP_TILE_BYTES);
+    // K-block width in elements of the operand type (128 bytes)
+    const int kx = KIND == kTcFp8 ? 128 : 64;
     // this split's units [u0, u0 + n_my)
     const int u0 = (int)((long long)a.tiles.units * split / a.n_splits);
     const int n_my = (int)((long long)a.tiles.units * (split + 1) / a.n_splits) - u0;
 
-    for (int i = threadIdx.x; i < TC_BM * TC_NK / 2; i += TP_THREADS)
-        reinterpret_cast<uint32_t *>(sOnes)[i] = 0x3F803F80u;
+    for (int i = threadIdx.x; i < TP_NORM_BYTES / 4; i += TP_THREADS)
+        reinterpret_cast<uint32_t *>(sOnes)[i] = a.ones_word;
     fence_proxy_async_smem();
     if (warp == 0 && lane == 0) {
         mbar_init(a_full, 1);
-        for (int s = 0; s < TP_STAGES; ++s) {
+        for (int s = 0; s < NST; ++s) {
             mbar_init(&b_full[s], 1);
             mbar_init(&b_empty[s], 1);
         }
@@ -236,6 +287,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
         prefetch_tensormap(&tmA);
         prefetch_tensormap(&tmB);
         prefetch_tensormap(&tmN);
+        if (KIND == kTcBf16x3) {
+            prefetch_tensormap(&tmA2);
+            prefetch_tensormap(&tmB2);
+        }
     }
     if (warp == 1) {
         tmem_alloc_pair(tmem_holder, TC_TMEM_COLS);
@@ -246,6 +301,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
     cluster_sync();   // both CTAs' barriers are initialised before any use
     tc_fence_after();
     const uint32_t tmem = *tmem_holder;
+    // ring stage s: tiles [KA + s * stage_tiles, + stage_tiles) of the region
+    auto stage_ptr = [&](int s) { return sR + (size_t)(KA + s * stage_tiles) * TP_TILE_BYTES; };
 
     if (warp == 0) {
         // ---------------- TMA producer (both CTAs) ----------------
@@ -253,12 +310,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
             int issued = 0, n_issued = 0;
             bool a_issued = false, ok = true;
             const int half_row = (int)rank * TC_BM;
-            if (n_my > 0) {
-                if (lead) mbar_arrive_expect_tx(a_full, (uint32_t)(2 * KB * TC_TILE_BYTES));
+            const int qrow0 = qpair * TC_QT + half_row;
+            if (n_my > 0 && KA > 0) {
+                if (lead) mbar_arrive_expect_tx(a_full, (uint32_t)(2 * KA * TP_TILE_BYTES));
                 const uint32_t bar = mapa_shared(smem_u32(a_full), 0);
-                for (int kb = 0; kb < KB; ++kb)
-                    tma_load_2d_pair(sA + (size_t)kb * TC_TILE_BYTES, &tmA, bar, kb * TC_BK,
-                                     qpair * TC_QT + half_row);
+                for (int t = 0; t < KA; ++t) {
+                    // split BF16: hi tiles 0 .. KB-1, lo tiles KB .. 2 KB-1
+                    const CUtensorMap *m = (KIND == kTcBf16x3 && t >= KB) ? &tmA2 : &tmA;
+                    tma_load_2d_pair(sR + (size_t)t * TP_TILE_BYTES, m, bar, (t % KB) * kx, qrow0);
+                }
                 a_issued = true;
             }
             for (int j = 0; j < n_my && ok; ++j) {
@@ -269,24 +329,32 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                     break;
                 }
                 if (*abort_flag) break;
-                if (lead) mbar_arrive_expect_tx(&n_full[ns], 2 * TC_NORM_BYTES);
-                tma_load_2d_pair(sN + (size_t)ns * TC_NORM_BYTES, &tmN,
+                if (lead) mbar_arrive_expect_tx(&n_full[ns], 2 * TP_NORM_BYTES);
+                tma_load_2d_pair(sN + (size_t)ns * TP_NORM_BYTES, &tmN,
                                  mapa_shared(smem_u32(&n_full[ns]), 0), 0, row0);
                 n_issued = j + 1;
-                const int row_ahead = j + 2 < n_my
-                                          ? (a.tile_base + a.tiles.tile(u0 + j + 2)) * TP_BN + half_row
-                                          : a.N;
-                for (int kb = 0; kb < KB; ++kb) {
-                    const int it = j * KB + kb, s = it % TP_STAGES;
-                    if (it >= TP_STAGES && !mbar_wait(&b_empty[s], ((it / TP_STAGES) - 1) & 1)) {
+                const int row_ahead =
+                    j + 2 < n_my ? (a.tile_base + a.tiles.tile(u0 + j + 2)) * TP_BN + half_row
+                                 : a.N;
+                for (int i = 0; i < ITEMS; ++i) {
+                    const int it = j * ITEMS + i, s = it % NST;
+                    if (it >= NST && !mbar_wait(&b_empty[s], ((it / NST) - 1) & 1)) {
                         ok = false;
                         break;
                     }
                     if (*abort_flag) break;
-                    if (lead) mbar_arrive_expect_tx(&b_full[s], 2 * TC_TILE_BYTES);
-                    tma_load_2d_pair(sB + (size_t)s * TC_TILE_BYTES, &tmB,
-                                     mapa_shared(smem_u32(&b_full[s]), 0), kb * TC_BK, row0);
-                    if (row_ahead < a.N) tma_prefetch_l2_2d(&tmB, kb * TC_BK, row_ahead);
+                    if (lead) mbar_arrive_expect_tx(&b_full[s], 2 * stage_bytes);
+                    const uint32_t bar = mapa_shared(smem_u32(&b_full[s]), 0);
+                    unsigned char *dst = stage_ptr(s);
+                    // split BF16: items alternate hi, lo of K block i / 2
+                    const int kb = KIND == kTcBf16x3 ? (i >> 1) : i;
+                    const CUtensorMap *mb = (KIND == kTcBf16x3 && (i & 1)) ? &tmB2 : &tmB;
+                    if (streamed) {
+                        tma_load_2d_pair(dst, &tmA, bar, kb * kx, qrow0);
+                        dst += TP_TILE_BYTES;
+                    }
+                    tma_load_2d_pair(dst, mb, bar, kb * kx, row0);
+                    if (row_ahead < a.N) tma_prefetch_l2_2d(mb, kb * kx, row_ahead);
                     issued = it + 1;
                 }
                 if (*abort_flag) break;
@@ -300,8 +368,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
             // flight (the closing cluster barrier orders the odd CTA's exit
             // after this).
             if (lead) {
-                for (int it = max(0, issued - TP_STAGES); it < issued; ++it)
-                    if (!mbar_wait(&b_full[it % TP_STAGES], (it / TP_STAGES) & 1))
+                for (int it = max(0, issued - NST); it < issued; ++it)
+                    if (!mbar_wait(&b_full[it % NST], (it / NST) & 1))
                         atomicMax(a.status, (int)kDevTimeoutDrain);
                 for (int j = max(0, n_issued - TP_NSLOTS); j < n_issued; ++j)
                     if (!mbar_wait(&n_full[j % TP_NSLOTS], (j / TP_NSLOTS) & 1))
@@ -313,12 +381,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
     } else if (warp == 1) {
         // ---------------- MMA issuer (even CTA) ----------------
         if (lead && lane == 0) {
-            bool ok = n_my == 0 || mbar_wait(a_full, 0);
+            bool ok = n_my == 0 || KA == 0 || mbar_wait(a_full, 0);
             bool issued_mma = false;
             tc_fence_after();
             const uint64_t odesc = umma_desc_sw32(sOnes);
             for (int j = 0; j < n_my && ok; ++j) {
                 const int b = j & 1;
+                const uint32_t acc = tmem + (uint32_t)(b * TP_BN);
                 if (j >= 2 && !mbar_wait(&acc_empty[b], ((j >> 1) - 1) & 1)) {
                     ok = false;
                     break;
@@ -329,23 +398,36 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                     break;
                 }
                 tc_fence_after();
-                umma_bf16_pair(tmem + (uint32_t)(b * TP_BN), odesc,
-                               umma_desc_sw32(sN + (size_t)ns * TC_NORM_BYTES), TP_IDESC, 0u);
+                tp_mma_norm<KIND>(acc, odesc, umma_desc_sw32(sN + (size_t)ns * TP_NORM_BYTES));
                 umma_commit_pair_mc(&n_empty[ns], 0x3);
                 issued_mma = true;
-                for (int kb = 0; kb < KB; ++kb) {
-                    const int it = j * KB + kb, s = it % TP_STAGES;
-                    if (!mbar_wait(&b_full[s], (it / TP_STAGES) & 1) || *abort_flag) {
+                for (int i = 0; i < ITEMS; ++i) {
+                    const int it = j * ITEMS + i, s = it % NST;
+                    if (!mbar_wait(&b_full[s], (it / NST) & 1) || *abort_flag) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t adesc = umma_desc_sw128(sA + (size_t)kb * TC_TILE_BYTES);
-                    const uint64_t bdesc = umma_desc_sw128(sB + (size_t)s * TC_TILE_BYTES);
-#pragma unroll
-                    for (int k = 0; k < TC_BK / 16; ++k)
-                        umma_bf16_pair(tmem + (uint32_t)(b * TP_BN), adesc + (uint64_t)(2 * k),
-                                       bdesc + (uint64_t)(2 * k), TP_IDESC, 1u);
+                    const unsigned char *st = stage_ptr(s);
+                    const uint64_t bdesc = umma_desc_sw128(st + (streamed ? TP_TILE_BYTES : 0));
+                    if (streamed) {
+                        tp_mma_block<KIND>(acc, umma_desc_sw128(st), bdesc);
+                    } else if (KIND == kTcBf16x3) {
+                        const int kb = i >> 1;
+                        const uint64_t ahi = umma_desc_sw128(sR + (size_t)kb * TP_TILE_BYTES);
+                        if ((i & 1) == 0) {
+                            // B hi: A hi . B hi + A lo . B hi
+                            tp_mma_block<KIND>(acc, ahi, bdesc);
+                            tp_mma_block<KIND>(
+                                acc, umma_desc_sw128(sR + (size_t)(KB + kb) * TP_TILE_BYTES),
+                                bdesc);
+                        } else {
+                            tp_mma_block<KIND>(acc, ahi, bdesc);   // A hi . B lo
+                        }
+                    } else {
+                        tp_mma_block<KIND>(acc, umma_desc_sw128(sR + (size_t)i * TP_TILE_BYTES),
+                                           bdesc);
+                    }
                     umma_commit_pair_mc(&b_empty[s], 0x3);
                 }
                 if (!ok) break;
@@ -369,7 +451,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
         const int hc = (warp - 2) >> 2;
         const int qrow = qpair * TC_QT + (int)rank * TC_BM + qd * 32 + lane;
         float thr = -INFINITY;
-        if (MODE == 1 && qrow < a.Q) thr = a.thr[qrow];
+        if (MODE == 1 && qrow < a.Q) thr = a.thr[qrow] * a.thr_scale;
         float L[TC_KS];
 #pragma unroll
         for (int i = 0; i < TC_KS; ++i) L[i] = INFINITY;
@@ -455,13 +537,34 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
-// error bound of the BF16 expansion (see the file comment)
+// error bound of the expansion (see the file comment), per scan kind
 // ---------------------------------------------------------------------------
-KNN_DI float tc_error_bound(float qq, float r2, float T, int d_pad) {
-    const float g = (float)(d_pad + TC_NK) * 2.384185791015625e-07f;   // K * 2^-22
-    const float eps = 0.0078125f + 1.52587890625e-05f + g;              // 2^-7 + 2^-16 + g
-    return 2.f * eps * sqrtf(qq * r2) + g * (r2 + qq) + 9.5367431640625e-07f * (fabsf(T) + qq);
+// E_q = 2 eps ||q|| R + g (R^2 + ||q||^2) + abs_q ||q|| + abs_r R + abs_c
+//       + 2^-20 (|T| + ||q||^2),   R^2 = max ||r||^2:
+//   BF16        eps = 2^-7 + 2^-16 + g, g = (d_pad + 16) 2^-22
+//   split BF16  eps = 3 2^-16 + 2^-20 + g, g = (3 d_pad + 16) 2^-22: the
+//               dropped lo.lo product and the second roundings are 3u^2 +
+//               O(u^3) of sum |q_i r_i| (u = 2^-8)
+//   FP8 e4m3    eps = 2^-3 + 2^-8 + g, g = (d_pad8 + 32) 2^-22 (u = 2^-4),
+//               plus the absolute error of values below the normal range
+//               (half the subnormal spacing, 2^-10, in scaled units):
+//               abs_q = 2 (1 + u) 2^-10 sqrt(d) / s_r,
+//               abs_r = (1 + u) 2^-10 sqrt(d) / s_q,
+//               abs_c = d 2^-20 / (s_q s_r) + the norm split's residual.
+struct TcBound {
+    float eps, g, abs_q, abs_r, abs_c;
+};
+
+KNN_DI float tc_error_bound(float qq, float r2, float T, const TcBound &b) {
+    float e = 2.f * b.eps * sqrtf(qq * r2) + b.g * (r2 + qq) +
+              9.5367431640625e-07f * (fabsf(T) + qq);
+    if (b.abs_q != 0.f || b.abs_r != 0.f) e += b.abs_q * sqrtf(qq) + b.abs_r * sqrtf(r2);
+    return e + b.abs_c;
 }
+
+// Relative rounding of the FP32 direct-form distance chain used by the
+// re-rank's pruning: g = (d_pad + 16) 2^-22 (>= 4 gamma_d).
+KNN_DI float tc_fp32_gamma(int d_pad) { return (float)(d_pad + TC_NK) * 2.384185791015625e-07f; }
 
 // ---------------------------------------------------------------------------
 // prep kernels
@@ -496,30 +599,39 @@ KNN_DI void write_norm_row(__nv_bfloat16 *parts, int p, float s) {
 // Squared norm of each point of a dim x n set, translated by -center
 // (sequential FP32 fma over d), and optionally the largest squared norm
 // (non-negative float bits compare as unsigned).
+// With absmax_bits, also the largest |x - c| of any coordinate (FP8 scale).
 __global__ void tc_norms_kernel(const float *__restrict__ x, int n, long long ld, int d,
                                 const float *__restrict__ center, float *__restrict__ nrm,
-                                unsigned *__restrict__ max_bits) {
+                                unsigned *__restrict__ max_bits,
+                                unsigned *__restrict__ absmax_bits = nullptr) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    float s = 0.f;
+    float s = 0.f, am = 0.f;
     if (p < n) {
         for (int dd = 0; dd < d; ++dd) {
             const float v = x[(size_t)dd * ld + p] - center[dd];
             s = fmaf(v, v, s);
+            am = fmaxf(am, fabsf(v));
         }
         nrm[p] = s;
     }
-    unsigned m = __float_as_uint(s);
+    unsigned m = __float_as_uint(s), ma = __float_as_uint(am);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    for (int o = 16; o > 0; o >>= 1) {
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        ma = max(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+    }
     if ((threadIdx.x & 31) == 0 && max_bits) atomicMax(max_bits, m);
+    if ((threadIdx.x & 31) == 0 && absmax_bits) atomicMax(absmax_bits, ma);
 }
 
 // dim x n (row pitch ld) FP32 -> n x d_pad BF16 of scale * (x - center)
 // (scale a power of two, so bf16(scale y) = scale bf16(y)), zero-padded in
-// [d, d_pad).  32 x 32 tiles through shared memory.
+// [d, d_pad); with xlo also the lo part bf16(scale y - hi) of split BF16.
+// 32 x 32 tiles through shared memory.
 __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld, int d,
                                int d_pad, const float *__restrict__ center, float scale,
-                               __nv_bfloat16 *__restrict__ xb) {
+                               __nv_bfloat16 *__restrict__ xb,
+                               __nv_bfloat16 *__restrict__ xlo = nullptr) {
     __shared__ float tile[32][33];
     const int p0 = blockIdx.x * 32, d0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -534,7 +646,10 @@ __global__ void tc_pack_kernel(const float *__restrict__ x, int n, long long ld,
         const int p = p0 + ty + 8 * i, dd = d0 + tx;
         if (p < n && dd < d_pad) {
             const float v = dd < d ? tile[tx][ty + 8 * i] - center[dd] : 0.f;
-            xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(v * scale);
+            const __nv_bfloat16 hi = __float2bfloat16_rn(v * scale);
+            xb[(size_t)p * d_pad + dd] = hi;
+            if (xlo)
+                xlo[(size_t)p * d_pad + dd] = __float2bfloat16_rn(v * scale - __bfloat162float(hi));
         }
     }
 }
@@ -590,9 +705,11 @@ __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long
                                    const float *__restrict__ center,
                                    __nv_bfloat16 *__restrict__ xb, float *__restrict__ xt,
                                    __nv_bfloat16 *__restrict__ parts,
-                                   unsigned *__restrict__ max_bits) {
+                                   unsigned *__restrict__ max_bits,
+                                   unsigned *__restrict__ absmax_bits) {
     __shared__ float tile[32][33];
     __shared__ float cs[32];   // the chunk's translation
+    float am = 0.f;            // largest |x - c| this thread wrote
     const int p0 = (tile0 + tiles.tile((int)(blockIdx.x >> 3))) * TP_BN + (blockIdx.x & 7) * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     float s = 0.f;
@@ -626,11 +743,19 @@ __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long
             const int p = p0 + ty + 8 * i, dd = d0 + tx;
             if (p < n) {
                 const float v = tile[tx][ty + 8 * i];
-                xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(dd < d ? v - cs[tx] : 0.f);
+                const float y = dd < d ? v - cs[tx] : 0.f;
+                xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(y);
                 xt[(size_t)p * d_pad + dd] = v;
+                am = fmaxf(am, fabsf(y));
             }
         }
         __syncthreads();
+    }
+    {
+        unsigned ma = __float_as_uint(am);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ma = max(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+        if (tx == 0) atomicMax(absmax_bits, ma);
     }
     if (ty == 0) {
         const int p = p0 + tx;
@@ -642,13 +767,122 @@ __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long
     }
 }
 
+// Lo parts of split BF16 for the whole prepared set: from the FP32
+// point-major copy r and the translation c, lo = bf16(y - bf16(y)) with
+// y = r - c computed as tc_prep_ref_kernel computes it (so hi + lo splits
+// the same y the BF16 copy rounded).  Four consecutive elements per thread.
+__global__ void tc_ref_lo_kernel(const float *__restrict__ xt, long long n_elems, int d,
+                                 int d_pad, const float *__restrict__ center,
+                                 __nv_bfloat16 *__restrict__ xlo) {
+    const long long e0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    if (e0 >= n_elems) return;
+    const float4 v = *reinterpret_cast<const float4 *>(xt + e0);
+    const float vv[4] = {v.x, v.y, v.z, v.w};
+    __nv_bfloat16 out[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int dd = (int)((e0 + i) % d_pad);
+        const float y = dd < d ? vv[i] - center[dd] : 0.f;
+        const __nv_bfloat16 hi = __float2bfloat16_rn(y);
+        out[i] = __float2bfloat16_rn(y - __bfloat162float(hi));
+    }
+    *reinterpret_cast<uint2 *>(xlo + e0) = *reinterpret_cast<const uint2 *>(out);
+}
+
+// FP8 (e4m3) copy of the prepared set: byte (p, dd) = e4m3(s_r (r - c)), one
+// warp per point (coalesced reads of the FP32 point-major copy), rows of
+// d_pad8 bytes (d rounded up to 128, one K block; the FP32 rows are d_pad
+// <= d_pad8 floats), and the norm-step row: ||r - c||^2 (FP32) as
+// v = s_r ||r - c||^2 / kappa split greedily into up to 8 e4m3 parts (each
+// at most 448, the format's largest value; the remainder carried in
+// double), then zeros.  The A side's ones tile holds c1 = s_q kappa, so the
+// parts contribute s_q s_r ||r - c||^2 to the accumulator.  resid_bits: the
+// largest residual |v - sum parts| in unscaled units (kappa / s_r per unit
+// of v), a term of the error bound.
+__global__ void tc_pack_ref_f8_kernel(const float *__restrict__ xt, int n, int d, int d_pad,
+                                      int d_pad8, const float *__restrict__ center, float s_r,
+                                      float kappa, unsigned char *__restrict__ x8,
+                                      unsigned char *__restrict__ parts8,
+                                      unsigned *__restrict__ resid_bits) {
+    const int warps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    const int p = blockIdx.x * warps + (threadIdx.x >> 5);
+    if (p >= n) return;
+    const float *row = xt + (size_t)p * d_pad;
+    float s = 0.f;
+    for (int d0 = lane * 4; d0 < d_pad8; d0 += 128) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (d0 < d_pad) v = *reinterpret_cast<const float4 *>(row + d0);
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+        uint32_t packed = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float y = d0 + i < d ? vv[i] - center[d0 + i] : 0.f;
+            s = fmaf(y, y, s);
+            const __nv_fp8_e4m3 f(y * s_r);
+            packed |= (uint32_t)f.__x << (8 * i);
+        }
+        *reinterpret_cast<uint32_t *>(x8 + (size_t)p * d_pad8 + d0) = packed;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        double rem = (double)s * (double)s_r / (double)kappa;
+        unsigned char row8[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) row8[j] = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const __nv_fp8_e4m3 f((float)fmin(rem, 448.0));
+            row8[j] = f.__x;
+            rem -= (double)(float)f;
+        }
+        uint4 *dst = reinterpret_cast<uint4 *>(parts8 + (size_t)p * 32);
+        dst[0] = *reinterpret_cast<const uint4 *>(row8);
+        dst[1] = *reinterpret_cast<const uint4 *>(row8 + 16);
+        const float resid = (float)(fabs(rem) * (double)kappa / (double)s_r);
+        atomicMax(resid_bits, __float_as_uint(resid * 1.0000001f));
+    }
+}
+
+// dim x n FP32 queries -> n x d_pad8 e4m3 of scale (x - c) (scale = -2 s_q),
+// zero-padded; 32 x 32 tiles through shared memory as in tc_pack_kernel.
+__global__ void tc_pack_f8_kernel(const float *__restrict__ x, int n, long long ld, int d,
+                                  int d_pad8, const float *__restrict__ center, float scale,
+                                  unsigned char *__restrict__ x8) {
+    __shared__ float tile[32][33];
+    const int p0 = blockIdx.x * 32, d0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int dd = d0 + ty + 8 * i, p = p0 + tx;
+        tile[ty + 8 * i][tx] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int p = p0 + ty + 8 * i, dd = d0 + tx;
+        if (p < n && dd < d_pad8) {
+            const float v = dd < d ? tile[tx][ty + 8 * i] - center[dd] : 0.f;
+            x8[(size_t)p * d_pad8 + dd] = __nv_fp8_e4m3(v * scale).__x;
+        }
+    }
+}
+
 // Emission threshold: the KS-th smallest of the per-split pass-1 lists plus
 // the error bound E_q (so that the k-th exact distance only has to lie below
 // the sample's KS-th approximate one to certify); resets candidate counts.
+// The lists hold accumulator values (inv_scale turns them into a units).
+// thr_raw keeps the sample's KS-th value itself (a second scan of another
+// kind re-derives its threshold from it).  A query whose bound exceeds
+// three times the spread of its KS sample values is expected to overflow
+// its candidate list (about KS x stride points lie below T, and the band
+// [T, T + E] adds E / (T - L_0) times as many): n_wide counts them.
 __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
                                     const float *__restrict__ qn,
-                                    const unsigned *__restrict__ rmax_bits, int d_pad,
-                                    float *__restrict__ thr, int *__restrict__ count) {
+                                    const unsigned *__restrict__ rmax_bits, float inv_scale,
+                                    TcBound bound, float *__restrict__ thr,
+                                    float *__restrict__ thr_raw, int *__restrict__ count,
+                                    int *__restrict__ n_wide) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= Q) return;
     float L[TC_KS];
@@ -665,9 +899,24 @@ __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
             L[0] = fminf(L[0], v);
         }
     }
-    const float T = L[TC_KS - 1];
-    thr[q] = T + tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T, d_pad);
+    const float T = L[TC_KS - 1] * inv_scale;
+    const float E = tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T, bound);
+    thr[q] = T + E;
+    thr_raw[q] = T;
     count[q] = 0;
+    if (n_wide && E > 3.f * (T - L[0] * inv_scale)) atomicAdd(n_wide, 1);
+}
+
+// Thresholds of a scan of another kind from the raw sample thresholds:
+// thr = T + E_q(T) under that kind's bound.
+__global__ void tc_rethreshold_kernel(const float *__restrict__ thr_raw, int Q,
+                                      const float *__restrict__ qn,
+                                      const unsigned *__restrict__ rmax_bits, TcBound bound,
+                                      float *__restrict__ thr) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= Q) return;
+    const float T = thr_raw[q];
+    thr[q] = T + tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T, bound);
 }
 
 // Ascending bitonic sort of keys[0..P) (P a power of two) by one warp.
@@ -751,17 +1000,34 @@ KNN_DI void cp_async_wait_n() {
 // widened by 8 E; an overflowing list is scanned again with the same
 // threshold and a longer list, and overflowing that too (final_pass) it
 // goes to the exact kernel (NaN).  Warp-uniform; true if rejected.
-KNN_DI bool rr_reject_list(int c, int cmax, int k, int q, float qq, float r2, float T, int d_pad,
-                           int final_pass, int *fail_list, int *n_fail, float *retry, int lane) {
+// Bounds a re-rank works with: those of the scan that emitted the
+// candidates, whose accumulator values are a / a_scale.
+struct RrBounds {
+    TcBound cur;
+    float a_scale;
+};
+
+// A query that fails leaves the threshold of its second scan as a base
+// value and a factor: thr = base + f E_q(base) under the bound of the kind
+// the second scan uses (chosen once the failures are counted; f = 0: base
+// is the threshold, NaN: exact kernel).  Overflowing lists count in n_fail[1].
+KNN_DI bool rr_reject_list(int c, int cmax, int k, int q, float qq, float r2, float T,
+                           float T_raw, const RrBounds &rb, int final_pass, int *fail_list,
+                           int *n_fail, float *retry, float *retry_f, int lane) {
     if (c <= cmax && c >= k) return false;
     if (lane == 0) {
         fail_list[atomicAdd(n_fail, 1)] = q;
-        retry[q] = c < k ? T + 8.f * tc_error_bound(qq, r2, T, d_pad)
-                         : (final_pass ? __int_as_float(0x7fc00000) : T);
+        if (c < k) {
+            retry[q] = T + 8.f * tc_error_bound(qq, r2, T, rb.cur);
+            retry_f[q] = 0.f;
+        } else {
+            atomicAdd(n_fail + 1, 1);
+            retry[q] = final_pass ? __int_as_float(0x7fc00000) : T_raw;
+            retry_f[q] = final_pass ? 0.f : 1.f;
+        }
     }
     return true;
 }
-
 // Exact FP32 distances of the candidates keys[0..n) (point index in the low
 // 32 bits), in place: keys[t] = (distance, index).  One warp, 32 candidates
 // at a time, one per lane: the rows of the FP32 point-major copy are staged
@@ -776,14 +1042,14 @@ KNN_DI bool rr_reject_list(int c, int cmax, int k, int q, float qq, float r2, fl
 // ||q||^2, E_q = e_q) as float bits in stat[0] (atomic max) and counts the
 // candidates checked in the 64-bit counter at stat + 2.
 struct BoundStat {
-    float qq, e_q;
+    float qq, e_q, a_scale;
     unsigned *stat;
 };
 
 template <bool STAT = false>
 KNN_DI void rr_exact_distances(unsigned long long *keys, int n, const float *__restrict__ refT,
                                int d_pad, const float *qv, float *rows, int lane,
-                               BoundStat bs = BoundStat{0.f, 0.f, nullptr}) {
+                               BoundStat bs = BoundStat{0.f, 0.f, 1.f, nullptr}) {
     const int nch = d_pad / TC_RR_DCH;
     const int total = ((n + 31) / 32) * nch;
     constexpr int CPL = TC_RR_DCH / 4;   // 16-byte copies per row and chunk
@@ -837,7 +1103,7 @@ KNN_DI void rr_exact_distances(unsigned long long *keys, int n, const float *__r
         if (ch == nch - 1) {
             const int t = g * 32 + lane;
             if (STAT && t < n) {
-                const float a = ord_float((uint32_t)(keys[t] >> 32));
+                const float a = ord_float((uint32_t)(keys[t] >> 32)) * bs.a_scale;
                 const float ratio = fabsf(a + bs.qq - acc) / bs.e_q;
                 atomicMax(bs.stat, __float_as_uint(ratio));
                 atomicAdd(reinterpret_cast<unsigned long long *>(bs.stat + 2), 1ull);
@@ -850,21 +1116,22 @@ KNN_DI void rr_exact_distances(unsigned long long *keys, int n, const float *__r
 
 // Certification from a query's k smallest exact keys (sorted; keys[k - 1]
 // the k-th): certified, the query's sqrt distances and indices are written;
-// otherwise it joins fail_list with the threshold of a second scan that
-// certifies (see tc_rerank_kernel).  Warp-uniform.
+// otherwise it joins fail_list with the base threshold of a second scan
+// that certifies (see tc_rerank_kernel).  Warp-uniform.
 KNN_DI void rr_certify(const unsigned long long *keys, int q, float qq, float r2, float T,
-                       int d_pad, int k, float *__restrict__ out_dist, int *__restrict__ out_idx,
-                       long long ld_out, int *fail_list, int *n_fail, float *retry, int lane) {
+                       int d_pad, int k, const RrBounds &rb, float *__restrict__ out_dist,
+                       int *__restrict__ out_idx, long long ld_out, int *fail_list, int *n_fail,
+                       float *retry, float *retry_f, int lane) {
     int failed = 0;
     if (lane == 0) {
         const float dk = key_dist2(keys[k - 1]);
-        const float E = tc_error_bound(qq, r2, T, d_pad);
+        const float E = tc_error_bound(qq, r2, T, rb.cur);
         const float dkg = dk * (1.f + (float)d_pad * 2.384185791015625e-07f);
         failed = !(dkg + E < T + qq);
         if (failed) {
             fail_list[atomicAdd(n_fail, 1)] = q;
-            const float T2 = dkg - qq;
-            retry[q] = T2 + 2.5f * tc_error_bound(qq, r2, T2, d_pad);
+            retry[q] = dkg - qq;
+            retry_f[q] = 2.5f;
         }
     }
     if (__shfl_sync(0xffffffffu, failed, 0)) return;
@@ -880,12 +1147,13 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
     tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
                      const float *__restrict__ qry, long long ldq, const float *__restrict__ qn,
                      const unsigned *__restrict__ rmax_bits, const float *__restrict__ thr,
+                     const float *__restrict__ thr_raw, RrBounds rb,
                      const unsigned long long *__restrict__ cand, const int *__restrict__ count,
                      int cmax, int cpow, int Q, int k, float *__restrict__ out_dist,
                      int *__restrict__ out_idx, long long ld_out, int *__restrict__ fail_list,
                      int *__restrict__ n_fail, float *__restrict__ retry,
-                     unsigned long long *__restrict__ cand_total, int final_pass,
-                     unsigned *__restrict__ bound_stat) {
+                     float *__restrict__ retry_f, unsigned long long *__restrict__ cand_total,
+                     int final_pass, unsigned *__restrict__ bound_stat) {
     extern __shared__ unsigned char rsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -900,8 +1168,8 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
     const float qq = qn[q];
     const float r2 = __uint_as_float(*rmax_bits);
     const float T = thr[q];
-    if (rr_reject_list(c, cmax, k, q, qq, r2, T, d_pad, final_pass, fail_list, n_fail, retry,
-                       lane))
+    if (rr_reject_list(c, cmax, k, q, qq, r2, T, thr_raw ? thr_raw[q] : T, rb, final_pass,
+                       fail_list, n_fail, retry, retry_f, lane))
         return;
     // candidates sorted by (a, index)
     const unsigned long long *cq = cand + (size_t)q * cmax;
@@ -914,10 +1182,10 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
     // the prefix that can still reach the top-k
     int n_s;
     {
-        const float ak = ord_float((uint32_t)(keys[k - 1] >> 32));
-        const float E = tc_error_bound(qq, r2, ak, d_pad);
-        const float g = (float)(d_pad + TC_NK) * 2.384185791015625e-07f;
-        const float lim = ak + 2.f * E + 2.f * g * (fabsf(ak) + qq + E);
+        const float ak = ord_float((uint32_t)(keys[k - 1] >> 32)) * rb.a_scale;
+        const float E = tc_error_bound(qq, r2, ak, rb.cur);
+        const float g = tc_fp32_gamma(d_pad);
+        const float lim = (ak + 2.f * E + 2.f * g * (fabsf(ak) + qq + E)) / rb.a_scale;
         const uint32_t lim_o = ord_bits(__float_as_uint(lim));
         int cnt = 0;
         for (int t0 = 0; t0 < c; t0 += 32) {
@@ -928,14 +1196,15 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
         n_s = max(cnt, k);   // keys are sorted, so the kept ones are a prefix
     }
     rr_exact_distances<STAT>(keys, n_s, refT, d_pad, qv, rows, lane,
-                             BoundStat{qq, tc_error_bound(qq, r2, T, d_pad), bound_stat});
+                             BoundStat{qq, tc_error_bound(qq, r2, T, rb.cur), rb.a_scale,
+                                       bound_stat});
     int P2 = 32;
     while (P2 < n_s) P2 <<= 1;
     for (int t = n_s + lane; t < P2; t += 32) keys[t] = kKeyInf;
     __syncwarp();
     warp_bitonic_sort(keys, P2, lane);
-    rr_certify(keys, q, qq, r2, T, d_pad, k, out_dist, out_idx, ld_out, fail_list, n_fail, retry,
-               lane);
+    rr_certify(keys, q, qq, r2, T, d_pad, k, rb, out_dist, out_idx, ld_out, fail_list, n_fail,
+               retry, retry_f, lane);
 }
 
 // Incremental re-rank for a reference set that arrives in pieces (the
@@ -988,11 +1257,12 @@ __global__ void tc_certify_pieces_kernel(const int *__restrict__ count, int cmax
                                          const float *__restrict__ qn,
                                          const unsigned *__restrict__ rmax_bits,
                                          const float *__restrict__ thr,
+                                         const float *__restrict__ thr_raw, RrBounds rb,
                                          const unsigned long long *__restrict__ run, int Q, int k,
                                          int d_pad, float *__restrict__ out_dist,
                                          int *__restrict__ out_idx, long long ld_out,
                                          int *__restrict__ fail_list, int *__restrict__ n_fail,
-                                         float *__restrict__ retry,
+                                         float *__restrict__ retry, float *__restrict__ retry_f,
                                          unsigned long long *__restrict__ cand_total) {
     const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (q >= Q) return;
@@ -1001,9 +1271,11 @@ __global__ void tc_certify_pieces_kernel(const int *__restrict__ count, int cmax
     const float qq = qn[q];
     const float r2 = __uint_as_float(*rmax_bits);
     const float T = thr[q];
-    if (rr_reject_list(c, cmax, k, q, qq, r2, T, d_pad, 0, fail_list, n_fail, retry, lane)) return;
-    rr_certify(run + (size_t)q * k, q, qq, r2, T, d_pad, k, out_dist, out_idx, ld_out, fail_list,
-               n_fail, retry, lane);
+    if (rr_reject_list(c, cmax, k, q, qq, r2, T, thr_raw[q], rb, 0, fail_list, n_fail, retry,
+                       retry_f, lane))
+        return;
+    rr_certify(run + (size_t)q * k, q, qq, r2, T, d_pad, k, rb, out_dist, out_idx, ld_out,
+               fail_list, n_fail, retry, retry_f, lane);
 }
 
 // Fallback plumbing: gather the uncertified queries into a dense d x m set
@@ -1028,13 +1300,21 @@ __global__ void scatter_results_kernel(const float *__restrict__ sd, const int *
     }
 }
 
-// Second-chance scan of the uncertified queries: compact thresholds.
+// Second-chance scan of the uncertified queries: compacted thresholds
+// under the bound of the second scan's kind (qn already holds the
+// compacted queries' norms).
 __global__ void tc_retry_prep_kernel(const int *__restrict__ list, int m,
-                                     const float *__restrict__ retry, float *__restrict__ thr,
-                                     int *__restrict__ count) {
+                                     const float *__restrict__ retry,
+                                     const float *__restrict__ retry_f,
+                                     const float *__restrict__ qn,
+                                     const unsigned *__restrict__ rmax_bits, TcBound bound,
+                                     float *__restrict__ thr, int *__restrict__ count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m) {
-        thr[i] = retry[list[i]];
+        const float base = retry[list[i]], f = retry_f[list[i]];
+        thr[i] = f == 0.f ? base
+                          : base + f * tc_error_bound(qn[i], __uint_as_float(*rmax_bits), base,
+                                                      bound);
         count[i] = 0;
     }
 }
@@ -1049,25 +1329,70 @@ bool encode_bf16_kmajor(CUtensorMap *m, const void *base, int rows, int d_pad) {
                      (uint64_t)rows, (uint64_t)d_pad, TC_BK, TC_BM, CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
-// Norm-step rows [rows][16] BF16, 128-row boxes with the 32-byte swizzle.
-bool encode_norm_rows(CUtensorMap *m, const void *base, int rows) {
-    return encode_2d(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, (uint64_t)TC_NK, (uint64_t)rows,
-                     (uint64_t)TC_NK, TC_NK, TC_BM, CU_TENSOR_MAP_SWIZZLE_32B);
+// FP8 operand rows [rows][d_pad8] bytes: 128-byte x 128-row boxes.
+bool encode_u8_kmajor(CUtensorMap *m, const void *base, int rows, int d_pad8) {
+    return encode_2d(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, base, (uint64_t)d_pad8, (uint64_t)rows,
+                     (uint64_t)d_pad8, 128, TC_BM, CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
-// Candidate lists: first scan cmax = 4 * KS * stride (<= 1280 for k <=
-// 128); the second scan of the queries whose list overflowed reuses the
+// Norm-step rows, 32 bytes each (16 BF16 or 32 FP8), 128-row boxes with the
+// 32-byte swizzle.
+bool encode_norm_rows(CUtensorMap *m, const void *base, int rows, bool fp8) {
+    return fp8 ? encode_2d(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, base, 32, (uint64_t)rows, 32, 32,
+                           TC_BM, CU_TENSOR_MAP_SWIZZLE_32B)
+               : encode_2d(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, (uint64_t)TC_NK,
+                           (uint64_t)rows, (uint64_t)TC_NK, TC_NK, TC_BM,
+                           CU_TENSOR_MAP_SWIZZLE_32B);
+}
+
+// Candidate lists: first scan cmax = 4 * KS * stride (<= 2560 for k <=
+// 256); the second scan of the queries whose list overflowed reuses the
 // whole list buffer, up to kTcCmaxRetry entries per query.  The re-rank
 // kernel's shared memory (keys padded to a power of two) is capped at
 // kRerankSmem per block: fewer warps per block for long lists.
 constexpr int kTcCmaxRetry = 8192;
 constexpr size_t kRerankSmem = 200 * 1024;
+constexpr int kTcMaxDim = 4096;
+constexpr int kTcMaxK = 256;
 
 struct TcPlan {
-    int d_pad, kb, qtiles, cmax;
+    int d_pad, d_pad8, qtiles, cmax;
     int n_tiles2, splits1;   // 256-point tiles; pass-1 splits over CTA pairs
     TileRuns sample;         // pass-1 tiles
 };
+
+// Operand feed of one scan kind: K blocks of 128 bytes per operand row,
+// resident A tiles (0: A streams beside B), ring stages and items per
+// reference tile.
+struct TcOp {
+    int kind, kb, ka, stages, items;
+};
+
+TcOp tc_op(int kind, int d_pad, int d_pad8) {
+    TcOp o;
+    o.kind = kind;
+    if (kind == kTcFp8) {
+        o.kb = d_pad8 / 128;
+        o.ka = o.kb;
+        o.items = o.kb;
+    } else if (kind == kTcBf16x3) {
+        o.kb = d_pad / 64;
+        o.ka = 2 * o.kb;
+        o.items = 2 * o.kb;
+    } else {
+        o.kb = d_pad / 64;
+        o.ka = o.kb <= TP_MAX_RESIDENT_A ? o.kb : 0;
+        o.items = o.kb;
+    }
+    o.stages = o.ka > 0 ? TP_REGION_TILES - o.ka : TP_REGION_TILES / 2;
+    return o;
+}
+
+bool kind_fits(int kind, int d_pad, int d_pad8) {
+    if (kind == kTcBf16x3) return 2 * (d_pad / 64) <= TP_MAX_RESIDENT_A;
+    if (kind == kTcFp8) return d_pad8 / 128 <= TP_MAX_RESIDENT_A;
+    return true;
+}
 
 // Splits that fill whole waves of one CTA per SM for `tiles` tiles per
 // query tile, with at least min_tiles per CTA; modelled per-CTA cost =
@@ -1090,7 +1415,7 @@ static int choose_splits(int qtiles, int tiles, int min_tiles, double fixed, int
 TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
     TcPlan p;
     p.d_pad = (d + 63) / 64 * 64;
-    p.kb = p.d_pad / 64;
+    p.d_pad8 = (d + 127) / 128 * 128;
     p.qtiles = (Q + TC_QT - 1) / TC_QT;
     // pass 1 samples one tile in `stride`: the sample must hold about 2.5k
     // points below T_q, KS * stride >= 2.5k
@@ -1109,6 +1434,28 @@ TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
     return p;
 }
 
+// Error-bound constants of each kind (see tc_error_bound).
+TcBound bound_of(int kind, int d, int d_pad, int d_pad8, float s_q, float s_r, float resid8) {
+    TcBound b{0.f, 0.f, 0.f, 0.f, 0.f};
+    const double two22 = 2.384185791015625e-07;   // 2^-22
+    if (kind == kTcBf16x3) {
+        b.g = (float)((3.0 * d_pad + TC_NK) * two22);
+        b.eps = (float)(3.0 * 1.52587890625e-05 + 9.5367431640625e-07) + b.g;
+    } else if (kind == kTcFp8) {
+        const double u = 0.0625, eta = 9.765625e-04;   // 2^-4, 2^-10
+        b.g = (float)((d_pad8 + 32.0) * two22);
+        b.eps = (float)(2.0 * u + u * u) + b.g;
+        const double sd = std::sqrt((double)d);
+        b.abs_q = (float)(2.0 * (1.0 + u) * eta * sd / s_r * 1.0000001);
+        b.abs_r = (float)((1.0 + u) * eta * sd / s_q * 1.0000001);
+        b.abs_c = (float)(((double)d * eta * eta / ((double)s_q * s_r) + resid8) * 1.0000001);
+    } else {
+        b.g = (float)((d_pad + TC_NK) * two22);
+        b.eps = 0.0078125f + 1.52587890625e-05f + b.g;
+    }
+    return b;
+}
+
 struct Carve {
     unsigned char *p;
     size_t used, cap;
@@ -1121,16 +1468,35 @@ struct Carve {
     }
 };
 
+int read_count(const int *dev, int *host_pinned, cudaStream_t st, int &out, int n = 1) {
+    if (cudaMemcpyAsync(host_pinned, dev, n * sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return kErrCuda;
+    out = *host_pinned;
+    return kOk;
+}
+
+float pow2_floor(double x) { return (float)std::ldexp(1.0, (int)std::floor(std::log2(x))); }
+float pow2_ceil(double x) { return (float)std::ldexp(1.0, (int)std::ceil(std::log2(x))); }
+
 }  // namespace
 
 bool tc_supported(int N, int Q, int d, int k) {
-    return d >= 16 && d <= TC_KBMAX * TC_BK && k >= 1 && k <= 128 && N >= 32768 && Q >= 1;
+    return d >= 16 && d <= kTcMaxDim && k >= 1 && k <= kTcMaxK && N >= 32768 && Q >= 1;
+}
+
+bool tc_fp8_supported(int d) {
+    const int d_pad = (d + 63) / 64 * 64, d_pad8 = (d + 127) / 128 * 128;
+    return kind_fits(kTcFp8, d_pad, d_pad8);
 }
 
 size_t tc_ref_bytes(int N, int d) {
-    const int d_pad = (d + 63) / 64 * 64;
+    const int d_pad = (d + 63) / 64 * 64, d_pad8 = (d + 127) / 128 * 128;
+    const size_t lo = kind_fits(kTcBf16x3, d_pad, d_pad8) ? (size_t)N * d_pad * 2 : 0;
+    const size_t f8 = kind_fits(kTcFp8, d_pad, d_pad8) ? (size_t)N * d_pad8 + (size_t)N * 32 : 0;
     return (size_t)N * d_pad * 2 + (size_t)N * d_pad * 4 + (size_t)N * TC_NK * 2 +
-           (size_t)d_pad * 4 + 5 * 256;
+           (size_t)d_pad * 4 + lo + f8 + 12 * 256;
 }
 
 static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
@@ -1141,16 +1507,18 @@ static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
 
 size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     const TcPlan p = plan_tc(N, Q, d, k, num_sms);
-    size_t b = (size_t)p.qtiles * TC_QT * p.d_pad * 2 + (size_t)Q * 4 * 6 + 16;
+    const size_t rows = (size_t)p.qtiles * TC_QT;
+    size_t b = rows * p.d_pad * 2 * 2 + rows * p.d_pad8 + (size_t)Q * 4 * 8 + 64;
     b += (size_t)TP_LISTS * p.splits1 * Q * TC_KS * 4;
     b += (size_t)Q * p.cmax * 8;
     b += fallback_bytes(N, Q, d, k, num_sms);   // worst case: every query uncertified
-    return b + 16 * 256;
+    return b + 24 * 256;
 }
 
 int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, int d,
                    cudaStream_t st) {
-    if (cudaMemsetAsync(v.rmax_bits, 0, sizeof(unsigned), st) != cudaSuccess) return kErrCuda;
+    if (cudaMemsetAsync(v.rmax_bits, 0, 3 * 256, st) != cudaSuccess) return kErrCuda;
+    if (v.state) *v.state = TcRefState{};
     const int n_tiles = (N + TP_BN - 1) / TP_BN;
     const int rc = tc_center_from_tiles(v, ref, N, ldr, d, contiguous_tiles(n_tiles),
                                         kCenterStride, st);
@@ -1172,89 +1540,217 @@ int tc_prepare_ref_tiles(const TcRefView &v, const float *ref, int N, long long 
     if (tiles.units <= 0) return kOk;
     if (tiles.run < 1 || tiles.period < tiles.run) return kErrInvalid;
     const int d_pad = (d + 63) / 64 * 64;
-    tc_prep_ref_kernel<<<tiles.units * 8, dim3(32, 8), 0, st>>>(ref, N, ldr, d, d_pad, tile0,
-                                                                tiles, v.center, v.refB, v.refT,
-                                                                v.refN, v.rmax_bits);
+    tc_prep_ref_kernel<<<tiles.units * 8, dim3(32, 8), 0, st>>>(
+        ref, N, ldr, d, d_pad, tile0, tiles, v.center, v.refB, v.refT, v.refN, v.rmax_bits,
+        v.absmax_bits);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
 int tc_tile_points() { return TP_BN; }
 
-TcRefView tc_carve_ref(void *mem, int N, int d) {
-    const int d_pad = (d + 63) / 64 * 64;
+TcRefView tc_carve_ref(void *mem, int N, int d, TcRefState *state) {
+    const int d_pad = (d + 63) / 64 * 64, d_pad8 = (d + 127) / 128 * 128;
     Carve cv{static_cast<unsigned char *>(mem), 0, 0};
     TcRefView v;
     v.refB = cv.take<__nv_bfloat16>((size_t)N * d_pad);
     v.refT = cv.take<float>((size_t)N * d_pad);
     v.refN = cv.take<__nv_bfloat16>((size_t)N * TC_NK);
-    v.rmax_bits = cv.take<unsigned>(1);
+    // three words 256 bytes apart, cleared together by tc_prepare_ref
+    v.rmax_bits = cv.take<unsigned>(64);
+    v.absmax_bits = cv.take<unsigned>(64);
+    v.resid8_bits = cv.take<unsigned>(64);
     v.center = cv.take<float>(d_pad);
+    v.refBlo = kind_fits(kTcBf16x3, d_pad, d_pad8) ? cv.take<__nv_bfloat16>((size_t)N * d_pad)
+                                                   : nullptr;
+    const bool f8 = kind_fits(kTcFp8, d_pad, d_pad8);
+    v.ref8 = f8 ? cv.take<unsigned char>((size_t)N * d_pad8) : nullptr;
+    v.refN8 = f8 ? cv.take<unsigned char>((size_t)N * 32) : nullptr;
+    v.state = state;
+    if (state) *state = TcRefState{};
     return v;
 }
 
 namespace {
 
-// Emission scan of the reference tiles [tb, te) (256-point tiles) for the Q
-// queries whose BF16 copy is qB, lists of stride cmax.
-int emit_scan(const TcRun &r, cudaStream_t st, const __nv_bfloat16 *qB, int Q, const float *thr,
-              int cmax, int tb, int te) {
+// The split-BF16 lo parts of the reference set, once per prepared set.
+int ensure_ref_lo(const TcRun &r, cudaStream_t st) {
+    TcRefState *s = r.R.state;
+    if (!r.R.refBlo || !s) return kErrUnsupported;
+    if (s->lo_ready) return kOk;
+    const long long n = (long long)r.P.N * r.d_pad;
+    tc_ref_lo_kernel<<<(unsigned)((n / 4 + 255) / 256), 256, 0, st>>>(r.R.refT, n, r.P.d, r.d_pad,
+                                                                     r.R.center, r.R.refBlo);
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    s->lo_ready = true;
+    return kOk;
+}
+
+// The FP8 copy of the reference set, once per prepared set: reads back
+// the set's largest |r - c| and ||r - c||^2 (one synchronisation) for the
+// scale s_r = 2^floor(log2(448 / max|r - c|)) and the norm-step unit
+// kappa = 2^ceil(log2(s_r max||r - c||^2 / 896)) (so the norm needs at most
+// two saturated parts before the remainder).
+int ensure_ref_f8(const TcRun &r, cudaStream_t st, unsigned *host_tmp) {
+    TcRefState *s = r.R.state;
+    if (!r.R.ref8 || !s) return kErrUnsupported;
+    if (s->f8_ready) return kOk;
+    if (cudaMemcpyAsync(host_tmp, r.R.rmax_bits, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(host_tmp + 1, r.R.absmax_bits, 4, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return kErrCuda;
+    float r2, am;
+    std::memcpy(&r2, host_tmp, 4);
+    std::memcpy(&am, host_tmp + 1, 4);
+    if (!(am > 0.f) || !std::isfinite(am) || !std::isfinite(r2)) return kErrUnsupported;
+    s->absmax_r = am;
+    s->r2max = r2;
+    s->s_r = pow2_floor(448.0 / am);
+    s->kappa = pow2_ceil(std::max(1e-30, (double)s->s_r * r2 / 896.0));
+    if (cudaMemsetAsync(r.R.resid8_bits, 0, 4, st) != cudaSuccess) return kErrCuda;
+    constexpr int W = 8;
+    tc_pack_ref_f8_kernel<<<(r.P.N + W - 1) / W, W * 32, 0, st>>>(
+        r.R.refT, r.P.N, r.P.d, r.d_pad, r.d_pad8, r.R.center, s->s_r, s->kappa, r.R.ref8,
+        r.R.refN8, r.R.resid8_bits);
+    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    if (cudaMemcpyAsync(host_tmp, r.R.resid8_bits, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return kErrCuda;
+    std::memcpy(&s->resid8, host_tmp, 4);
+    s->f8_ready = true;
+    return kOk;
+}
+
+// Scan of the reference tiles [tile_base + tiles.tile(u)) for the Q queries
+// of the operand copies qB (BF16 hi), qBlo (lo) or q8 (FP8), in `kind`.
+// MODE 1 (emit) with thresholds thr, lists of stride cmax; MODE 0 (sample)
+// into r.p1.
+template <int MODE>
+int launch_scan(const TcRun &r, cudaStream_t st, int kind, const __nv_bfloat16 *qB,
+                const __nv_bfloat16 *qBlo, const unsigned char *q8, int Q, const float *thr,
+                int cmax, int tile_base, const TileRuns &tiles, int n_splits) {
     const TcProblem &P = r.P;
-    CUtensorMap tmA, tmB, tmN;
-    if (!encode_bf16_kmajor(&tmA, qB, Q, r.d_pad)) return kErrTensorMap;
-    if (!encode_bf16_kmajor(&tmB, r.R.refB, P.N, r.d_pad)) return kErrTensorMap;
-    if (!encode_norm_rows(&tmN, r.R.refN, P.N)) return kErrTensorMap;
-    const int qtiles = (Q + TC_QT - 1) / TC_QT;
+    if (!kind_fits(kind, r.d_pad, r.d_pad8)) return kErrUnsupported;
+    const TcOp op = tc_op(kind, r.d_pad, r.d_pad8);
+    CUtensorMap tmA, tmA2, tmB, tmB2, tmN;
+    bool ok;
+    if (kind == kTcFp8) {
+        ok = encode_u8_kmajor(&tmA, q8, Q, r.d_pad8) &&
+             encode_u8_kmajor(&tmB, r.R.ref8, P.N, r.d_pad8) &&
+             encode_norm_rows(&tmN, r.R.refN8, P.N, true);
+        tmA2 = tmA;
+        tmB2 = tmB;
+    } else {
+        ok = encode_bf16_kmajor(&tmA, qB, Q, r.d_pad) &&
+             encode_bf16_kmajor(&tmB, r.R.refB, P.N, r.d_pad) &&
+             encode_norm_rows(&tmN, r.R.refN, P.N, false);
+        if (kind == kTcBf16x3) {
+            ok = ok && encode_bf16_kmajor(&tmA2, qBlo, Q, r.d_pad) &&
+                 encode_bf16_kmajor(&tmB2, r.R.refBlo, P.N, r.d_pad);
+        } else {
+            tmA2 = tmA;
+            tmB2 = tmB;
+        }
+    }
+    if (!ok) return kErrTensorMap;
     TpArgs a;
     a.N = P.N;
     a.Q = Q;
-    a.kb_count = r.kb;
-    a.tile_base = tb;
-    a.tiles = contiguous_tiles(te - tb);
-    a.n_splits = choose_splits(qtiles, te - tb, 8, 2.0, std::max(1, P.num_sms / 2));
+    a.kb = op.kb;
+    a.ka = op.ka;
+    a.stages = op.stages;
+    a.items = op.items;
+    a.tile_base = tile_base;
+    a.tiles = tiles;
+    a.n_splits = n_splits;
     a.thr = thr;
-    a.p1 = nullptr;
+    a.thr_scale = kind == kTcFp8 ? r.scale : 1.f;
+    if (kind == kTcFp8) {
+        // c1 = s_q kappa, a power of two the e4m3 format holds exactly
+        const unsigned char c1 = __nv_fp8_e4m3(r.s_q * r.R.state->kappa).__x;
+        a.ones_word = 0x01010101u * c1;
+    } else {
+        a.ones_word = 0x3F803F80u;   // BF16 1.0, twice
+    }
+    a.p1 = r.p1;
     a.cand = r.cand;
     a.count = r.count;
     a.cmax = cmax;
     a.status = P.status;
-    knn_tc_pair_scan_kernel<1><<<dim3(2 * qtiles, a.n_splits), TP_THREADS, TP_SMEM, st>>>(
-        tmA, tmB, tmN, a);
-    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
+    const dim3 grid(2 * ((Q + TC_QT - 1) / TC_QT), n_splits);
+    auto go = [&](auto kern) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)TP_SMEM);
+        if (e != cudaSuccess) return (int)kErrLaunch;
+        kern<<<grid, TP_THREADS, TP_SMEM, st>>>(tmA, tmA2, tmB, tmB2, tmN, a);
+        return cudaGetLastError() == cudaSuccess ? (int)kOk : (int)kErrLaunch;
+    };
+    switch (kind) {
+        case kTcBf16x3: return go(knn_tc_pair_scan_kernel<MODE, kTcBf16x3>);
+        case kTcFp8: return go(knn_tc_pair_scan_kernel<MODE, kTcFp8>);
+        default: return go(knn_tc_pair_scan_kernel<MODE, kTcBf16>);
+    }
+}
+
+// Emission scan of the reference tiles [tb, te).
+int emit_scan(const TcRun &r, cudaStream_t st, int kind, int Q, const float *thr, int cmax,
+              int tb, int te) {
+    const int qtiles = (Q + TC_QT - 1) / TC_QT;
+    const int splits = choose_splits(qtiles, te - tb, 8, 2.0, std::max(1, r.P.num_sms / 2));
+    return launch_scan<1>(r, st, kind, r.qB, r.qBlo, r.q8, Q, thr, cmax, tb,
+                          contiguous_tiles(te - tb), splits);
+}
+
+TcBound run_bound(const TcRun &r, int kind) {
+    const TcRefState *s = r.R.state;
+    return bound_of(kind, r.P.d, r.d_pad, r.d_pad8, r.s_q, s ? s->s_r : 1.f, s ? s->resid8 : 0.f);
 }
 
 // Exact re-rank + certification of Q queries (see tc_rerank_kernel) whose
-// candidate lists have stride cmax.
-int rerank(const TcRun &r, cudaStream_t st, int Q, int cmax, const float *qry, long long ldq,
-           const float *qn, const float *thr, float *out_dist, int *out_idx, long long ld_out,
-           int *fail, bool final_pass) {
+// candidate lists (from a scan of `kind`) have stride cmax.
+int rerank(const TcRun &r, cudaStream_t st, int kind, int Q, int cmax, const float *qry,
+           long long ldq, const float *qn, const float *thr, const float *thr_raw,
+           float *out_dist, int *out_idx, long long ld_out, int *fail, bool final_pass) {
     const TcProblem &P = r.P;
-    if (cudaMemsetAsync(r.nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
+    if (cudaMemsetAsync(r.nfail, 0, 2 * sizeof(int), st) != cudaSuccess) return kErrCuda;
     int cpow = 1;
     while (cpow < cmax) cpow <<= 1;
     int warps = TC_RR_WARPS;
     while (warps > 1 && (size_t)warps * tc_rr_warp_bytes(r.d_pad, cpow) > kRerankSmem) warps >>= 1;
     const size_t rsmem = (size_t)warps * tc_rr_warp_bytes(r.d_pad, cpow);
-    // one fixed limit for every launch, so that calls from several host
-    // threads never lower it under each other
+    RrBounds rb;
+    rb.cur = run_bound(r, kind);
+    rb.a_scale = kind == kTcFp8 ? 1.f / r.scale : 1.f;
     // the bound statistic runs in its own instantiation, only when asked for
     auto kern = P.bound_stat ? tc_rerank_kernel<true> : tc_rerank_kernel<false>;
+    // one fixed limit for every launch, so that calls from several host
+    // threads never lower it under each other
     if (rsmem > kRerankSmem ||
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kRerankSmem) != cudaSuccess)
         return kErrLaunch;
     kern<<<(Q + warps - 1) / warps, warps * 32, rsmem, st>>>(
-        r.R.refT, P.d, r.d_pad, qry, ldq, qn, r.R.rmax_bits, thr, r.cand, r.count, cmax, cpow,
-        Q, P.k, out_dist, out_idx, ld_out, fail, r.nfail, r.retry, r.cand_total,
-        final_pass ? 1 : 0, P.bound_stat);
+        r.R.refT, P.d, r.d_pad, qry, ldq, qn, r.R.rmax_bits, thr, thr_raw, rb, r.cand, r.count,
+        cmax, cpow, Q, P.k, out_dist, out_idx, ld_out, fail, r.nfail, r.retry, r.retry_f,
+        r.cand_total, final_pass ? 1 : 0, P.bound_stat);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
-int read_count(const int *dev, int *host_pinned, cudaStream_t st, int &out) {
-    if (cudaMemcpyAsync(host_pinned, dev, sizeof(int), cudaMemcpyDeviceToHost, st) !=
-            cudaSuccess ||
+// FP8 query scale (reads back the batch's largest |q - c|): s_q =
+// 2^floor(log2(min(224 / max|q - c|, 256 / kappa))), so that -2 s_q q and
+// the ones value c1 = s_q kappa both fit e4m3.
+int fp8_query_scale(TcRun &r, cudaStream_t st, unsigned *dev_absmax, unsigned *host_tmp) {
+    if (cudaMemcpyAsync(host_tmp, dev_absmax, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return kErrCuda;
-    out = *host_pinned;
+    float aq;
+    std::memcpy(&aq, host_tmp, 4);
+    const TcRefState *s = r.R.state;
+    const double lim = std::min(aq > 0.f ? 224.0 / aq : 1e30, 256.0 / s->kappa);
+    r.s_q = pow2_floor(lim);
+    const double c1 = (double)r.s_q * s->kappa;
+    if (!(c1 >= 1.0 / 512.0) || !std::isfinite(aq)) return kErrUnsupported;
+    r.scale = r.s_q * s->s_r;
     return kOk;
 }
 
@@ -1270,21 +1766,32 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     r.P = P;
     r.R = R;
     r.d_pad = p.d_pad;
-    r.kb = p.kb;
+    r.d_pad8 = p.d_pad8;
     r.qtiles = p.qtiles;
     r.n_tiles2 = p.n_tiles2;
     r.splits1 = p.splits1;
     r.sample = p.sample;
     r.cmax = p.cmax;
+    r.kind = kTcBf16;
+    r.s_q = 1.f;
+    r.scale = 1.f;
+    const bool fp8 = P.request == kTcReqFp8;
+    if (fp8 && (!R.ref8 || !R.state || !P.host_tmp)) return kErrUnsupported;
     Carve cv{static_cast<unsigned char *>(P.scratch), 0, P.scratch_bytes};
-    r.qB = cv.take<__nv_bfloat16>((size_t)p.qtiles * TC_QT * p.d_pad);
+    const size_t rows = (size_t)p.qtiles * TC_QT;
+    r.qB = cv.take<__nv_bfloat16>(rows * p.d_pad);
+    r.qBlo = cv.take<__nv_bfloat16>(rows * p.d_pad);
+    r.q8 = cv.take<unsigned char>(rows * p.d_pad8);
     r.qn = cv.take<float>(P.Q);
     r.thr = cv.take<float>(P.Q);
+    r.thr_raw = cv.take<float>(P.Q);
     r.retry = cv.take<float>(P.Q);
+    r.retry_f = cv.take<float>(P.Q);
     r.count = cv.take<int>(P.Q);
     r.fail = cv.take<int>(P.Q);
     r.fail2 = cv.take<int>(P.Q);
     r.nfail = cv.take<int>(4);
+    r.nwide = cv.take<int>(4);   // [0] predicted overflows, [2] query max |q - c| bits
     r.cand_total = cv.take<unsigned long long>(1);
     r.p1 = cv.take<float>((size_t)TP_LISTS * p.splits1 * P.Q * TC_KS);
     r.cand = cv.take<unsigned long long>((size_t)P.Q * p.cmax);
@@ -1299,20 +1806,27 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     r.run_keys = nullptr;
     r.done = nullptr;
 
-    // queries: norms + BF16 K-major copy of -2 q
-    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(P.qry, P.Q, P.ldq, P.d, R.center, r.qn,
-                                                       nullptr);
-    tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
-        P.qry, P.Q, P.ldq, P.d, p.d_pad, R.center, -2.0f, r.qB);
+    // queries: norms (and their largest |q - c|) + BF16 K-major copy of -2 q
+    if (cudaMemsetAsync(r.nwide, 0, 4 * sizeof(int), st) != cudaSuccess) return kErrCuda;
+    tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
+        P.qry, P.Q, P.ldq, P.d, R.center, r.qn, nullptr,
+        fp8 ? reinterpret_cast<unsigned *>(r.nwide + 2) : nullptr);
+    if (!fp8)
+        tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
+            P.qry, P.Q, P.ldq, P.d, p.d_pad, R.center, -2.0f, r.qB);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    if (fp8) {
+        // the reference set's FP8 copy, then the queries' scale and copy
+        unsigned *host_tmp = reinterpret_cast<unsigned *>(P.host_tmp);
+        int rc = ensure_ref_f8(r, st, host_tmp);
+        if (rc == kOk) rc = fp8_query_scale(r, st, reinterpret_cast<unsigned *>(r.nwide + 2), host_tmp);
+        if (rc != kOk) return rc;
+        tc_pack_f8_kernel<<<dim3((P.Q + 31) / 32, p.d_pad8 / 32), dim3(32, 8), 0, st>>>(
+            P.qry, P.Q, P.ldq, P.d, p.d_pad8, R.center, -2.0f * r.s_q, r.q8);
+        if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+        r.kind = kTcFp8;
+    }
     if (P.timer) P.timer->mark(st, kPhaseTcPrepQuery);
-    if (cudaFuncSetAttribute(knn_tc_pair_scan_kernel<0>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TP_SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(knn_tc_pair_scan_kernel<1>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TP_SMEM) != cudaSuccess)
-        return kErrLaunch;
     if (cudaMemsetAsync(r.cand_total, 0, sizeof(unsigned long long), st) != cudaSuccess)
         return kErrCuda;
     return kOk;
@@ -1320,32 +1834,33 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
 
 int tc_run_pass1(TcRun &r, cudaStream_t st) {
     const TcProblem &P = r.P;
-    CUtensorMap tmA, tmB, tmN;
-    if (!encode_bf16_kmajor(&tmA, r.qB, P.Q, r.d_pad)) return kErrTensorMap;
-    if (!encode_bf16_kmajor(&tmB, r.R.refB, P.N, r.d_pad)) return kErrTensorMap;
-    if (!encode_norm_rows(&tmN, r.R.refN, P.N)) return kErrTensorMap;
-    TpArgs a;
-    a.N = P.N;
-    a.Q = P.Q;
-    a.kb_count = r.kb;
-    a.tile_base = 0;
-    a.tiles = r.sample;
-    a.n_splits = r.splits1;
-    a.thr = nullptr;
-    a.p1 = r.p1;
-    a.cand = r.cand;
-    a.count = r.count;
-    a.cmax = r.cmax;
-    a.status = P.status;
-    knn_tc_pair_scan_kernel<0><<<dim3(2 * r.qtiles, r.splits1), TP_THREADS, TP_SMEM, st>>>(
-        tmA, tmB, tmN, a);
-    if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    int rc = launch_scan<0>(r, st, r.kind, r.qB, r.qBlo, r.q8, P.Q, nullptr, r.cmax, 0,
+                            r.sample, r.splits1);
+    if (rc != kOk) return rc;
     if (P.timer) P.timer->mark(st, kPhaseTcPass1);
     // TP_LISTS lists (column ranges) per pair and split; resets the counts
-    tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(r.p1, TP_LISTS * r.splits1, P.Q, r.qn,
-                                                           r.R.rmax_bits, r.d_pad, r.thr,
-                                                           r.count);
+    const bool may_switch = P.adaptive && P.host_tmp && r.kind == kTcBf16 &&
+                            kind_fits(kTcBf16x3, r.d_pad, r.d_pad8) && r.R.refBlo && r.R.state;
+    tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
+        r.p1, TP_LISTS * r.splits1, P.Q, r.qn, r.R.rmax_bits,
+        r.kind == kTcFp8 ? 1.f / r.scale : 1.f, run_bound(r, r.kind), r.thr, r.thr_raw, r.count,
+        may_switch ? r.nwide : nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    if (may_switch) {
+        // most lists expected to overflow in BF16: the whole pass 2 runs in
+        // split BF16 instead (thresholds re-derived from the sample's values)
+        int wide = 0;
+        if ((rc = read_count(r.nwide, P.host_tmp, st, wide)) != kOk) return rc;
+        if (2 * wide > P.Q) {
+            if ((rc = ensure_ref_lo(r, st)) != kOk) return rc;
+            tc_pack_kernel<<<dim3((P.Q + 31) / 32, r.d_pad / 32), dim3(32, 8), 0, st>>>(
+                P.qry, P.Q, P.ldq, P.d, r.d_pad, r.R.center, -2.0f, r.qB, r.qBlo);
+            tc_rethreshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
+                r.thr_raw, P.Q, r.qn, r.R.rmax_bits, run_bound(r, kTcBf16x3), r.thr);
+            if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+            r.kind = kTcBf16x3;
+        }
+    }
     if (P.timer) P.timer->mark(st, kPhaseTcThreshold);
     return kOk;
 }
@@ -1353,7 +1868,7 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
 int tc_run_pass2(TcRun &r, int tile_begin, int tile_end, cudaStream_t st) {
     tile_end = std::min(tile_end, r.n_tiles2);
     if (tile_begin >= tile_end) return kOk;
-    const int rc = emit_scan(r, st, r.qB, r.P.Q, r.thr, r.cmax, tile_begin, tile_end);
+    const int rc = emit_scan(r, st, r.kind, r.P.Q, r.thr, r.cmax, tile_begin, tile_end);
     if (rc == kOk && r.P.timer) r.P.timer->mark(st, kPhaseTcPass2);
     return rc;
 }
@@ -1375,20 +1890,22 @@ int tc_run_rerank_piece(TcRun &r, cudaStream_t st) {
         r.done = done;
         r.pieces = true;
     }
-    const int kcap = P.k <= 32 ? 32 : (P.k <= 64 ? 64 : 128);
+    const int kcap = P.k <= 32 ? 32 : (P.k <= 64 ? 64 : (P.k <= 128 ? 128 : 256));
     const size_t smem = (size_t)r.d_pad * 4 + (size_t)TC_RR_NBUF * TC_RR_BUF * 4 +
-                        (size_t)(kcap + EX_CB) * 8;   // < 48 KB for d_pad <= 256
+                        (size_t)(kcap + EX_CB) * 8;
+    if (smem > kRerankSmem) return kErrUnsupported;
     auto go = [&](auto kern) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kRerankSmem) != cudaSuccess)
+            return (int)kErrLaunch;
         kern<<<P.Q, 32, smem, st>>>(r.R.refT, P.d, r.d_pad, P.qry, P.ldq, r.cand, r.count, r.cmax,
                                     P.k, r.run_keys, r.done);
+        return cudaGetLastError() == cudaSuccess ? (int)kOk : (int)kErrLaunch;
     };
-    if (kcap == 32)
-        go(tc_rerank_piece_kernel<32>);
-    else if (kcap == 64)
-        go(tc_rerank_piece_kernel<64>);
-    else
-        go(tc_rerank_piece_kernel<128>);
-    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
+    if (kcap == 32) return go(tc_rerank_piece_kernel<32>);
+    if (kcap == 64) return go(tc_rerank_piece_kernel<64>);
+    if (kcap == 128) return go(tc_rerank_piece_kernel<128>);
+    return go(tc_rerank_piece_kernel<256>);
 }
 
 int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
@@ -1397,45 +1914,62 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     int *host_tmp = host_stats + 2;
     host_stats[0] = host_stats[1] = 0;
     host_stats[4] = host_stats[5] = 0;
+    host_stats[6] = r.kind;
+    host_stats[7] = -1;
     int rc = kOk;
     if (r.pieces) {
         // every candidate was re-ranked piece by piece: certify
-        if (cudaMemsetAsync(r.nfail, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
+        if (cudaMemsetAsync(r.nfail, 0, 2 * sizeof(int), st) != cudaSuccess) return kErrCuda;
+        RrBounds rb;
+        rb.cur = run_bound(r, r.kind);
+        rb.a_scale = 1.f;
         constexpr int W = 4;
         tc_certify_pieces_kernel<<<(P.Q + W - 1) / W, W * 32, 0, st>>>(
-            r.count, r.cmax, r.qn, r.R.rmax_bits, r.thr, r.run_keys, P.Q, P.k, r.d_pad,
-            P.out_dist, P.out_idx, P.ld_out, r.fail, r.nfail, r.retry, r.cand_total);
+            r.count, r.cmax, r.qn, r.R.rmax_bits, r.thr, r.thr_raw, rb, r.run_keys, P.Q, P.k,
+            r.d_pad, P.out_dist, P.out_idx, P.ld_out, r.fail, r.nfail, r.retry, r.retry_f,
+            r.cand_total);
         if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     } else {
-        rc = rerank(r, st, P.Q, r.cmax, P.qry, P.ldq, r.qn, r.thr, P.out_dist, P.out_idx,
-                    P.ld_out, r.fail, false);
+        rc = rerank(r, st, r.kind, P.Q, r.cmax, P.qry, P.ldq, r.qn, r.thr, r.thr_raw, P.out_dist,
+                    P.out_idx, P.ld_out, r.fail, false);
     }
     if (rc != kOk) return rc;
     if (tm) tm->mark(st, kPhaseTcRerank);
-    int nf = 0;
     if (cudaMemcpyAsync(host_stats + 4, r.cand_total, sizeof(unsigned long long),
                         cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return kErrCuda;
-    if ((rc = read_count(r.nfail, host_tmp, st, nf)) != kOk) return rc;
+    int nf = 0;
+    if ((rc = read_count(r.nfail, host_tmp, st, nf, 2)) != kOk) return rc;
+    const int n_over = host_tmp[1];
     host_stats[0] = nf;
     if (nf == 0) return kOk;
 
     // second chance: the uncertified queries, compacted, scanned again with
-    // thresholds that certify (list overflows excepted)
+    // thresholds that certify (list overflows excepted).  Kind: split BF16
+    // when most failures are overflowing BF16 lists (BF16 too coarse for
+    // this data), BF16 after an FP8 scan, else the first scan's kind.
+    const bool lo_ok = kind_fits(kTcBf16x3, r.d_pad, r.d_pad8) && r.R.refBlo && r.R.state;
+    int kind2 = r.kind == kTcFp8 ? kTcBf16 : r.kind;
+    if (kind2 == kTcBf16 && r.kind == kTcBf16 && lo_ok && 2 * n_over > nf) kind2 = kTcBf16x3;
+    host_stats[7] = kind2;
+    if (kind2 == kTcBf16x3 && (rc = ensure_ref_lo(r, st)) != kOk) return rc;
     gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, r.fail,
                                                                        nf, r.qsub, r.ldf);
     tc_norms_kernel<<<(nf + 255) / 256, 256, 0, st>>>(r.qsub, nf, r.ldf, P.d, r.R.center, r.qn,
                                                       nullptr);
     tc_pack_kernel<<<dim3((nf + 31) / 32, r.d_pad / 32), dim3(32, 8), 0, st>>>(
-        r.qsub, nf, r.ldf, P.d, r.d_pad, r.R.center, -2.0f, r.qB);
-    tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(r.fail, nf, r.retry, r.thr, r.count);
+        r.qsub, nf, r.ldf, P.d, r.d_pad, r.R.center, -2.0f, r.qB,
+        kind2 == kTcBf16x3 ? r.qBlo : nullptr);
+    tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(
+        r.fail, nf, r.retry, r.retry_f, r.qn, r.R.rmax_bits, run_bound(r, kind2), r.thr, r.count);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     // the compacted queries share the whole list buffer (Q * cmax entries)
     const int cmax2 = (int)std::min<long long>(
         kTcCmaxRetry, std::max<long long>(r.cmax, (long long)P.Q * r.cmax / nf));
-    if ((rc = emit_scan(r, st, r.qB, nf, r.thr, cmax2, 0, r.n_tiles2)) != kOk) return rc;
+    if ((rc = emit_scan(r, st, kind2, nf, r.thr, cmax2, 0, r.n_tiles2)) != kOk) return rc;
     if (tm) tm->mark(st, kPhaseTcRetryScan);
-    rc = rerank(r, st, nf, cmax2, r.qsub, r.ldf, r.qn, r.thr, r.sd, r.si, r.ldf, r.fail2, true);
+    rc = rerank(r, st, kind2, nf, cmax2, r.qsub, r.ldf, r.qn, r.thr, nullptr, r.sd, r.si, r.ldf,
+                r.fail2, true);
     if (rc != kOk) return rc;
     if (tm) tm->mark(st, kPhaseTcRetryRerank);
     int nf2 = 0;
@@ -1444,7 +1978,7 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     if (nf2 > 0) {
         // still uncertified (list overflow): the exact kernel recomputes the
         // compacted batch
-        const long long per_split = (long long)nf * P.k * 8;
+        const long long per_split = (long long)nf * std::min(P.k, 256) * 8;
         const int splits = (int)std::max<long long>(
             1, std::min<long long>(exact_plan_splits(P.N, nf, P.d, P.k, P.num_sms),
                                    (long long)(r.xcap / per_split)));
@@ -1475,9 +2009,25 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     return kOk;
 }
 
+int tc_prepare_extras(const TcRefView &v, int N, int d, cudaStream_t st, int *host_tmp) {
+    TcRun r;
+    r.P = TcProblem{};
+    r.P.N = N;
+    r.P.d = d;
+    r.R = v;
+    r.d_pad = (d + 63) / 64 * 64;
+    r.d_pad8 = (d + 127) / 128 * 128;
+    int rc = v.refBlo ? ensure_ref_lo(r, st) : kOk;
+    if (rc == kOk && v.ref8) rc = ensure_ref_f8(r, st, reinterpret_cast<unsigned *>(host_tmp));
+    if (rc == kOk && cudaStreamSynchronize(st) != cudaSuccess) rc = kErrCuda;
+    return rc;
+}
+
 int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_stats) {
     TcRun r;
-    int rc = tc_run_begin(P, R, st, r);
+    TcProblem p = P;
+    if (!p.host_tmp) p.host_tmp = host_stats + 2;
+    int rc = tc_run_begin(p, R, st, r);
     if (rc == kOk) rc = tc_run_pass1(r, st);
     if (rc == kOk) rc = tc_run_pass2(r, 0, r.n_tiles2, st);
     if (rc == kOk) rc = tc_run_finish(r, st, host_stats);

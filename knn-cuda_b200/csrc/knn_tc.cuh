@@ -51,6 +51,11 @@ constexpr uint32_t umma_idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
            ((uint32_t)(M >> 4) << 24);
 }
+// Instruction descriptor, kind::f8f6f4: D = F32, A = B = E4M3 (format 0 in
+// bits 7-9 and 10-12), both K-major, N >> 3 in [17,23), M >> 4 in [24,29).
+constexpr uint32_t umma_idesc_e4m3(int M, int N) {
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
 
 // ---------------------------------------------------------------------------
 // CTA pairs (cluster of 2, cta_group::2): one MMA spans both CTAs' tensor
@@ -113,6 +118,17 @@ KNN_DI void umma_bf16_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, ui
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+// The same MMA on FP8 operands (kind::f8f6f4; K = 32 per instruction, so a
+// K step is again 32 bytes of each operand row).
+KNN_DI void umma_f8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
