@@ -311,7 +311,8 @@ def run_ours(args, D: Dist):
     warm = max(3, args.warmup)
     tiers = {}
     outs = {}
-    for name, method in (("exact_fp32", "global"), ("bf16_rerank", "cublas")):
+    tier_methods = [("exact_fp32", "global"), ("bf16_rerank", "cublas"), ("fp8_rerank", "fp8")]
+    for name, method in tier_methods:
         dist_d = torch.empty((k, qn), dtype=torch.float32, device=dev)
         idx_d = torch.empty((k, qn), dtype=torch.int32, device=dev)
 
@@ -326,24 +327,43 @@ def run_ours(args, D: Dist):
         outs[name] = (dist_d, idx_d)
         tiers[name] = {"value": D.world * qn / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
                        "phase_ms": phases, "uncertified_queries_per_step": fb}
+        if method != "global":
+            first, second = knncuda.last_tc_kinds()
+            tiers[name]["scan_kinds"] = {"pass2": first, "second_scan": second}
         if clk is not None:
             tiers[name]["clocks"] = clk
 
     # identical answers, and recall / error against FP64 on sampled queries
-    same = bool(torch.equal(outs["exact_fp32"][0], outs["bf16_rerank"][0]) and
-                torch.equal(outs["exact_fp32"][1], outs["bf16_rerank"][1]))
     sample = list(range(0, qn, max(1, qn // 32)))[:32]
-    recall, relerr = fp64_recall(torch, ref_d, qry_d, outs["bf16_rerank"][1],
-                                 outs["bf16_rerank"][0], k, sample)
-    tiers["bf16_rerank"].update(identical_to_exact=same, recall_at_k_fp64=recall,
-                                max_rel_dist_err_fp64=relerr,
-                                fp64_sample_queries=len(sample))
+    for name, _ in tier_methods:
+        same = bool(torch.equal(outs["exact_fp32"][0], outs[name][0]) and
+                    torch.equal(outs["exact_fp32"][1], outs[name][1]))
+        recall, relerr = fp64_recall(torch, ref_d, qry_d, outs[name][1], outs[name][0], k,
+                                     sample)
+        tiers[name].update(identical_to_exact=same, recall_at_k_fp64=recall,
+                           max_rel_dist_err_fp64=relerr, fp64_sample_queries=len(sample))
+    tiers["fp8_rerank"]["vs_bf16_rerank"] = (tiers["fp8_rerank"]["value"] /
+                                             tiers["bf16_rerank"]["value"])
 
     # end to end through the drop-in host entry points (pinned buffers)
     ref_np, qry_np = ref_h.numpy(), qry_h.numpy()
     out_d = torch.empty((k, qn), dtype=torch.float32).pin_memory().numpy()
     out_i = torch.empty((k, qn), dtype=torch.int32).pin_memory().numpy()
     e2e = {}
+    # the reference's harness passes malloc'd (pageable) buffers
+    # (code/test.cpp:314-317): knn_cublas from pageable memory
+    out_pd = np.empty((k, qn), np.float32)
+    out_pi = np.empty((k, qn), np.int32)
+    ref_pg, qry_pg = np.array(ref_np), np.array(qry_np)
+    knncuda.knn_cublas(ref_pg, N, qry_pg, qn, dim, k, out_pd, out_pi)
+    D.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        if not knncuda.knn_cublas(ref_pg, N, qry_pg, qn, dim, k, out_pd, out_pi):
+            raise RuntimeError("knn_cublas (pageable) failed")
+    e2e_pageable = D.max((time.perf_counter() - t0) / args.e2e_steps)
+    if not np.array_equal(out_pi, outs["exact_fp32"][1].cpu().numpy()):
+        raise RuntimeError("pageable knn_cublas disagrees with the device path")
     for name, fn in (("exact_fp32", knncuda.knn_cuda_global),
                      ("bf16_rerank", knncuda.knn_cublas)):
         fn(ref_np, N, qry_np, qn, dim, k, out_d, out_i)   # warm (workspace growth)
@@ -406,6 +426,10 @@ def run_ours(args, D: Dist):
         "clocks": head.get("clocks"),
         "tiers": tiers,
         "speedup_bf16_vs_exact": head["value"] / ex["value"],
+        "e2e_pageable": {"value": D.world * qn / e2e_pageable, "unit": UNIT,
+                         "ms_per_step": e2e_pageable * 1e3,
+                         "api": "knn_cublas (drop-in C-ABI, pageable numpy buffers as in "
+                                "code/test.cpp)"},
     }
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
         rates, threads, desc, kind, qs = cpu_sample_rate(ref, query, k, args.cpu_seconds)
@@ -575,6 +599,26 @@ def run_serving(args, D: Dist):
                        "qps": open_loop["qps"], "p50_ms": open_loop["p50_ms"],
                        "p99_ms": open_loop["p99_ms"], "requests": open_loop["requests"],
                        "batches": open_loop["batches"]}
+    # exactness of served results: 16 requests against an FP64 brute force
+    # on the GPU (first and last query of each)
+    ref_d = torch.from_numpy(ref).to(torch.device(f"cuda:{D.local_rank}"))
+    srv = knncuda.Server(rs, slots=3, memory_budget=16 << 30, max_batch_queries=8192,
+                         method="cublas")
+    chk = [reqs[j] for j in range(0, 16 * 7, 7)]
+    tickets = [srv.submit(q, k) for q, k in chk]
+    hits, total, worst = 0.0, 0, 0.0
+    for (q, k), t in zip(chk, tickets):
+        d, i, _ = srv.wait(t)
+        qd = torch.from_numpy(q).to(ref_d.device)
+        sample = sorted({0, q.shape[1] - 1})
+        rec, err = fp64_recall(torch, ref_d, qd, torch.from_numpy(i).to(ref_d.device),
+                               torch.from_numpy(d).to(ref_d.device), k, sample)
+        hits += rec * len(sample)
+        total += len(sample)
+        worst = max(worst, err)
+    srv.close()
+    out["cublas"].update(recall_at_k_fp64=hits / total, max_rel_dist_err_fp64=worst,
+                         fp64_sample_queries=total)
     line = {"metric": "serving queries/s and p50/p99 latency (resident 2M x 128, k in {10,50,100})",
             "value": out["cublas"]["qps"], "unit": "queries/s", "n_gpus": D.world,
             "higher_is_better": True, "impl": "ours", "mode": "serving",
@@ -631,23 +675,39 @@ def run_batched(args, D: Dist):
     ms_single = timed(per_problem, args.steps)
     ref_out = [(d.clone(), i.clone()) for d, i in outs]
     arr = knncuda.problems_from([(r, q, k, d, i) for (r, q, k), (d, i) in zip(probs, outs)])
-    best, tuned_ms = knncuda.batched_autotune(arr)
-    plan = knncuda.BatchedPlan(arr, item_stages=best)
+    # the work-item-size tuner alone as the baseline configuration
+    best_stages, _ = knncuda.batched_autotune(arr)
+    plan0 = knncuda.BatchedPlan(arr, item_stages=best_stages)
+    ms_items_only = timed(plan0.run, args.steps)
+    plan0.close()
+    best, tuned_ms = knncuda.batched_autotune_config(arr)
+    plan = knncuda.BatchedPlan(arr, config=best)
     ms_batched = timed(plan.run, args.steps)
     plan.capture_graph()
     ms_graph = timed(plan.replay, args.steps)
     same = all(torch.equal(d, a) and torch.equal(i, b) for (d, i), (a, b) in zip(outs, ref_out))
+    # exactness against FP64: first and last query of every 8th problem
+    hits, total, worst = 0.0, 0, 0.0
+    for (ref, qry, k), (d, i) in list(zip(probs, outs))[::8]:
+        sample = sorted({0, qry.shape[1] - 1})
+        rec, err = fp64_recall(torch, ref, qry, i, d, k, sample)
+        hits += rec * len(sample)
+        total += len(sample)
+        worst = max(worst, err)
     if plan.status() != 0:
         raise RuntimeError("device status error")
     line = {"metric": "batched k-NN: 512 uneven problems per step",
             "value": 1e3 / ms_graph, "unit": "steps/s (512 problems each)", "n_gpus": D.world,
             "higher_is_better": True, "impl": "ours", "mode": "batched",
             "config": {"workload": "batched512", "problems": len(shapes),
-                       "pairs_per_step": pairs, "autotuned_item_stages": best,
+                       "pairs_per_step": pairs, "autotuned": plan.config(),
                        "work_items": plan.items()},
             "ms_per_problem_launches": ms_single, "ms_persistent_launch": ms_batched,
+            "ms_item_size_tuned_only": ms_items_only,
+            "item_size_tuned_only": {"item_stages": best_stages},
             "ms_graph_replay": ms_graph, "speedup_vs_per_problem": ms_single / ms_graph,
-            "identical_to_per_problem": same}
+            "identical_to_per_problem": same, "recall_at_k_fp64": hits / total,
+            "max_rel_dist_err_fp64": worst, "fp64_sample_queries": total}
     plan.close()
     if D.rank == 0:
         print(json.dumps(line), flush=True)

@@ -31,7 +31,10 @@ LIB_PATH = os.path.join(HERE, "libknnb200.so")
 METHOD_GLOBAL = 0
 METHOD_TEXTURE = 1
 METHOD_CUBLAS = 2
-METHODS = {"global": METHOD_GLOBAL, "texture": METHOD_TEXTURE, "cublas": METHOD_CUBLAS}
+METHOD_FP8 = 3
+METHODS = {"global": METHOD_GLOBAL, "texture": METHOD_TEXTURE, "cublas": METHOD_CUBLAS,
+           "fp8": METHOD_FP8}
+TC_KINDS = {-1: None, 0: "bf16", 1: "bf16x3", 2: "fp8"}
 
 _FP = ctypes.POINTER(ctypes.c_float)
 _IP = ctypes.POINTER(ctypes.c_int)
@@ -52,8 +55,20 @@ C_SYMBOLS = (
     "knnb200_batched_items", "knnb200_batched_plan_destroy", "knnb200_batched_graph_create",
     "knnb200_graph_launch", "knnb200_graph_destroy", "knnb200_batched_autotune",
     "knnb200_set_bound_check", "knnb200_last_bound_check", "knnb200_set_memory_cap",
-    "knnb200_last_query_chunks", "knnb200_call_bytes",
+    "knnb200_last_query_chunks", "knnb200_call_bytes", "knnb200_last_tc_kinds",
+    "knnb200_batched_plan_create_config", "knnb200_batched_plan_config",
+    "knnb200_batched_autotune_config",
 )
+
+
+class BatchedConfig(ctypes.Structure):
+    """Mirror of knnb200_batched_config (include/knn_b200.h)."""
+    _fields_ = [("item_stages", ctypes.c_int), ("queries_per_warp", ctypes.c_int),
+                ("lowdim_kernel", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {"item_stages": self.item_stages, "queries_per_warp": self.queries_per_warp,
+                "lowdim_kernel": self.lowdim_kernel}
 
 
 class Problem(ctypes.Structure):
@@ -167,8 +182,19 @@ def lib():
         L.knnb200_set_memory_cap.argtypes = [ctypes.c_size_t]
         L.knnb200_last_query_chunks.restype = ctypes.c_int
         L.knnb200_last_query_chunks.argtypes = []
+        L.knnb200_last_tc_kinds.restype = None
+        L.knnb200_last_tc_kinds.argtypes = [_IP, _IP]
         L.knnb200_call_bytes.restype = ctypes.c_size_t
         L.knnb200_call_bytes.argtypes = [ctypes.c_int] * 6
+        CP = ctypes.POINTER(BatchedConfig)
+        L.knnb200_batched_plan_create_config.restype = ctypes.c_int
+        L.knnb200_batched_plan_create_config.argtypes = [PP, ctypes.c_int, CP,
+                                                         ctypes.POINTER(vp)]
+        L.knnb200_batched_plan_config.restype = ctypes.c_int
+        L.knnb200_batched_plan_config.argtypes = [vp, CP, _IP]
+        L.knnb200_batched_autotune_config.restype = ctypes.c_int
+        L.knnb200_batched_autotune_config.argtypes = [PP, ctypes.c_int, vp, CP,
+                                                      ctypes.POINTER(ctypes.c_float)]
         L.knnb200_version.restype = ctypes.c_char_p
         L.knnb200_version.argtypes = []
         _lib = L
@@ -387,19 +413,34 @@ def problems_from(tensors):
 
 
 class BatchedPlan:
-    """Many independent exact k-NN problems in one persistent launch."""
+    """Many independent exact k-NN problems in one persistent launch.
 
-    def __init__(self, problems, item_stages: int = 0):
+    ``config`` (a BatchedConfig, e.g. from batched_autotune_config) overrides
+    ``item_stages``."""
+
+    def __init__(self, problems, item_stages: int = 0, config=None):
         self._arr = problems
         self._h = ctypes.c_void_p()
-        rc = lib().knnb200_batched_plan_create(problems, len(problems), item_stages,
-                                               ctypes.byref(self._h))
+        if config is not None:
+            rc = lib().knnb200_batched_plan_create_config(problems, len(problems),
+                                                          ctypes.byref(config),
+                                                          ctypes.byref(self._h))
+        else:
+            rc = lib().knnb200_batched_plan_create(problems, len(problems), item_stages,
+                                                   ctypes.byref(self._h))
         if rc != 0:
             raise RuntimeError(f"knnb200_batched_plan_create failed: {status_string(rc)}")
         self._graph = ctypes.c_void_p()
 
     def items(self) -> int:
         return lib().knnb200_batched_items(self._h)
+
+    def config(self) -> dict:
+        """The plan's configuration and how many problems it sends to the
+        low-dimension kernel."""
+        c, n = BatchedConfig(), ctypes.c_int(0)
+        lib().knnb200_batched_plan_config(self._h, ctypes.byref(c), ctypes.byref(n))
+        return dict(c.as_dict(), lowdim_problems=n.value)
 
     def run(self, stream=None):
         import torch
@@ -455,6 +496,21 @@ def batched_autotune(problems, stream=None):
     if rc != 0:
         raise RuntimeError(f"knnb200_batched_autotune failed: {status_string(rc)}")
     return best.value, ms.value
+
+
+def batched_autotune_config(problems, stream=None):
+    """(best BatchedConfig, ms per run) over work-item size, tile shape and
+    low-d routing."""
+    import torch
+
+    stream = stream or torch.cuda.current_stream()
+    best, ms = BatchedConfig(), ctypes.c_float(0)
+    rc = lib().knnb200_batched_autotune_config(problems, len(problems),
+                                               ctypes.c_void_p(stream.cuda_stream),
+                                               ctypes.byref(best), ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"knnb200_batched_autotune_config failed: {status_string(rc)}")
+    return best, ms.value
 
 
 def sync_status(stream=None) -> int:
@@ -542,6 +598,14 @@ def call_bytes(ref_nb, query_nb, dim, k, method="global", host=True) -> int:
 def last_query_chunks() -> int:
     """Query chunks the last host or device call ran in."""
     return lib().knnb200_last_query_chunks()
+
+
+def last_tc_kinds() -> tuple:
+    """(first scan kind, second scan kind) of the last tensor-path call, as
+    names: "bf16", "bf16x3" (split BF16), "fp8" or None."""
+    a, b = ctypes.c_int(0), ctypes.c_int(0)
+    lib().knnb200_last_tc_kinds(ctypes.byref(a), ctypes.byref(b))
+    return TC_KINDS.get(a.value), TC_KINDS.get(b.value)
 
 
 def last_fallback_counts() -> tuple:

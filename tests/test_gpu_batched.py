@@ -78,3 +78,45 @@ def test_batched_graph_replay_and_autotune(knncuda, gpu):
         for (d, i), (ed, ei) in zip(outs, exp):
             assert torch.equal(d, ed) and torch.equal(i, ei)
     plan.close()
+
+
+@pytest.mark.parametrize("qpw,lowdim", [(2, 0), (2, 1), (4, 1)])
+def test_batched_configurations_equal_per_problem(knncuda, gpu, qpw, lowdim):
+    """Both tile shapes, with and without routing d <= 4 / k <= 16 problems
+    to the low-dimension kernel, give exactly the per-problem answers, also
+    replayed from a captured graph."""
+    import torch
+
+    probs = _problems(torch, gpu, 31 + qpw + lowdim, 80, kmax=40)
+    exp = _expected(knncuda, torch, probs)
+    outs = _outputs(torch, gpu, probs)
+    arr = knncuda.problems_from([(r, q, k, d, i) for (r, q, k), (d, i) in zip(probs, outs)])
+    cfg = knncuda.BatchedConfig(128, qpw, lowdim)
+    plan = knncuda.BatchedPlan(arr, config=cfg)
+    info = plan.config()
+    assert info["queries_per_warp"] == qpw
+    n_low = sum(1 for r, q, k in probs if r.shape[0] <= 4 and k <= 16)
+    assert info["lowdim_problems"] == (n_low if lowdim else 0)
+    plan.capture_graph()
+    plan.replay()
+    assert plan.status() == 0
+    for (d, i), (ed, ei) in zip(outs, exp):
+        assert torch.equal(d, ed) and torch.equal(i, ei)
+    plan.close()
+
+
+def test_batched_autotune_config(knncuda, gpu):
+    import torch
+
+    probs = _problems(torch, gpu, 41, 48)
+    exp = _expected(knncuda, torch, probs)
+    outs = _outputs(torch, gpu, probs)
+    arr = knncuda.problems_from([(r, q, k, d, i) for (r, q, k), (d, i) in zip(probs, outs)])
+    best, ms = knncuda.batched_autotune_config(arr)
+    assert best.queries_per_warp in (2, 4) and best.lowdim_kernel in (0, 1) and ms > 0
+    plan = knncuda.BatchedPlan(arr, config=best)
+    plan.run()
+    assert plan.status() == 0
+    for (d, i), (ed, ei) in zip(outs, exp):
+        assert torch.equal(d, ed) and torch.equal(i, ei)
+    plan.close()

@@ -200,3 +200,89 @@ def test_cublas_host_streamed_from_pinned_memory(knncuda, gpu, n, dim, k):
         assert knncuda.knn_cublas(ref, n, query, q, dim, k, d1, i1)
         assert np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
         assert np.array_equal(i0, i1)
+
+
+HIGH_DIM = [
+    # (seed, ref_nb, query_nb, dim, k): d > 256 (A streamed beside B above
+    # d = 512) and k in (128, 256]
+    (61, 40000, 300, 384, 200),
+    (62, 36000, 260, 512, 200),
+    (63, 33000, 200, 1024, 200),
+    (64, 50000, 300, 130, 256),
+    (65, 40000, 513, 640, 64),
+]
+
+
+@pytest.mark.parametrize("case", HIGH_DIM, ids=[f"n{c[1]}q{c[2]}d{c[3]}k{c[4]}" for c in HIGH_DIM])
+def test_tensor_path_high_dim_and_large_k(knncuda, gpu, case):
+    """knn_cublas on d up to 1024 and k up to 256 runs the tcgen05 scan and
+    returns exactly knn_cuda_global's answer (the reference's knn_cublas
+    has no d limit, code/knncuda.cu:612-832)."""
+    seed, n, q, dim, k = case
+    ref, query = _uniform(seed, dim, n, q)
+    dg, ig = knncuda.knn(ref, query, k, "global")
+    dc, ic = knncuda.knn(ref, query, k, "cublas")
+    first, _ = knncuda.last_tc_kinds()
+    assert first in ("bf16", "bf16x3"), first
+    assert knncuda.last_tc_stats()["candidates"] > 0
+    assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
+    assert np.array_equal(ic, ig)
+
+
+FP8_CASES = [
+    (71, 65536, 300, 64, 16),
+    (72, 65536, 513, 128, 100),
+    (73, 40000, 257, 256, 128),
+    (74, 50000, 200, 200, 50),       # d not a multiple of 128: zero-padded K block
+    (75, 33000, 150, 1024, 32),
+]
+
+
+@pytest.mark.parametrize("case", FP8_CASES, ids=[f"n{c[1]}q{c[2]}d{c[3]}k{c[4]}" for c in FP8_CASES])
+def test_fp8_scan_equals_global_bitwise(knncuda, gpu, case):
+    """The FP8 (e4m3, power-of-two scaled) candidate scan, certified against
+    its own error bound and re-ranked exactly, returns the exact kernel's
+    answer bit for bit."""
+    import torch
+
+    seed, n, q, dim, k = case
+    ref, query = _uniform(seed, dim, n, q)
+    r, x = torch.from_numpy(ref).to(gpu), torch.from_numpy(query).to(gpu)
+    dg, ig = knncuda.knn_device(r, x, k, "global")
+    df, i8 = knncuda.knn_device(r, x, k, "fp8")
+    assert knncuda.sync_status() == 0
+    first, second = knncuda.last_tc_kinds()
+    assert first == "fp8", first
+    assert torch.equal(df, dg) and torch.equal(i8, ig)
+
+
+def test_fp8_scan_on_headline_mixture(knncuda, gpu):
+    import torch
+    import workloads
+
+    w = workloads.WORKLOADS["mixture256"]
+    ref, query = workloads.generate(w, query_nb=1024)
+    r, x = torch.from_numpy(ref).to(gpu), torch.from_numpy(query).to(gpu)
+    dg, ig = knncuda.knn_device(r, x, w.k, "global")
+    df, i8 = knncuda.knn_device(r, x, w.k, "fp8")
+    assert knncuda.sync_status() == 0
+    assert knncuda.last_tc_kinds()[0] == "fp8"
+    assert torch.equal(df, dg) and torch.equal(i8, ig)
+
+
+def test_split_bf16_when_bf16_would_overflow(knncuda, gpu):
+    """mixture128's BF16 error slack exceeds its in-cluster spread: the
+    threshold pass predicts overflowing lists and pass 2 runs in split BF16
+    (hi + lo parts), so the exact kernel is not needed."""
+    import workloads
+
+    w = workloads.WORKLOADS["mixture128"]
+    ref, query = workloads.generate(w, ref_nb=262144, query_nb=2000)
+    dg, ig = knncuda.knn(ref, query, w.k, "global")
+    dc, ic = knncuda.knn(ref, query, w.k, "cublas")
+    first, second = knncuda.last_tc_kinds()
+    _, exact = knncuda.last_fallback_counts()
+    assert first == "bf16x3", (first, second)
+    assert exact == 0
+    assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
+    assert np.array_equal(ic, ig)
