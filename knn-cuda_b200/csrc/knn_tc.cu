@@ -877,10 +877,13 @@ __global__ void tc_pack_f8_kernel(const float *__restrict__ x, int n, long long 
 // three times the spread of its KS sample values is expected to overflow
 // its candidate list (about KS x stride points lie below T, and the band
 // [T, T + E] adds E / (T - L_0) times as many): n_wide counts them.
+// The prediction uses the `probe` bound: the BF16 one, whether the scan
+// itself is BF16 (switch its pass 2 to split BF16) or FP8 (choose the kind
+// of the second scan).
 __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
                                     const float *__restrict__ qn,
                                     const unsigned *__restrict__ rmax_bits, float inv_scale,
-                                    TcBound bound, float *__restrict__ thr,
+                                    TcBound bound, TcBound probe, float *__restrict__ thr,
                                     float *__restrict__ thr_raw, int *__restrict__ count,
                                     int *__restrict__ n_wide) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -904,7 +907,9 @@ __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
     thr[q] = T + E;
     thr_raw[q] = T;
     count[q] = 0;
-    if (n_wide && E > 3.f * (T - L[0] * inv_scale)) atomicAdd(n_wide, 1);
+    if (n_wide && tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T, probe) >
+                      3.f * (T - L[0] * inv_scale))
+        atomicAdd(n_wide, 1);
 }
 
 // Thresholds of a scan of another kind from the raw sample thresholds:
@@ -1829,12 +1834,14 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
     if (rc != kOk) return rc;
     if (P.timer) P.timer->mark(st, kPhaseTcPass1);
     // TP_LISTS lists (column ranges) per pair and split; resets the counts
-    const bool may_switch = P.adaptive && P.host_tmp && r.kind == kTcBf16 &&
-                            kind_fits(kTcBf16x3, r.d_pad, r.d_pad8) && r.R.refBlo && r.R.state;
+    const bool lo_ok = kind_fits(kTcBf16x3, r.d_pad, r.d_pad8) && r.R.refBlo && r.R.state;
+    const bool may_switch = P.adaptive && P.host_tmp && r.kind == kTcBf16 && lo_ok;
+    // FP8: the same prediction for BF16 picks the second scan's kind
+    const bool probe_fp8 = r.kind == kTcFp8 && lo_ok;
     tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
         r.p1, TP_LISTS * r.splits1, P.Q, r.qn, r.R.rmax_bits,
-        r.kind == kTcFp8 ? 1.f / r.scale : 1.f, run_bound(r, r.kind), r.thr, r.thr_raw, r.count,
-        may_switch ? r.nwide : nullptr);
+        r.kind == kTcFp8 ? 1.f / r.scale : 1.f, run_bound(r, r.kind), run_bound(r, kTcBf16),
+        r.thr, r.thr_raw, r.count, (may_switch || probe_fp8) ? r.nwide : nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     if (may_switch) {
         // most lists expected to overflow in BF16: the whole pass 2 runs in
@@ -1936,10 +1943,17 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     // second chance: the uncertified queries, compacted, scanned again with
     // thresholds that certify (list overflows excepted).  Kind: split BF16
     // when most failures are overflowing BF16 lists (BF16 too coarse for
-    // this data), BF16 after an FP8 scan, else the first scan's kind.
+    // this data); after an FP8 scan, BF16 unless the threshold pass
+    // predicted BF16 lists to overflow for most queries; else the first
+    // scan's kind.
     const bool lo_ok = kind_fits(kTcBf16x3, r.d_pad, r.d_pad8) && r.R.refBlo && r.R.state;
-    int kind2 = r.kind == kTcFp8 ? kTcBf16 : r.kind;
-    if (kind2 == kTcBf16 && r.kind == kTcBf16 && lo_ok && 2 * n_over > nf) kind2 = kTcBf16x3;
+    int kind2 = r.kind;
+    if (r.kind == kTcBf16 && lo_ok && 2 * n_over > nf) kind2 = kTcBf16x3;
+    if (r.kind == kTcFp8) {
+        int wide = 0;
+        if (lo_ok && (rc = read_count(r.nwide, host_tmp, st, wide)) != kOk) return rc;
+        kind2 = (lo_ok && 2 * wide > P.Q) ? kTcBf16x3 : kTcBf16;
+    }
     host_stats[7] = kind2;
     if (kind2 == kTcBf16x3 && (rc = ensure_ref_lo(r, st)) != kOk) return rc;
     gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, r.fail,
