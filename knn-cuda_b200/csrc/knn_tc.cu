@@ -957,29 +957,35 @@ KNN_DI void warp_bitonic_sort(unsigned long long *keys, int P, int lane) {
 // also absorbs the roundings of this bound) is re-ranked; the k-th exact
 // distance of that prefix is the k-th of all candidates.
 //
-// The prefix is handled 32 candidates at a time, one per lane
-// (rr_exact_distances: each lane streams its candidate's FP32 row into
-// registers and runs the FMA chain in increasing d -- the fused exact
-// kernel's arithmetic and order, so distances are identical).  The
-// (distance, index) keys are bitonic-sorted by the warp.  One warp per
-// block: the gather is latency-bound, and single-warp blocks let the SM hold
-// as many warps as registers and the keys' shared memory allow.
+// The prefix is handled 32 candidates at a time, one per lane: the warp
+// copies the 32 candidate rows of the FP32 point-major copy, TC_RR_DCH
+// dimensions at a time, into a padded shared tile with asynchronous 16-byte
+// copies (cp.async, several rows per instruction, coalesced), through a ring
+// of TC_RR_NBUF buffers so the next chunks are in flight while each lane
+// runs its candidate's FMA chain in increasing d -- the fused exact kernel's
+// arithmetic and order, so distances are identical.  The (distance, index)
+// keys are bitonic-sorted by the warp.  One warp per block: the gather is
+// latency-bound, and single-warp blocks let the SM hold as many warps as
+// its shared memory allows (about 14 at d = 256).
 //
-// An uncertified query is appended to fail_list with the base of a second
-// scan's threshold: when it had at least k candidates, their k-th exact
-// distance D_k bounds the true k-th from above, so every point of the true
-// top-k has a < D_k (1+g) + E - ||q||^2 and a second scan emitting below
+// An uncertified query is appended to fail_list and retry[q] receives a
+// threshold for a second scan: when it had at least k candidates, their k-th
+// exact distance D_k bounds the true k-th from above, so every point of the
+// true top-k has a < D_k (1+g) + E - ||q||^2 and a second scan emitting below
 // D_k (1+g) + 2.5 E - ||q||^2 passes the check; with fewer than k candidates
-// the threshold is widened by 8 E; an overflowing list gets a threshold for
-// a second scan with a longer list (final_pass = 0) or NaN (exact
+// the threshold is widened by 8 E; an overflowing list keeps its threshold
+// for a second scan with a longer list (final_pass = 0) or gets NaN (exact
 // kernel).
 constexpr int TC_RR_WARPS = 1;
-constexpr int TC_RR_DCH = 16;                 // dimensions per step (64 bytes of a row)
-constexpr int TC_RR_NBUF = 3;                 // register buffers per lane (ring)
+constexpr int TC_RR_DCH = 32;                 // dimensions per staged chunk
+constexpr int TC_RR_NBUF = 2;                 // staging buffers per warp (ring)
+// padded row (floats): 16-byte aligned, and 16-byte reads of one row per lane
+// fall in distinct bank groups for every 8 consecutive lanes
+constexpr int TC_RR_STRIDE = TC_RR_DCH + 4;
+constexpr int TC_RR_BUF = 32 * TC_RR_STRIDE;  // floats per staging buffer
 
-// shared memory of one re-rank warp: the query and the sort keys
 __host__ __device__ inline size_t tc_rr_warp_bytes(int d_pad, int cpow) {
-    return (size_t)d_pad * 4 + (size_t)cpow * 8;
+    return (size_t)d_pad * 4 + TC_RR_NBUF * TC_RR_BUF * 4 + (size_t)cpow * 8;
 }
 
 KNN_DI void cp_async16(void *smem_dst, const void *gmem_src) {
@@ -1029,14 +1035,11 @@ KNN_DI bool rr_reject_list(int c, int cmax, int k, int q, float qq, float r2, fl
 }
 // Exact FP32 distances of the candidates keys[0..n) (point index in the low
 // 32 bits), in place: keys[t] = (distance, index).  One warp, 32 candidates
-// at a time, one per lane: each lane reads its own candidate's row of the
-// FP32 point-major copy straight into registers, TC_RR_DCH dimensions (one
-// 64-byte piece of the row) per step, through TC_RR_NBUF rotating register
-// buffers, so the loads of the next NBUF - 1 steps are in flight while the
-// lane runs its candidate's FMA chain on the current one against the query
-// qv (d_pad floats in shared memory, broadcast reads) in increasing d.  No
-// shared-memory staging: the warp's footprint is the query and the keys, so
-// many more warps (and loads) fit per SM than with staged copies.
+// at a time, one per lane: the rows of the FP32 point-major copy are staged
+// TC_RR_DCH dimensions at a time through the TC_RR_NBUF buffers `rows`
+// (steps s = (group, chunk); the copies of steps s + 1 .. s + NBUF - 1
+// overlap step s), and each lane runs its candidate's FMA chain against the
+// query qv (d_pad floats) in increasing d.
 //
 // Bound check (STAT, a test-only instantiation): before a key is replaced,
 // its entry still holds the BF16-expansion value a of that candidate; the
@@ -1050,65 +1053,70 @@ struct BoundStat {
 
 template <bool STAT = false>
 KNN_DI void rr_exact_distances(unsigned long long *keys, int n, const float *__restrict__ refT,
-                               int d_pad, const float *qv, int lane,
+                               int d_pad, const float *qv, float *rows, int lane,
                                BoundStat bs = BoundStat{0.f, 0.f, 1.f, nullptr}) {
-    constexpr int V = TC_RR_DCH / 4;   // float4 per step
     const int nch = d_pad / TC_RR_DCH;
     const int total = ((n + 31) / 32) * nch;
-    float4 buf[TC_RR_NBUF][V];
+    constexpr int CPL = TC_RR_DCH / 4;   // 16-byte copies per row and chunk
+    constexpr int RPI = 32 / CPL;        // rows per copy instruction
+    auto issue = [&](int buf, int rr, int ch) {
+        float *dstb = rows + buf * TC_RR_BUF;
+#pragma unroll
+        for (int i = 0; i < 32 / RPI; ++i) {
+            const int row = RPI * i + lane / CPL;
+            const int r = __shfl_sync(0xffffffffu, rr, row);
+            if (r >= 0)
+                cp_async16(dstb + row * TC_RR_STRIDE + (lane % CPL) * 4,
+                           refT + (size_t)r * d_pad + ch + (lane % CPL) * 4);
+        }
+    };
     auto row_of = [&](int grp) {
         const int t = grp * 32 + lane;
         return t < n ? (int)(uint32_t)keys[t] : -1;
     };
-    auto load = [&](float4 (&dst)[V], int step) {
-        if (step >= total) return;
-        const int r = row_of(step / nch);
-        if (r < 0) return;
-        const float4 *src = reinterpret_cast<const float4 *>(
-            refT + (size_t)r * d_pad + (step % nch) * TC_RR_DCH);
 #pragma unroll
-        for (int v = 0; v < V; ++v) dst[v] = __ldg(src + v);
-    };
-#pragma unroll
-    for (int b = 0; b < TC_RR_NBUF - 1; ++b) load(buf[b], b);
+    for (int s = 0; s < TC_RR_NBUF - 1; ++s) {
+        if (s < total) issue(s, row_of(s / nch), (s % nch) * TC_RR_DCH);
+        cp_async_commit();
+    }
     float acc = 0.f;
     int r_cur = -1;
-    // steps in rounds of NBUF so that every buffer index is a constant
-    for (int s0 = 0; s0 < total; s0 += TC_RR_NBUF) {
+    for (int s = 0; s < total; ++s) {
+        const int g = s / nch, ch = s - g * nch;
+        if (ch == 0) r_cur = row_of(g);
+        const int s1 = s + TC_RR_NBUF - 1;
+        if (s1 < total) issue(s1 % TC_RR_NBUF, row_of(s1 / nch), (s1 % nch) * TC_RR_DCH);
+        cp_async_commit();
+        cp_async_wait_n<TC_RR_NBUF - 1>();   // step s's copies have landed
+        __syncwarp();
+        const float4 *myrow = reinterpret_cast<const float4 *>(
+            rows + (s % TC_RR_NBUF) * TC_RR_BUF + lane * TC_RR_STRIDE);
+        const float4 *qc = reinterpret_cast<const float4 *>(qv + ch * TC_RR_DCH);
 #pragma unroll
-        for (int b = 0; b < TC_RR_NBUF; ++b) {
-            const int s = s0 + b;
-            if (s >= total) break;
-            load(buf[(b + TC_RR_NBUF - 1) % TC_RR_NBUF], s + TC_RR_NBUF - 1);
-            const int g = s / nch, ch = s - g * nch;
-            if (ch == 0) r_cur = row_of(g);
-            const float4 *qc = reinterpret_cast<const float4 *>(qv + ch * TC_RR_DCH);
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                const float4 rv = buf[b][v], qq4 = qc[v];
-                float t0 = __fsub_rn(rv.x, qq4.x);
-                acc = __fmaf_rn(t0, t0, acc);
-                t0 = __fsub_rn(rv.y, qq4.y);
-                acc = __fmaf_rn(t0, t0, acc);
-                t0 = __fsub_rn(rv.z, qq4.z);
-                acc = __fmaf_rn(t0, t0, acc);
-                t0 = __fsub_rn(rv.w, qq4.w);
-                acc = __fmaf_rn(t0, t0, acc);
+        for (int j = 0; j < TC_RR_DCH / 4; ++j) {
+            const float4 rv = myrow[j], qq4 = qc[j];
+            float t0 = __fsub_rn(rv.x, qq4.x);
+            acc = __fmaf_rn(t0, t0, acc);
+            t0 = __fsub_rn(rv.y, qq4.y);
+            acc = __fmaf_rn(t0, t0, acc);
+            t0 = __fsub_rn(rv.z, qq4.z);
+            acc = __fmaf_rn(t0, t0, acc);
+            t0 = __fsub_rn(rv.w, qq4.w);
+            acc = __fmaf_rn(t0, t0, acc);
+        }
+        __syncwarp();   // this buffer is refilled NBUF - 1 steps later
+        if (ch == nch - 1) {
+            const int t = g * 32 + lane;
+            if (STAT && t < n) {
+                const float a = ord_float((uint32_t)(keys[t] >> 32)) * bs.a_scale;
+                const float ratio = fabsf(a + bs.qq - acc) / bs.e_q;
+                atomicMax(bs.stat, __float_as_uint(ratio));
+                atomicAdd(reinterpret_cast<unsigned long long *>(bs.stat + 2), 1ull);
             }
-            if (ch == nch - 1) {
-                const int t = g * 32 + lane;
-                if (STAT && t < n) {
-                    const float a = ord_float((uint32_t)(keys[t] >> 32)) * bs.a_scale;
-                    const float ratio = fabsf(a + bs.qq - acc) / bs.e_q;
-                    atomicMax(bs.stat, __float_as_uint(ratio));
-                    atomicAdd(reinterpret_cast<unsigned long long *>(bs.stat + 2), 1ull);
-                }
-                if (t < n) keys[t] = make_key(acc, (uint32_t)r_cur);
-                acc = 0.f;
-            }
+            if (t < n) keys[t] = make_key(acc, (uint32_t)r_cur);
+            acc = 0.f;
         }
     }
-    __syncwarp();
 }
 
 // Certification from a query's k smallest exact keys (sorted; keys[k - 1]
@@ -1157,7 +1165,8 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
     if (q >= Q) return;
     unsigned char *mine = rsm + (size_t)warp * tc_rr_warp_bytes(d_pad, cpow);
     float *qv = reinterpret_cast<float *>(mine);
-    unsigned long long *keys = reinterpret_cast<unsigned long long *>(qv + d_pad);
+    float *rows = qv + d_pad;   // two staging buffers
+    unsigned long long *keys = reinterpret_cast<unsigned long long *>(rows + TC_RR_NBUF * TC_RR_BUF);
 
     const int c = count[q];
     if (lane == 0) atomicAdd(cand_total, (unsigned long long)c);
@@ -1191,7 +1200,7 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
         }
         n_s = max(cnt, k);   // keys are sorted, so the kept ones are a prefix
     }
-    rr_exact_distances<STAT>(keys, n_s, refT, d_pad, qv, lane,
+    rr_exact_distances<STAT>(keys, n_s, refT, d_pad, qv, rows, lane,
                              BoundStat{qq, tc_error_bound(qq, r2, T, rb.cur), rb.a_scale,
                                        bound_stat});
     int P2 = 32;
@@ -1227,7 +1236,8 @@ __global__ void __launch_bounds__(32)
     const int s0 = done[q];
     if (s0 >= c) return;
     float *qv = reinterpret_cast<float *>(rsm);
-    unsigned long long *L = reinterpret_cast<unsigned long long *>(qv + d_pad);
+    float *rows = qv + d_pad;
+    unsigned long long *L = reinterpret_cast<unsigned long long *>(rows + TC_RR_NBUF * TC_RR_BUF);
     unsigned long long *C = L + KCAP;   // warp_merge's candidate slots (EX_CB)
     for (int dd = lane; dd < d_pad; dd += 32) qv[dd] = dd < d ? qry[(size_t)dd * ldq + q] : 0.f;
     for (int t = lane; t < KCAP; t += 32) L[t] = t < k ? run[(size_t)q * k + t] : kKeyInf;
@@ -1237,7 +1247,7 @@ __global__ void __launch_bounds__(32)
         const int n = min(EX_CB, c - b0);
         for (int t = lane; t < n; t += 32) C[t] = cq[b0 + t];
         __syncwarp();
-        rr_exact_distances(C, n, refT, d_pad, qv, lane);
+        rr_exact_distances(C, n, refT, d_pad, qv, rows, lane);
         __syncwarp();
         warp_merge<KCAP>(L, n, k, lane);
     }
@@ -1888,7 +1898,8 @@ int tc_run_rerank_piece(TcRun &r, cudaStream_t st) {
         r.pieces = true;
     }
     const int kcap = P.k <= 32 ? 32 : (P.k <= 64 ? 64 : (P.k <= 128 ? 128 : 256));
-    const size_t smem = (size_t)r.d_pad * 4 + (size_t)(kcap + EX_CB) * 8;
+    const size_t smem = (size_t)r.d_pad * 4 + (size_t)TC_RR_NBUF * TC_RR_BUF * 4 +
+                        (size_t)(kcap + EX_CB) * 8;
     if (smem > kRerankSmem) return kErrUnsupported;
     auto go = [&](auto kern) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
