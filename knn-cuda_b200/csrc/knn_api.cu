@@ -377,9 +377,15 @@ size_t usable_memory(const Workspace &ws) {
 
 // Largest query chunk (all of Q when it fits, else a multiple of 256) whose
 // memory, per_chunk(qc) on top of `fixed`, fits the usable memory; 0 when
-// not even one query fits.
+// not even one query fits.  When the whole call fits in what the workspace
+// already holds (repeated calls of one shape) and no cap is set, the device
+// is not asked for its free memory: cudaMemGetInfo costs a driver round
+// trip on every call otherwise.
 template <class F>
 int plan_query_chunk(const Workspace &ws, int Q, size_t fixed, F per_chunk) {
+    const size_t held = ws.ref.bytes + ws.qry.bytes + ws.dist.bytes + ws.idx.bytes +
+                        ws.scratch.bytes + ws.tcref.bytes;
+    if (!g_mem_cap && fixed + per_chunk(Q) <= held) return Q;
     const size_t avail = usable_memory(ws);
     auto fits = [&](int qc) { return fixed + per_chunk(qc) <= avail; };
     if (fits(Q)) return Q;

@@ -877,9 +877,7 @@ __global__ void tc_pack_f8_kernel(const float *__restrict__ x, int n, long long 
 // three times the spread of its KS sample values is expected to overflow
 // its candidate list (about KS x stride points lie below T, and the band
 // [T, T + E] adds E / (T - L_0) times as many): n_wide counts them.
-// The prediction uses the `probe` bound: the BF16 one, whether the scan
-// itself is BF16 (switch its pass 2 to split BF16) or FP8 (choose the kind
-// of the second scan).
+// The prediction uses the `probe` bound (the scan kind's own).
 __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
                                     const float *__restrict__ qn,
                                     const unsigned *__restrict__ rmax_bits, float inv_scale,
@@ -1842,23 +1840,36 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
     int rc = launch_scan<0>(r, st, r.kind, r.qB, r.qBlo, r.q8, P.Q, nullptr, r.cmax, 0,
                             r.sample, r.splits1);
     if (rc != kOk) return rc;
-    if (P.timer) P.timer->mark(st, kPhaseTcPass1);
-    // TP_LISTS lists (column ranges) per pair and split; resets the counts
+    if (P.timer) P.timer->mark(st, r.kind == kTcFp8 ? kPhaseTcPass1Fp8 : kPhaseTcPass1);
+    // TP_LISTS lists (column ranges) per pair and split; resets the counts.
+    // Predicted overflow (n_wide, under this kind's own bound) decides: a
+    // BF16 pass 2 switches to split BF16, an FP8 one falls back to BF16.
     const bool lo_ok = kind_fits(kTcBf16x3, r.d_pad, r.d_pad8) && r.R.refBlo && r.R.state;
-    const bool may_switch = P.adaptive && P.host_tmp && r.kind == kTcBf16 && lo_ok;
-    // FP8: the same prediction for BF16 picks the second scan's kind
-    const bool probe_fp8 = r.kind == kTcFp8 && lo_ok;
+    const bool probe = P.host_tmp && ((r.kind == kTcBf16 && P.adaptive && lo_ok) ||
+                                      r.kind == kTcFp8);
+    const TcBound bound = run_bound(r, r.kind);
+    if (probe && cudaMemsetAsync(r.nwide, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
     tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
         r.p1, TP_LISTS * r.splits1, P.Q, r.qn, r.R.rmax_bits,
-        r.kind == kTcFp8 ? 1.f / r.scale : 1.f, run_bound(r, r.kind), run_bound(r, kTcBf16),
-        r.thr, r.thr_raw, r.count, (may_switch || probe_fp8) ? r.nwide : nullptr);
+        r.kind == kTcFp8 ? 1.f / r.scale : 1.f, bound, bound, r.thr, r.thr_raw, r.count,
+        probe ? r.nwide : nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-    if (may_switch) {
-        // most lists expected to overflow in BF16: the whole pass 2 runs in
-        // split BF16 instead (thresholds re-derived from the sample's values)
+    if (probe) {
         int wide = 0;
         if ((rc = read_count(r.nwide, P.host_tmp, st, wide)) != kOk) return rc;
-        if (2 * wide > P.Q) {
+        if (2 * wide > P.Q && r.kind == kTcFp8) {
+            // FP8's bound is too wide for this data: most lists would
+            // overflow.  The sample pass is repeated in BF16 and the call
+            // continues on the BF16 path.
+            tc_pack_kernel<<<dim3((P.Q + 31) / 32, r.d_pad / 32), dim3(32, 8), 0, st>>>(
+                P.qry, P.Q, P.ldq, P.d, r.d_pad, r.R.center, -2.0f, r.qB);
+            if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+            r.kind = kTcBf16;
+            return tc_run_pass1(r, st);
+        }
+        if (2 * wide > P.Q && r.kind == kTcBf16) {
+            // most lists expected to overflow in BF16: the whole pass 2
+            // runs in split BF16 (thresholds re-derived from the sample)
             if ((rc = ensure_ref_lo(r, st)) != kOk) return rc;
             tc_pack_kernel<<<dim3((P.Q + 31) / 32, r.d_pad / 32), dim3(32, 8), 0, st>>>(
                 P.qry, P.Q, P.ldq, P.d, r.d_pad, r.R.center, -2.0f, r.qB, r.qBlo);
@@ -1952,19 +1963,12 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     if (nf == 0) return kOk;
 
     // second chance: the uncertified queries, compacted, scanned again with
-    // thresholds that certify (list overflows excepted).  Kind: split BF16
-    // when most failures are overflowing BF16 lists (BF16 too coarse for
-    // this data); after an FP8 scan, BF16 unless the threshold pass
-    // predicted BF16 lists to overflow for most queries; else the first
-    // scan's kind.
+    // thresholds that certify (list overflows excepted).  Kind: BF16 after
+    // an FP8 scan, else the first scan's kind -- split BF16 instead of BF16
+    // when most failures are overflowing lists (BF16 too coarse for them).
     const bool lo_ok = kind_fits(kTcBf16x3, r.d_pad, r.d_pad8) && r.R.refBlo && r.R.state;
-    int kind2 = r.kind;
-    if (r.kind == kTcBf16 && lo_ok && 2 * n_over > nf) kind2 = kTcBf16x3;
-    if (r.kind == kTcFp8) {
-        int wide = 0;
-        if (lo_ok && (rc = read_count(r.nwide, host_tmp, st, wide)) != kOk) return rc;
-        kind2 = (lo_ok && 2 * wide > P.Q) ? kTcBf16x3 : kTcBf16;
-    }
+    int kind2 = r.kind == kTcFp8 ? kTcBf16 : r.kind;
+    if (kind2 == kTcBf16 && lo_ok && 2 * n_over > nf) kind2 = kTcBf16x3;
     host_stats[7] = kind2;
     if (kind2 == kTcBf16x3 && (rc = ensure_ref_lo(r, st)) != kOk) return rc;
     gather_queries_kernel<<<dim3((nf + 127) / 128, P.d), 128, 0, st>>>(P.qry, P.ldq, P.d, r.fail,

@@ -48,7 +48,7 @@ def _case(name):
         # directions, so the translation by the mean does not shrink the
         # norms and the error bound exceeds the in-cluster spread (lists
         # overflow, second scan)
-        both = _far_clusters(31, 256, 32768 + 300, 16, 6.0, 0.01)
+        both = _far_clusters(31, 256, 32768 + 300, 16, 6.0, 0.05)
         return (np.ascontiguousarray(both[:, :32768]), np.ascontiguousarray(both[:, 32768:]),
                 100)
     if name == "uniform1000_d128":
@@ -67,8 +67,9 @@ CASES = ["mixture256_q2048", "offset50_d64", "mixture128_q1000", "far_clusters_d
 def test_observed_error_within_half_the_bound(knncuda, gpu, name, method):
     """cublas: the BF16 scan, or split BF16 where the threshold pass switches
     to it (mixture128, the far clusters); fp8: the e4m3 scan with its own
-    bound (uncertified queries are scanned again in BF16 and checked under
-    the BF16 bound)."""
+    bound where it runs, the BF16 path where its sample pass predicts
+    overflowing lists (uncertified queries are scanned again in BF16 and
+    checked under that bound)."""
     import torch
 
     ref, query, k = _case(name)
