@@ -11,9 +11,14 @@
 // workspace (grow-only device buffers, one stream, one status word) guarded
 // by a mutex, so calls are thread-safe and no distance matrix exists.
 #include <algorithm>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <functional>
+#include <memory>
 #include <mutex>
+#include <thread>
+#include <vector>
 
 #include <cudaTypedefs.h>
 
@@ -86,6 +91,81 @@ struct Buffer {
     }
 };
 
+// A small pool of host threads for gathering pageable input into pinned
+// staging buffers (memcpy of many rows at once).  run(n, fn) calls fn(i)
+// for i in [0, n) on the pool and the calling thread, and returns when all
+// are done.
+class HostPool {
+  public:
+    explicit HostPool(int threads) {
+        for (int t = 0; t < threads; ++t) workers_.emplace_back([this] { loop(); });
+    }
+    ~HostPool() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (std::thread &t : workers_) t.join();
+    }
+    void run(int n, const std::function<void(int)> &fn) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            fn_ = &fn;
+            n_ = n;
+            next_ = 0;
+            done_ = 0;
+            ++gen_;
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> g(mu_);
+        done_cv_.wait(g, [this] { return done_ == n_; });
+        fn_ = nullptr;
+    }
+
+  private:
+    void work() {
+        for (;;) {
+            int i;
+            const std::function<void(int)> *fn;
+            {
+                std::lock_guard<std::mutex> g(mu_);
+                if (!fn_ || next_ >= n_) return;
+                i = next_++;
+                fn = fn_;
+            }
+            (*fn)(i);
+            std::lock_guard<std::mutex> g(mu_);
+            if (++done_ == n_) done_cv_.notify_all();
+        }
+    }
+    void loop() {
+        long long seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            work();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(int)> *fn_ = nullptr;
+    int n_ = 0, next_ = 0, done_ = 0;
+    long long gen_ = 0;
+    bool stop_ = false;
+};
+
+// Pinned staging of the streamed host entry for pageable input: two
+// buffers; the host gathers a piece of the reference set into one while the
+// other's copy is in flight.
+constexpr size_t kStageBytes = 32u << 20;
+
 // Host entry of knn_cublas on large sets: the reference set is copied in
 // this many chunks (after the sample runs of the threshold pass), each
 // chunk's prep and scan overlapping the copy of the next.  Relative chunk
@@ -113,6 +193,25 @@ struct Workspace {
     int *tc_stats = nullptr;           // pinned: [0] second-scan queries, [1] exact fallbacks
     cudaStream_t copy_stream = nullptr;          // host entry: reference copies
     cudaEvent_t copied[1 + kStreamChunks] = {};  // sample, then each chunk
+    float *stage[2] = {nullptr, nullptr};        // pinned staging for pageable input
+    cudaEvent_t stage_done[2] = {};              // the copy out of each stage has ended
+    int stage_slot = 0;
+    std::unique_ptr<HostPool> pool;              // gathers into the staging buffers
+
+    // Staging buffers and the pool, on first use.
+    bool ensure_staging() {
+        if (stage[0]) return true;
+        for (int i = 0; i < 2; ++i) {
+            if (cudaMallocHost(reinterpret_cast<void **>(&stage[i]), kStageBytes) != cudaSuccess ||
+                cudaEventCreateWithFlags(&stage_done[i], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                return false;
+            }
+        }
+        const unsigned hc = std::thread::hardware_concurrency();
+        pool.reset(new HostPool((int)std::max(1u, std::min(16u, hc ? hc : 4u)) - 1));
+        return true;
+    }
 
     bool setup(int dev) {
         if (init) return true;
@@ -230,11 +329,12 @@ int for_each_gap(const TileRuns &s, int tb, int te, F fn) {
 // overlaps the threshold pass and the pass-2 scan of all but the last
 // (smallest) chunk.  Every byte crosses the bus once.
 int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_host,
-                        cudaStream_t st) {
+                        bool pinned, cudaStream_t st) {
     for (int i = 0; i < 8; ++i) ws.tc_stats[i] = 0;
     ws.tc_stats[6] = ws.tc_stats[7] = -1;
     ws.timer.begin(st);
     if (!ws.tcref.ensure(tc_ref_bytes(p.N, p.d))) return kErrNoMemory;
+    if (!pinned && !ws.ensure_staging()) return kErrNoMemory;
     const TcRefView rv = tc_carve_ref(ws.tcref.ptr, p.N, p.d, &ws.tc_state);
     float *ref_d = const_cast<float *>(p.ref);
     const int T = tc_tile_points();
@@ -242,15 +342,41 @@ int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_h
     const TileRuns sample = tc_sample_runs(p.N, p.Q, p.d, p.k, p.num_sms);
     const size_t fb = sizeof(float);
     cudaStream_t cs = ws.copy_stream;
-    // points [t0 T, t1 T) of every dimension, one 2-D copy
+    // points [c0, c0 + len) of every dimension from page-locked memory: one
+    // 2-D copy
+    auto copy_direct = [&](size_t c0, size_t len) -> int {
+        return cudaMemcpy2DAsync(ref_d + c0, (size_t)p.ldr * fb, ref_host + c0, (size_t)p.N * fb,
+                                 len * fb, p.d, cudaMemcpyHostToDevice, cs) == cudaSuccess
+                   ? kOk
+                   : kErrCuda;
+    };
+    // the same from pageable memory: through the staging buffers, at most
+    // kStageBytes per piece; the host gathers the piece's rows (the pool
+    // splits them) while the previous piece's copy is in flight
+    auto copy_staged = [&](size_t c0, size_t len) -> int {
+        const size_t cols = std::max<size_t>(1, kStageBytes / ((size_t)p.d * fb));
+        for (size_t q0 = c0; q0 < c0 + len; q0 += cols) {
+            const size_t n = std::min(cols, c0 + len - q0);
+            const int slot = ws.stage_slot;
+            ws.stage_slot ^= 1;
+            if (cudaEventSynchronize(ws.stage_done[slot]) != cudaSuccess) return kErrCuda;
+            float *dst = ws.stage[slot];
+            const std::function<void(int)> rows = [&](int dd) {
+                std::memcpy(dst + (size_t)dd * n, ref_host + (size_t)dd * p.N + q0, n * fb);
+            };
+            ws.pool->run(p.d, rows);
+            if (cudaMemcpy2DAsync(ref_d + q0, (size_t)p.ldr * fb, dst, n * fb, n * fb, p.d,
+                                  cudaMemcpyHostToDevice, cs) != cudaSuccess ||
+                cudaEventRecord(ws.stage_done[slot], cs) != cudaSuccess)
+                return kErrCuda;
+        }
+        return kOk;
+    };
+    // points [t0 T, t1 T) of every dimension
     auto copy_tiles = [&](int t0, int t1) -> int {
         const size_t p0 = (size_t)t0 * T, p1 = std::min<size_t>(p.N, (size_t)t1 * T);
         if (p0 >= p1) return kOk;
-        return cudaMemcpy2DAsync(ref_d + p0, (size_t)p.ldr * fb, ref_host + p0, (size_t)p.N * fb,
-                                 (p1 - p0) * fb, p.d, cudaMemcpyHostToDevice,
-                                 cs) == cudaSuccess
-                   ? kOk
-                   : kErrCuda;
+        return pinned ? copy_direct(p0, p1 - p0) : copy_staged(p0, p1 - p0);
     };
     // the copies start after everything queued so far on the compute stream
     // (an earlier call may still read the reference buffer)
@@ -268,10 +394,6 @@ int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_h
     for (int c = 0, acc = 0; c < kStreamChunks; ++c) {
         acc += kStreamWeights[c];
         bound[c + 1] = (int)((long long)n_tiles * acc / wsum);
-    }
-    for (int c = 0; c < kStreamChunks; ++c) {
-        if ((rc = for_each_gap(sample, bound[c], bound[c + 1], copy_tiles)) != kOk) return rc;
-        if (cudaEventRecord(ws.copied[1 + c], cs) != cudaSuccess) return kErrCuda;
     }
 
     TcProblem t;
@@ -307,8 +429,14 @@ int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_h
     auto prep_tiles = [&](int t0, int t1) {
         return tc_prepare_ref_tiles(rv, p.ref, p.N, p.ldr, p.d, t0, contiguous_tiles(t1 - t0), st);
     };
+    // each chunk's copy, then its prep, scan and re-rank (queued behind the
+    // copy's event), so the work of chunk c is on the device while the host
+    // gathers chunk c + 1 (pageable input)
     for (int c = 0; c < kStreamChunks; ++c) {
-        if (cudaStreamWaitEvent(st, ws.copied[1 + c], 0) != cudaSuccess) return kErrCuda;
+        if ((rc = for_each_gap(sample, bound[c], bound[c + 1], copy_tiles)) != kOk) return rc;
+        if (cudaEventRecord(ws.copied[1 + c], cs) != cudaSuccess ||
+            cudaStreamWaitEvent(st, ws.copied[1 + c], 0) != cudaSuccess)
+            return kErrCuda;
         if (bound[c] >= bound[c + 1]) continue;
         if ((rc = for_each_gap(sample, bound[c], bound[c + 1], prep_tiles)) != kOk ||
             (rc = tc_run_pass2(run, bound[c], bound[c + 1], st)) != kOk ||
@@ -463,8 +591,11 @@ bool host_entry(int method, const float *ref, int ref_nb, const float *query, in
     cudaStream_t st = ws->stream;
     float *ref_d = static_cast<float *>(ws->ref.ptr);
     float *qry_d = static_cast<float *>(ws->qry.ptr);
-    // the streamed reference copy serves a call that runs as one chunk
-    const bool streamed = tc && qc == query_nb && ref_nb >= kStreamMinPoints && host_pinned(ref);
+    // the streamed reference copy serves a call that runs as one chunk;
+    // page-locked input is copied directly, pageable input through the
+    // pinned staging buffers
+    const bool streamed = tc && qc == query_nb && ref_nb >= kStreamMinPoints;
+    const bool pinned = streamed && host_pinned(ref);
     cudaError_t e0 = streamed ? cudaSuccess
                               : cudaMemcpy2DAsync(ref_d, ldr * sizeof(float), ref,
                                                   ref_nb * sizeof(float), ref_nb * sizeof(float),
@@ -502,7 +633,7 @@ bool host_entry(int method, const float *ref, int ref_nb, const float *query, in
         p.status = static_cast<int *>(ws->status.ptr);
         p.num_sms = ws->num_sms;
         p.force_splits = 0;
-        rc = streamed ? enqueue_tc_streamed(*ws, p, ref, st)
+        rc = streamed ? enqueue_tc_streamed(*ws, p, ref, pinned, st)
                       : enqueue(*ws, p, method, st, /*ref_prepared=*/q0 > 0);
         if (rc != kOk) {
             std::printf("ERROR: Unable to execute kernel (%s)\n", knnb200_status_string(rc));
