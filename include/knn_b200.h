@@ -297,10 +297,9 @@ KNNB200_API void knnb200_set_phase_timing(int enable);
  * indexed by phase: 0 tensor-path reference prep, 1 query prep, 2 pass-1 scan,
  * 3 thresholds, 4 pass-2 scan, 5 exact re-rank, 6 uncertified-query fallback,
  * 7 fused exact kernel, 8 split merge, 9 second-chance scan of uncertified
- * queries (with the host round trip before it), 10 their re-rank, 11 the
- * FP8 sample pass of an FP8-method call; -1 for phases the call did not
- * run.  Waits for the call's last event.  Returns the number of phases
- * (12), or 0 when nothing was timed. */
+ * queries (with the host round trip before it), 10 their re-rank; -1 for
+ * phases the call did not run.  Waits for the call's last event.  Returns
+ * the number of phases (11), or 0 when nothing was timed. */
 KNNB200_API int knnb200_last_phase_times(float *ms, int n);
 
 /* Library version string. */

@@ -38,8 +38,7 @@ enum Phase : int {
     kPhaseExactMerge = 8,
     kPhaseTcRetryScan = 9,     // second-chance scan of uncertified queries
     kPhaseTcRetryRerank = 10,
-    kPhaseTcPass1Fp8 = 11,     // the FP8 sample pass (an FP8 request)
-    kNumPhases = 12,
+    kNumPhases = 11,
 };
 
 struct PhaseTimer {
@@ -214,6 +213,7 @@ struct TcRun {
     TileRuns sample;
     int d_pad, d_pad8, qtiles, n_tiles2, splits1, cmax;
     int kind;               // kind of the first scan's pass 2 (TcKind in knn_tc.cu)
+    bool want_fp8;          // FP8 requested: pass 2 in FP8 if predicted to fit
     float s_q, scale;       // FP8: query scale, accumulator units per a unit (s_q s_r)
     long long ldf;
     __nv_bfloat16 *qB, *qBlo;
@@ -265,8 +265,8 @@ int tc_prepare_extras(const TcRefView &v, int N, int d, cudaStream_t st, int *ho
 // given the second scan, [1] queries recomputed by the exact kernel, [2..3]
 // scratch, [4..5] total first-scan candidates (64-bit), [6] kind of the
 // first scan's pass 2, [7] kind of the second scan (-1: none); kinds are
-// 0 BF16, 1 split BF16, 2 FP8 (an FP8 request whose sample pass predicts
-// overflowing lists runs BF16 and reports that).
+// 0 BF16, 1 split BF16, 2 FP8 (an FP8 request whose BF16 sample pass
+// predicts overflowing FP8 lists runs BF16 and reports that).
 int launch_tc(const TcProblem &P, const TcRefView &R, cudaStream_t st, int *host_stats);
 
 }  // namespace knnb200

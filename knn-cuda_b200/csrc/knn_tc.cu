@@ -871,17 +871,17 @@ __global__ void tc_pack_f8_kernel(const float *__restrict__ x, int n, long long 
 // Emission threshold: the KS-th smallest of the per-split pass-1 lists plus
 // the error bound E_q (so that the k-th exact distance only has to lie below
 // the sample's KS-th approximate one to certify); resets candidate counts.
-// The lists hold accumulator values (inv_scale turns them into a units).
-// thr_raw keeps the sample's KS-th value itself (a second scan of another
-// kind re-derives its threshold from it).  A query whose bound exceeds
-// three times the spread of its KS sample values is expected to overflow
-// its candidate list (about KS x stride points lie below T, and the band
-// [T, T + E] adds E / (T - L_0) times as many): n_wide counts them.
-// The prediction uses the `probe` bound (the scan kind's own).
+// thr_raw keeps the sample's KS-th value itself (a scan of another kind
+// re-derives its threshold from it).  Overflow prediction: a query whose
+// bound under a probe kind exceeds three times the spread of its KS sample
+// values is expected to overflow its candidate list in that kind (about
+// KS x stride points lie below T, and the band [T, T + E] adds E / (T - L_0)
+// times as many); n_wide[0] counts them for probe0 (BF16: switch to split
+// BF16), n_wide[1] for probe1 (FP8: whether an FP8 pass 2 pays).
 __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
                                     const float *__restrict__ qn,
-                                    const unsigned *__restrict__ rmax_bits, float inv_scale,
-                                    TcBound bound, TcBound probe, float *__restrict__ thr,
+                                    const unsigned *__restrict__ rmax_bits, TcBound bound,
+                                    TcBound probe0, TcBound probe1, float *__restrict__ thr,
                                     float *__restrict__ thr_raw, int *__restrict__ count,
                                     int *__restrict__ n_wide) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -900,26 +900,32 @@ __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
             L[0] = fminf(L[0], v);
         }
     }
-    const float T = L[TC_KS - 1] * inv_scale;
-    const float E = tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T, bound);
-    thr[q] = T + E;
+    const float T = L[TC_KS - 1];
+    const float r2 = __uint_as_float(*rmax_bits);
+    thr[q] = T + tc_error_bound(qn[q], r2, T, bound);
     thr_raw[q] = T;
     count[q] = 0;
-    if (n_wide && tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T, probe) >
-                      3.f * (T - L[0] * inv_scale))
-        atomicAdd(n_wide, 1);
+    if (n_wide) {
+        const float spread3 = 3.f * (T - L[0]);
+        if (tc_error_bound(qn[q], r2, T, probe0) > spread3) atomicAdd(n_wide, 1);
+        if (tc_error_bound(qn[q], r2, T, probe1) > spread3) atomicAdd(n_wide + 1, 1);
+    }
 }
 
 // Thresholds of a scan of another kind from the raw sample thresholds:
-// thr = T + E_q(T) under that kind's bound.
+// thr = T + E_q(T) under that kind's bound, plus E_q(T) under `extra` (the
+// sample's own kind when it differs from the scan's: the sample value
+// itself is then off by up to that bound).
 __global__ void tc_rethreshold_kernel(const float *__restrict__ thr_raw, int Q,
                                       const float *__restrict__ qn,
                                       const unsigned *__restrict__ rmax_bits, TcBound bound,
-                                      float *__restrict__ thr) {
+                                      TcBound extra, int use_extra, float *__restrict__ thr) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= Q) return;
-    const float T = thr_raw[q];
-    thr[q] = T + tc_error_bound(qn[q], __uint_as_float(*rmax_bits), T, bound);
+    const float T = thr_raw[q], r2 = __uint_as_float(*rmax_bits);
+    float t = T + tc_error_bound(qn[q], r2, T, bound);
+    if (use_extra) t += tc_error_bound(qn[q], r2, T, extra);
+    thr[q] = t;
 }
 
 // Ascending bitonic sort of keys[0..P) (P a power of two) by one warp.
@@ -1814,12 +1820,14 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     tc_norms_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
         P.qry, P.Q, P.ldq, P.d, R.center, r.qn, nullptr,
         fp8 ? reinterpret_cast<unsigned *>(r.nwide + 2) : nullptr);
-    if (!fp8)
-        tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
-            P.qry, P.Q, P.ldq, P.d, p.d_pad, R.center, -2.0f, r.qB);
+    tc_pack_kernel<<<dim3((P.Q + 31) / 32, p.d_pad / 32), dim3(32, 8), 0, st>>>(
+        P.qry, P.Q, P.ldq, P.d, p.d_pad, R.center, -2.0f, r.qB);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    r.want_fp8 = false;
     if (fp8) {
-        // the reference set's FP8 copy, then the queries' scale and copy
+        // the reference set's FP8 copy, then the queries' scale and copy;
+        // the sample pass still runs in BF16 and decides whether pass 2
+        // runs in FP8
         unsigned *host_tmp = reinterpret_cast<unsigned *>(P.host_tmp);
         int rc = ensure_ref_f8(r, st, host_tmp);
         if (rc == kOk) rc = fp8_query_scale(r, st, reinterpret_cast<unsigned *>(r.nwide + 2), host_tmp);
@@ -1827,7 +1835,7 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
         tc_pack_f8_kernel<<<dim3((P.Q + 31) / 32, p.d_pad8 / 32), dim3(32, 8), 0, st>>>(
             P.qry, P.Q, P.ldq, P.d, p.d_pad8, R.center, -2.0f * r.s_q, r.q8);
         if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-        r.kind = kTcFp8;
+        r.want_fp8 = true;
     }
     if (P.timer) P.timer->mark(st, kPhaseTcPrepQuery);
     if (cudaMemsetAsync(r.cand_total, 0, sizeof(unsigned long long), st) != cudaSuccess)
@@ -1837,44 +1845,43 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
 
 int tc_run_pass1(TcRun &r, cudaStream_t st) {
     const TcProblem &P = r.P;
-    int rc = launch_scan<0>(r, st, r.kind, r.qB, r.qBlo, r.q8, P.Q, nullptr, r.cmax, 0,
-                            r.sample, r.splits1);
+    // the sample pass runs in BF16 for every request: its values are close
+    // enough to the exact ones to set thresholds and to predict whether a
+    // pass 2 of another kind would overflow its lists
+    int rc = launch_scan<0>(r, st, kTcBf16, r.qB, r.qBlo, r.q8, P.Q, nullptr, r.cmax, 0, r.sample,
+                            r.splits1);
     if (rc != kOk) return rc;
-    if (P.timer) P.timer->mark(st, r.kind == kTcFp8 ? kPhaseTcPass1Fp8 : kPhaseTcPass1);
-    // TP_LISTS lists (column ranges) per pair and split; resets the counts.
-    // Predicted overflow (n_wide, under this kind's own bound) decides: a
-    // BF16 pass 2 switches to split BF16, an FP8 one falls back to BF16.
+    if (P.timer) P.timer->mark(st, kPhaseTcPass1);
+    // TP_LISTS lists (column ranges) per pair and split; resets the counts
     const bool lo_ok = kind_fits(kTcBf16x3, r.d_pad, r.d_pad8) && r.R.refBlo && r.R.state;
-    const bool probe = P.host_tmp && ((r.kind == kTcBf16 && P.adaptive && lo_ok) ||
-                                      r.kind == kTcFp8);
-    const TcBound bound = run_bound(r, r.kind);
-    if (probe && cudaMemsetAsync(r.nwide, 0, sizeof(int), st) != cudaSuccess) return kErrCuda;
+    const bool probe = P.host_tmp && ((P.adaptive && lo_ok) || r.want_fp8);
+    if (probe && cudaMemsetAsync(r.nwide, 0, 2 * sizeof(int), st) != cudaSuccess) return kErrCuda;
+    const TcBound b16 = run_bound(r, kTcBf16);
     tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
-        r.p1, TP_LISTS * r.splits1, P.Q, r.qn, r.R.rmax_bits,
-        r.kind == kTcFp8 ? 1.f / r.scale : 1.f, bound, bound, r.thr, r.thr_raw, r.count,
+        r.p1, TP_LISTS * r.splits1, P.Q, r.qn, r.R.rmax_bits, b16, b16,
+        r.want_fp8 ? run_bound(r, kTcFp8) : b16, r.thr, r.thr_raw, r.count,
         probe ? r.nwide : nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+    r.kind = kTcBf16;
     if (probe) {
-        int wide = 0;
-        if ((rc = read_count(r.nwide, P.host_tmp, st, wide)) != kOk) return rc;
-        if (2 * wide > P.Q && r.kind == kTcFp8) {
-            // FP8's bound is too wide for this data: most lists would
-            // overflow.  The sample pass is repeated in BF16 and the call
-            // continues on the BF16 path.
-            tc_pack_kernel<<<dim3((P.Q + 31) / 32, r.d_pad / 32), dim3(32, 8), 0, st>>>(
-                P.qry, P.Q, P.ldq, P.d, r.d_pad, r.R.center, -2.0f, r.qB);
+        int wide16 = 0;
+        if ((rc = read_count(r.nwide, P.host_tmp, st, wide16, 2)) != kOk) return rc;
+        const int wide8 = P.host_tmp[1];
+        if (r.want_fp8 && 2 * wide8 <= P.Q) {
+            // FP8 pass 2: thresholds T + E_bf16 + E_fp8 (the sample value
+            // is a BF16 one)
+            tc_rethreshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
+                r.thr_raw, P.Q, r.qn, r.R.rmax_bits, run_bound(r, kTcFp8), b16, 1, r.thr);
             if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
-            r.kind = kTcBf16;
-            return tc_run_pass1(r, st);
-        }
-        if (2 * wide > P.Q && r.kind == kTcBf16) {
-            // most lists expected to overflow in BF16: the whole pass 2
-            // runs in split BF16 (thresholds re-derived from the sample)
+            r.kind = kTcFp8;
+        } else if (P.adaptive && lo_ok && 2 * wide16 > P.Q) {
+            // most lists expected to overflow in BF16: pass 2 runs in split
+            // BF16 (thresholds re-derived from the sample)
             if ((rc = ensure_ref_lo(r, st)) != kOk) return rc;
             tc_pack_kernel<<<dim3((P.Q + 31) / 32, r.d_pad / 32), dim3(32, 8), 0, st>>>(
                 P.qry, P.Q, P.ldq, P.d, r.d_pad, r.R.center, -2.0f, r.qB, r.qBlo);
             tc_rethreshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
-                r.thr_raw, P.Q, r.qn, r.R.rmax_bits, run_bound(r, kTcBf16x3), r.thr);
+                r.thr_raw, P.Q, r.qn, r.R.rmax_bits, run_bound(r, kTcBf16x3), b16, 0, r.thr);
             if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
             r.kind = kTcBf16x3;
         }

@@ -79,8 +79,7 @@ class Problem(ctypes.Structure):
                 ("knn_dist", ctypes.c_void_p), ("knn_index", ctypes.c_void_p),
                 ("out_ld", ctypes.c_longlong)]
 PHASES = ("tc_prep_ref", "tc_prep_query", "tc_pass1", "tc_threshold", "tc_pass2", "tc_rerank",
-          "tc_fallback", "exact_main", "exact_merge", "tc_retry_scan", "tc_retry_rerank",
-          "tc_pass1_fp8")
+          "tc_fallback", "exact_main", "exact_merge", "tc_retry_scan", "tc_retry_rerank")
 CXX_SYMBOLS = (
     "_Z15knn_cuda_globalPKfiS0_iiiPfPi",
     "_Z16knn_cuda_texturePKfiS0_iiiPfPi",
