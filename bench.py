@@ -76,8 +76,8 @@ def parse_args(argv=None):
     p.add_argument("--cpu-seconds", type=float, default=15.0,
                    help="target CPU time of the bounded knn_c sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--no-fp8-showcase", action="store_true",
-                   help="skip the FP8 / BF16 comparison on uniform128")
+    p.add_argument("--no-fp8-forced", action="store_true",
+                   help="skip the measurement of an FP8 pass 2 forced on the workload")
     p.add_argument("--mode", choices=["batch", "serving", "batched"], default="batch",
                    help="serving: resident serving128 set, Poisson request stream; "
                         "batched: 512 uneven problems, one persistent launch vs per-problem")
@@ -291,44 +291,41 @@ def fp64_recall(torch, ref_d, qry_d, idx, dist, k, sample):
     return hits / (k * len(sample)), worst
 
 
-def fp8_showcase(knncuda, torch, dev, stream, warm, steps=3):
-    """FP8 and BF16 scans on data where the FP8 bound is small against the
-    distance spread (U[0,1)^128, 1M points, 16384 queries, k = 16): both
-    tiers timed like the main ones, answers checked against the exact path."""
-    ref, query = workloads.generate(workloads.WORKLOADS["uniform128"])
-    r, q = torch.from_numpy(ref).to(dev), torch.from_numpy(query).to(dev)
-    k, qn = 16, query.shape[1]
-    out = {"workload": "uniform128 (1,048,576 x 16,384, d = 128, k = 16, U[0,1))"}
-    res = {}
-    for method in ("global", "cublas", "fp8"):
-        d = torch.empty((k, qn), dtype=torch.float32, device=dev)
-        i = torch.empty((k, qn), dtype=torch.int32, device=dev)
-        for _ in range(warm):
-            knncuda.knn_device(r, q, k, method, d, i, stream)
+def fp8_forced(knncuda, torch, dev, ref_d, qry_d, k, stream, outs, steps=2):
+    """The FP8 request with pass 2 forced to FP8 (the library's test and
+    measurement override), timed like the tiers: what an FP8 candidate scan
+    costs on this data, answers still exact."""
+    qn = qry_d.shape[1]
+    d = torch.empty((k, qn), dtype=torch.float32, device=dev)
+    i = torch.empty((k, qn), dtype=torch.int32, device=dev)
+    knncuda.set_tc_kind_override("fp8")
+    try:
+        knncuda.knn_device(ref_d, qry_d, k, "fp8", d, i, stream)
         torch.cuda.synchronize(dev)
         knncuda.set_phase_timing(True)
+        ph, st = {}, {}
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ph = {}
         e0.record(stream)
         for _ in range(steps):
-            knncuda.knn_device(r, q, k, method, d, i, stream)
+            knncuda.knn_device(ref_d, qry_d, k, "fp8", d, i, stream)
             torch.cuda.synchronize(dev)
             for kk, v in knncuda.last_phase_times().items():
                 ph[kk] = ph.get(kk, 0.0) + v / steps
+            st = knncuda.last_tc_stats()
         e1.record(stream)
         torch.cuda.synchronize(dev)
         knncuda.set_phase_timing(False)
-        ms = e0.elapsed_time(e1) / steps
-        res[method] = (d, i)
-        out[method] = {"value": qn / (ms * 1e-3), "ms_per_step": ms,
-                       "phase_ms": {kk: round(v, 4) for kk, v in ph.items()}}
-        if method != "global":
-            first, second = knncuda.last_tc_kinds()
-            out[method]["scan_kinds"] = {"pass2": first, "second_scan": second}
-            out[method]["identical_to_exact"] = bool(
-                torch.equal(d, res["global"][0]) and torch.equal(i, res["global"][1]))
-    out["fp8_vs_bf16"] = out["fp8"]["value"] / out["cublas"]["value"]
-    return out
+        kinds = knncuda.last_tc_kinds()
+    finally:
+        knncuda.set_tc_kind_override(None)
+    ms = e0.elapsed_time(e1) / steps
+    return {"value": qn / (ms * 1e-3), "ms_per_step": ms,
+            "phase_ms": {kk: round(v, 4) for kk, v in ph.items()},
+            "scan_kinds": {"pass2": kinds[0], "second_scan": kinds[1]},
+            "first_scan_candidates": st.get("candidates"),
+            "second_scan_queries": st.get("second_scan"), "exact_queries": st.get("exact"),
+            "identical_to_exact": bool(torch.equal(d, outs["exact_fp32"][0]) and
+                                       torch.equal(i, outs["exact_fp32"][1]))}
 
 
 def run_ours(args, D: Dist):
@@ -387,11 +384,11 @@ def run_ours(args, D: Dist):
     f8 = tiers["fp8_rerank"]
     f8["vs_bf16_rerank"] = f8["value"] / tiers["bf16_rerank"]["value"]
     if f8.get("scan_kinds", {}).get("pass2") != "fp8":
-        f8["note"] = ("the sample pass predicted overflowing FP8 candidate lists (the FP8 error "
-                      "bound exceeds this data's distance spread): pass 2 ran in BF16; "
-                      "see fp8_uniform128 for data where FP8 runs")
-    if D.world == 1 and not args.no_fp8_showcase:
-        tiers["fp8_uniform128"] = fp8_showcase(knncuda, torch, dev, stream, warm)
+        f8["note"] = ("the BF16 sample pass predicted overflowing FP8 candidate lists (the FP8 "
+                      "error bound exceeds this data's distance spread): pass 2 ran in BF16; "
+                      "fp8_forced is the same call with pass 2 forced to FP8")
+    if not args.no_fp8_forced:
+        f8["fp8_forced"] = fp8_forced(knncuda, torch, dev, ref_d, qry_d, k, stream, outs)
 
     # end to end through the drop-in host entry points (pinned buffers)
     ref_np, qry_np = ref_h.numpy(), qry_h.numpy()

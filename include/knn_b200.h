@@ -289,6 +289,14 @@ KNNB200_API int knnb200_last_bound_check(double *max_ratio, long long *checked);
  * no second scan).  Either pointer may be NULL. */
 KNNB200_API void knnb200_last_tc_kinds(int *first, int *second);
 
+/* Test and measurement override of the pass-2 kind of the device-entry
+ * tensor path (no counterpart in the reference): 0 BF16, 1 split BF16,
+ * 2 FP8 (FP8-method calls only), -1 none (the default: the kind the
+ * threshold pass predicts to fit).  Results stay exact whatever the kind:
+ * a forced kind whose lists overflow only costs time (second scan, exact
+ * kernel).  Process-wide. */
+KNNB200_API void knnb200_set_tc_kind_override(int kind);
+
 /* Per-phase device timing of the calls on the current device (CUDA events on
  * the launching stream between the kernels of a call).  Off by default. */
 KNNB200_API void knnb200_set_phase_timing(int enable);

@@ -238,6 +238,7 @@ struct Workspace {
 };
 
 Workspace g_ws[kMaxDevices];
+int g_force_kind = -1;   // knnb200_set_tc_kind_override
 
 long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
@@ -295,6 +296,7 @@ int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st,
     t.num_sms = p.num_sms;
     t.timer = &ws.timer;
     t.request = (method == KNNB200_METHOD_FP8 && tc_fp8_supported(p.d)) ? kTcReqFp8 : kTcReqBf16;
+    t.force_kind = g_force_kind;
     if (ws.bound_check) {
         if (cudaMemsetAsync(ws.bound.ptr, 0, 16, st) != cudaSuccess) return kErrCuda;
         t.bound_stat = static_cast<unsigned *>(ws.bound.ptr);
@@ -945,6 +947,10 @@ int knnb200_last_bound_check(double *max_ratio, long long *checked) {
     if (max_ratio) *max_ratio = r;
     if (checked) *checked = (long long)v[2] | ((long long)v[3] << 32);
     return KNNB200_OK;
+}
+
+void knnb200_set_tc_kind_override(int kind) {
+    g_force_kind = (kind >= 0 && kind <= 2) ? kind : -1;
 }
 
 void knnb200_last_tc_kinds(int *first, int *second) {

@@ -178,6 +178,9 @@ struct TcProblem {
     // the first scan's kind may switch to split BF16 after the threshold
     // pass (not with a reference set still streaming in)
     bool adaptive = true;
+    // pass-2 kind forced regardless of the overflow prediction (-1: none;
+    // a kind that does not fit the shape is ignored); tests and benchmarks
+    int force_kind = -1;
 };
 
 // A sample of the 256-point tiles: `run` consecutive tiles out of every

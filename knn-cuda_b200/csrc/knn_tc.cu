@@ -104,10 +104,10 @@ KNN_DI uint32_t select32(const uint32_t (&v)[32], int e) {
 }
 
 // Candidates found by one epilogue thread, appended to its query's list
-// later with one atomicAdd that reserves all their slots: the append's
-// round trip then overlaps the wait for the next accumulator instead of
-// lengthening the test of the current one (the next tile's TMEM load waits
-// for that test).
+// later with one atomicAdd that reserves all their slots.  The atomic is
+// issued before the wait for the next accumulator and the entries are
+// written once that accumulator has been read and released, so the
+// round trip overlaps the wait instead of delaying the release.
 struct PendingCands {
     static constexpr int kMax = 4;
     unsigned long long e[kMax];
@@ -115,6 +115,16 @@ struct PendingCands {
     KNN_DI void flush(int *count, unsigned long long *cand, int cmax, int qrow) {
         if (n == 0) return;
         const int pos = atomicAdd(&count[qrow], n);
+#pragma unroll
+        for (int p = 0; p < kMax; ++p)
+            if (p < n && pos + p < cmax) cand[(size_t)qrow * cmax + pos + p] = e[p];
+        n = 0;
+    }
+    // the slots for the buffered entries: issue the atomic now, use `pos`
+    // later (the round trip overlaps whatever runs in between)
+    KNN_DI int reserve(int *count, int qrow) const { return n ? atomicAdd(&count[qrow], n) : 0; }
+    KNN_DI void commit(int pos, unsigned long long *cand, int cmax, int qrow) {
+        if (n == 0) return;
 #pragma unroll
         for (int p = 0; p < kMax; ++p)
             if (p < n && pos + p < cmax) cand[(size_t)qrow * cmax + pos + p] = e[p];
@@ -308,6 +318,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
         // ---------------- TMA producer (both CTAs) ----------------
         if (lane == 0) {
             int issued = 0, n_issued = 0;
+            int ps = 0;          // ring stage of the next item
+            uint32_t pph = 0;    // its phase parity
             bool a_issued = false, ok = true;
             const int half_row = (int)rank * TC_BM;
             const int qrow0 = qpair * TC_QT + half_row;
@@ -337,8 +349,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                     j + 2 < n_my ? (a.tile_base + a.tiles.tile(u0 + j + 2)) * TP_BN + half_row
                                  : a.N;
                 for (int i = 0; i < ITEMS; ++i) {
-                    const int it = j * ITEMS + i, s = it % NST;
-                    if (it >= NST && !mbar_wait(&b_empty[s], ((it / NST) - 1) & 1)) {
+                    const int it = j * ITEMS + i, s = ps;
+                    const uint32_t ph = pph;
+                    if (++ps == NST) { ps = 0; pph ^= 1u; }
+                    if (it >= NST && !mbar_wait(&b_empty[s], ph ^ 1u)) {
                         ok = false;
                         break;
                     }
@@ -383,6 +397,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
         if (lead && lane == 0) {
             bool ok = n_my == 0 || KA == 0 || mbar_wait(a_full, 0);
             bool issued_mma = false;
+            int ms = 0;          // ring stage of the next item
+            uint32_t mph = 0;    // its phase parity
             tc_fence_after();
             const uint64_t odesc = umma_desc_sw32(sOnes);
             for (int j = 0; j < n_my && ok; ++j) {
@@ -402,8 +418,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                 umma_commit_pair_mc(&n_empty[ns], 0x3);
                 issued_mma = true;
                 for (int i = 0; i < ITEMS; ++i) {
-                    const int it = j * ITEMS + i, s = it % NST;
-                    if (!mbar_wait(&b_full[s], (it / NST) & 1) || *abort_flag) {
+                    const int s = ms;
+                    const uint32_t ph = mph;
+                    if (++ms == NST) { ms = 0; mph ^= 1u; }
+                    if (!mbar_wait(&b_full[s], ph) || *abort_flag) {
                         ok = false;
                         break;
                     }
@@ -458,9 +476,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
         PendingCands pend;
         for (int j = 0; j < n_my; ++j) {
             const int b = j & 1;
-            if (MODE == 1) pend.flush(a.count, a.cand, a.cmax, qrow);
+            const int pos = MODE == 1 ? pend.reserve(a.count, qrow) : 0;
             const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
             if (__any_sync(0xffffffffu, !got || *abort_flag != 0)) {
+                if (MODE == 1) pend.commit(pos, a.cand, a.cmax, qrow);
                 if (lane == 0) {
                     if (!got) atomicMax(a.status, (int)kDevTimeoutFull);
                     *abort_flag = 1;
@@ -487,6 +506,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                 else
                     mbar_arrive_cluster(mapa_shared(smem_u32(&acc_empty[b]), 0));
             }
+            if (MODE == 1) pend.commit(pos, a.cand, a.cmax, qrow);
             // first reference of this warp
             const int col0 = (a.tile_base + a.tiles.tile(u0 + j)) * TP_BN + hc * TP_COLS;
             const int valid = a.N - col0;
@@ -873,11 +893,13 @@ __global__ void tc_pack_f8_kernel(const float *__restrict__ x, int n, long long 
 // the sample's KS-th approximate one to certify); resets candidate counts.
 // thr_raw keeps the sample's KS-th value itself (a scan of another kind
 // re-derives its threshold from it).  Overflow prediction: a query whose
-// bound under a probe kind exceeds three times the spread of its KS sample
-// values is expected to overflow its candidate list in that kind (about
-// KS x stride points lie below T, and the band [T, T + E] adds E / (T - L_0)
-// times as many); n_wide[0] counts them for probe0 (BF16: switch to split
-// BF16), n_wide[1] for probe1 (FP8: whether an FP8 pass 2 pays).
+// bound under a probe kind exceeds the spread of its KS sample values
+// (T - L_0) is expected to overflow its candidate list in that kind: about
+// KS x stride points lie below T, and the density of points grows steeply
+// above the sample's smallest values, so a band [T, T + E] wider than
+// [L_0, T] holds many times that; n_wide[0] counts them for probe0 (BF16:
+// switch to split BF16), n_wide[1] for probe1 (FP8: whether an FP8 pass 2
+// pays).
 __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
                                     const float *__restrict__ qn,
                                     const unsigned *__restrict__ rmax_bits, TcBound bound,
@@ -906,9 +928,9 @@ __global__ void tc_threshold_kernel(const float *__restrict__ p1, int S, int Q,
     thr_raw[q] = T;
     count[q] = 0;
     if (n_wide) {
-        const float spread3 = 3.f * (T - L[0]);
-        if (tc_error_bound(qn[q], r2, T, probe0) > spread3) atomicAdd(n_wide, 1);
-        if (tc_error_bound(qn[q], r2, T, probe1) > spread3) atomicAdd(n_wide + 1, 1);
+        const float spread = T - L[0];
+        if (tc_error_bound(qn[q], r2, T, probe0) > spread) atomicAdd(n_wide, 1);
+        if (tc_error_bound(qn[q], r2, T, probe1) > spread) atomicAdd(n_wide + 1, 1);
     }
 }
 
@@ -1854,7 +1876,10 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
     if (P.timer) P.timer->mark(st, kPhaseTcPass1);
     // TP_LISTS lists (column ranges) per pair and split; resets the counts
     const bool lo_ok = kind_fits(kTcBf16x3, r.d_pad, r.d_pad8) && r.R.refBlo && r.R.state;
-    const bool probe = P.host_tmp && ((P.adaptive && lo_ok) || r.want_fp8);
+    const int force = P.force_kind;
+    const bool forced = (force == kTcBf16) || (force == kTcBf16x3 && lo_ok) ||
+                        (force == kTcFp8 && r.want_fp8);
+    const bool probe = !forced && P.host_tmp && ((P.adaptive && lo_ok) || r.want_fp8);
     if (probe && cudaMemsetAsync(r.nwide, 0, 2 * sizeof(int), st) != cudaSuccess) return kErrCuda;
     const TcBound b16 = run_bound(r, kTcBf16);
     tc_threshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
@@ -1863,10 +1888,17 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
         probe ? r.nwide : nullptr);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     r.kind = kTcBf16;
+    int wide16 = 0, wide8 = 0;
     if (probe) {
-        int wide16 = 0;
         if ((rc = read_count(r.nwide, P.host_tmp, st, wide16, 2)) != kOk) return rc;
-        const int wide8 = P.host_tmp[1];
+        wide8 = P.host_tmp[1];
+    }
+    if (forced) {
+        // the caller's kind: predicted fit or not
+        wide16 = force == kTcBf16x3 ? P.Q : 0;
+        wide8 = force == kTcFp8 ? 0 : P.Q;
+    }
+    if (probe || forced) {
         if (r.want_fp8 && 2 * wide8 <= P.Q) {
             // FP8 pass 2: thresholds T + E_bf16 + E_fp8 (the sample value
             // is a BF16 one)
@@ -1874,7 +1906,7 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
                 r.thr_raw, P.Q, r.qn, r.R.rmax_bits, run_bound(r, kTcFp8), b16, 1, r.thr);
             if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
             r.kind = kTcFp8;
-        } else if (P.adaptive && lo_ok && 2 * wide16 > P.Q) {
+        } else if ((P.adaptive || forced) && lo_ok && 2 * wide16 > P.Q) {
             // most lists expected to overflow in BF16: pass 2 runs in split
             // BF16 (thresholds re-derived from the sample)
             if ((rc = ensure_ref_lo(r, st)) != kOk) return rc;

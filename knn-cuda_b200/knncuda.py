@@ -57,7 +57,7 @@ C_SYMBOLS = (
     "knnb200_set_bound_check", "knnb200_last_bound_check", "knnb200_set_memory_cap",
     "knnb200_last_query_chunks", "knnb200_call_bytes", "knnb200_last_tc_kinds",
     "knnb200_batched_plan_create_config", "knnb200_batched_plan_config",
-    "knnb200_batched_autotune_config",
+    "knnb200_batched_autotune_config", "knnb200_set_tc_kind_override",
 )
 
 
@@ -182,6 +182,8 @@ def lib():
         L.knnb200_set_memory_cap.argtypes = [ctypes.c_size_t]
         L.knnb200_last_query_chunks.restype = ctypes.c_int
         L.knnb200_last_query_chunks.argtypes = []
+        L.knnb200_set_tc_kind_override.restype = None
+        L.knnb200_set_tc_kind_override.argtypes = [ctypes.c_int]
         L.knnb200_last_tc_kinds.restype = None
         L.knnb200_last_tc_kinds.argtypes = [_IP, _IP]
         L.knnb200_call_bytes.restype = ctypes.c_size_t
@@ -598,6 +600,13 @@ def call_bytes(ref_nb, query_nb, dim, k, method="global", host=True) -> int:
 def last_query_chunks() -> int:
     """Query chunks the last host or device call ran in."""
     return lib().knnb200_last_query_chunks()
+
+
+def set_tc_kind_override(kind) -> None:
+    """Force the tensor path's pass-2 kind ("bf16", "bf16x3", "fp8") or
+    restore the predicted choice (None).  For tests and measurements."""
+    code = {None: -1, "bf16": 0, "bf16x3": 1, "fp8": 2}[kind]
+    lib().knnb200_set_tc_kind_override(code)
 
 
 def last_tc_kinds() -> tuple:

@@ -18,9 +18,6 @@ Workloads (name: ref_nb, query_nb, dim, k, distribution, seed):
 * ``batched512`` 512 independent problems (seed 5): ref_nb log-uniform
   1k-64k, query_nb log-uniform 16-2048, dim in {3, 32, 64, 128, 256}, k
   uniform 1-64, i.i.d. U[0,1) -- ``batched_problems``.
-* ``uniform128`` 1048576, 16384, 128, 16 -- i.i.d. U[0,1)^128: distance
-  spread large against the vector norms, the data where an FP8 candidate
-  scan certifies.
 * ``serving128`` 2097152 resident points, dim 128 -- mixture of 2048
   unit-norm centres, sigma 0.1; requests of 1..1024 queries (log-uniform)
   with k in {10, 50, 100}, Poisson arrivals (query_nb / k below are the
@@ -61,7 +58,6 @@ WORKLOADS = {
     "cloud3": Workload("cloud3", 1048576, 65536, 3, 8, "uniform", 3),
     "mixture256": Workload("mixture256", 1048576, 16384, 256, 100, "mixture", 4,
                            centres=1024, sigma=0.1, centre_kind="unitnorm"),
-    "uniform128": Workload("uniform128", 1048576, 16384, 128, 16, "uniform", 7),
     "serving128": Workload("serving128", 2097152, 1024, 128, 100, "mixture", 6,
                            centres=2048, sigma=0.1, centre_kind="unitnorm"),
 }

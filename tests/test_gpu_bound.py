@@ -51,6 +51,14 @@ def _case(name):
         both = _far_clusters(31, 256, 32768 + 300, 16, 6.0, 0.05)
         return (np.ascontiguousarray(both[:, :32768]), np.ascontiguousarray(both[:, 32768:]),
                 100)
+    if name == "clusters256_d128":
+        # tight, far-apart clusters: the case where FP8 lists fit
+        rng = np.random.default_rng(81)
+        c = rng.standard_normal((128, 512))
+        c /= np.linalg.norm(c, axis=0, keepdims=True)
+        pick = rng.integers(0, 512, size=131072 + 500)
+        x = (c[:, pick] + 0.01 * rng.standard_normal((128, 131072 + 500))).astype(np.float32)
+        return np.ascontiguousarray(x[:, :131072]), np.ascontiguousarray(x[:, 131072:]), 16
     if name == "uniform1000_d128":
         rng = np.random.default_rng(38)
         return (1000 * rng.random((128, 65536), dtype=np.float32),
@@ -59,29 +67,32 @@ def _case(name):
 
 
 CASES = ["mixture256_q2048", "offset50_d64", "mixture128_q1000", "far_clusters_d256",
-         "uniform1000_d128"]
+         "uniform1000_d128", "clusters256_d128"]
+RUNS = [(name, "cublas") for name in CASES] + [("clusters256_d128", "fp8")]
 
 
-@pytest.mark.parametrize("method", ["cublas", "fp8"])
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name,method", RUNS)
 def test_observed_error_within_half_the_bound(knncuda, gpu, name, method):
     """cublas: the BF16 scan, or split BF16 where the threshold pass switches
-    to it (mixture128, the far clusters); fp8: the e4m3 scan with its own
-    bound where it runs, the BF16 path where its sample pass predicts
-    overflowing lists (uncertified queries are scanned again in BF16 and
-    checked under that bound)."""
+    to it (mixture128, the far clusters); fp8: the e4m3 scan forced on the
+    tight clusters, where its lists fit, under its own bound."""
     import torch
 
     ref, query, k = _case(name)
     r = torch.from_numpy(np.ascontiguousarray(ref, dtype=np.float32)).to(gpu)
-    x = torch.from_numpy(np.ascontiguousarray(query, dtype=np.float32)).to(gpu)
+    xq = np.ascontiguousarray(query, dtype=np.float32)
+    xb = torch.zeros((xq.shape[0], (xq.shape[1] + 3) // 4 * 4), dtype=torch.float32, device=gpu)
+    xb[:, :xq.shape[1]] = torch.from_numpy(xq)
+    x = xb[:, :xq.shape[1]]
     dg, ig = knncuda.knn_device(r, x, k, "global")
     knncuda.set_bound_check(True)
+    knncuda.set_tc_kind_override("fp8" if method == "fp8" else None)
     try:
         dc, ic = knncuda.knn_device(r, x, k, method)
         ratio, checked = knncuda.last_bound_check()
     finally:
         knncuda.set_bound_check(False)
+        knncuda.set_tc_kind_override(None)
     kinds = knncuda.last_tc_kinds()
     assert checked >= k * x.shape[1] // 2, checked
     assert ratio <= MARGIN, (name, method, kinds, ratio, checked)

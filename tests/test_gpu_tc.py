@@ -261,21 +261,55 @@ def _pitched(torch, gpu, x):
 def test_fp8_scan_equals_global_bitwise(knncuda, gpu):
     """The FP8 (e4m3, power-of-two scaled) candidate scan, certified against
     its own error bound and re-ranked exactly, returns the exact kernel's
-    answer bit for bit.  Where the sample pass predicts that FP8 lists would
-    overflow for most queries, the call runs BF16 instead (reported by the
-    scan kinds); on low-dimensional uniform data FP8 itself runs."""
+    answer bit for bit.  Pass 2 is forced to FP8 (the sample pass would
+    predict overflowing FP8 lists on uniform data and run BF16): queries
+    whose FP8 lists overflow take the second scan, the rest certify."""
     import torch
 
-    kinds = []
-    for seed, n, q, dim, k in FP8_CASES:
-        ref, query = _uniform(seed, dim, n, q)
-        r, x = _pitched(torch, gpu, ref), _pitched(torch, gpu, query)
-        dg, ig = knncuda.knn_device(r, x, k, "global")
-        df, i8 = knncuda.knn_device(r, x, k, "fp8")
-        assert knncuda.sync_status() == 0
-        kinds.append(knncuda.last_tc_kinds())
-        assert torch.equal(df, dg) and torch.equal(i8, ig), (dim, kinds[-1])
-    assert any(first == "fp8" for first, _ in kinds), kinds
+    knncuda.set_tc_kind_override("fp8")
+    try:
+        for seed, n, q, dim, k in FP8_CASES:
+            ref, query = _uniform(seed, dim, n, q)
+            r, x = _pitched(torch, gpu, ref), _pitched(torch, gpu, query)
+            dg, ig = knncuda.knn_device(r, x, k, "global")
+            df, i8 = knncuda.knn_device(r, x, k, "fp8")
+            assert knncuda.sync_status() == 0
+            assert knncuda.last_tc_kinds()[0] == "fp8", (dim, knncuda.last_tc_kinds())
+            assert torch.equal(df, dg) and torch.equal(i8, ig), dim
+    finally:
+        knncuda.set_tc_kind_override(None)
+
+
+def _clusters(seed, dim, n, centres, sigma, q):
+    """Tight clusters (about n / centres points each) around unit-norm
+    centres: distance gaps between clusters far above the FP8 bound."""
+    rng = np.random.default_rng(seed)
+    c = rng.standard_normal((dim, centres))
+    c /= np.linalg.norm(c, axis=0, keepdims=True)
+    pick = rng.integers(0, centres, size=n + q)
+    x = (c[:, pick] + sigma * rng.standard_normal((dim, n + q))).astype(np.float32)
+    return np.ascontiguousarray(x[:, :n]), np.ascontiguousarray(x[:, n:])
+
+
+def test_fp8_scan_certifies_on_tight_clusters(knncuda, gpu):
+    """Clusters of about 256 points, far apart: forced FP8 lists hold the
+    query's own cluster and certify without a second scan for most queries;
+    exact answers."""
+    import torch
+
+    ref, query = _clusters(81, 128, 131072, 512, 0.01, 500)
+    r, x = torch.from_numpy(ref).to(gpu), _pitched(torch, gpu, query)
+    dg, ig = knncuda.knn_device(r, x, 16, "global")
+    knncuda.set_tc_kind_override("fp8")
+    try:
+        df, i8 = knncuda.knn_device(r, x, 16, "fp8")
+        kinds = knncuda.last_tc_kinds()
+        second, _ = knncuda.last_fallback_counts()
+    finally:
+        knncuda.set_tc_kind_override(None)
+    assert kinds[0] == "fp8"
+    assert second <= 50, second
+    assert torch.equal(df, dg) and torch.equal(i8, ig)
 
 
 def test_fp8_request_on_headline_mixture(knncuda, gpu):
@@ -301,16 +335,19 @@ def test_split_bf16_when_bf16_would_overflow(knncuda, gpu):
     (hi + lo parts), so the exact kernel is not needed."""
     import workloads
 
+    import torch
+
     w = workloads.WORKLOADS["mixture128"]
     ref, query = workloads.generate(w, ref_nb=262144, query_nb=2000)
-    dg, ig = knncuda.knn(ref, query, w.k, "global")
-    dc, ic = knncuda.knn(ref, query, w.k, "cublas")
+    r, x = torch.from_numpy(ref).to(gpu), torch.from_numpy(query).to(gpu)
+    dg, ig = knncuda.knn_device(r, x, w.k, "global")
+    dc, ic = knncuda.knn_device(r, x, w.k, "cublas")
+    assert knncuda.sync_status() == 0
     first, second = knncuda.last_tc_kinds()
     _, exact = knncuda.last_fallback_counts()
     assert first == "bf16x3", (first, second)
     assert exact == 0
-    assert np.array_equal(dc.view(np.uint32), dg.view(np.uint32))
-    assert np.array_equal(ic, ig)
+    assert torch.equal(dc, dg) and torch.equal(ic, ig)
 
 
 @pytest.mark.parametrize("n,dim,k", [(299108, 96, 100), (1 << 20, 256, 100)])
