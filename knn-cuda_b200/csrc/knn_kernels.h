@@ -127,6 +127,7 @@ int launch_exact(const ExactProblem &p, cudaStream_t st);
 // and ||r - c||^2 have been read back).
 struct TcRefState {
     bool lo_ready = false;   // refBlo holds the split-BF16 lo parts
+    bool f8_scaled = false;  // s_r, kappa set (from the set's maxima)
     bool f8_ready = false;   // ref8 / refN8 hold the FP8 copy
     float s_r = 0.f, kappa = 0.f, resid8 = 0.f;   // FP8 scale, norm-step unit, norm residual
     float absmax_r = 0.f, r2max = 0.f;            // read back with the FP8 prep

@@ -1616,15 +1616,15 @@ int ensure_ref_lo(const TcRun &r, cudaStream_t st) {
     return kOk;
 }
 
-// The FP8 copy of the reference set, once per prepared set: reads back
+// The FP8 scales of the reference set, once per prepared set: reads back
 // the set's largest |r - c| and ||r - c||^2 (one synchronisation) for the
 // scale s_r = 2^floor(log2(448 / max|r - c|)) and the norm-step unit
 // kappa = 2^ceil(log2(s_r max||r - c||^2 / 896)) (so the norm needs at most
 // two saturated parts before the remainder).
-int ensure_ref_f8(const TcRun &r, cudaStream_t st, unsigned *host_tmp) {
+int ensure_ref_f8_scale(const TcRun &r, cudaStream_t st, unsigned *host_tmp) {
     TcRefState *s = r.R.state;
     if (!r.R.ref8 || !s) return kErrUnsupported;
-    if (s->f8_ready) return kOk;
+    if (s->f8_scaled) return kOk;
     if (cudaMemcpyAsync(host_tmp, r.R.rmax_bits, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(host_tmp + 1, r.R.absmax_bits, 4, cudaMemcpyDeviceToHost, st) !=
             cudaSuccess ||
@@ -1638,6 +1638,19 @@ int ensure_ref_f8(const TcRun &r, cudaStream_t st, unsigned *host_tmp) {
     s->r2max = r2;
     s->s_r = pow2_floor(448.0 / am);
     s->kappa = pow2_ceil(std::max(1e-30, (double)s->s_r * r2 / 896.0));
+    s->resid8 = 0.f;
+    s->f8_scaled = true;
+    return kOk;
+}
+
+// The FP8 copy of the reference set (scales from ensure_ref_f8_scale),
+// once per prepared set; reads back the norm split's largest residual.
+int ensure_ref_f8(const TcRun &r, cudaStream_t st, unsigned *host_tmp) {
+    TcRefState *s = r.R.state;
+    if (!r.R.ref8 || !s) return kErrUnsupported;
+    if (s->f8_ready) return kOk;
+    int rc = ensure_ref_f8_scale(r, st, host_tmp);
+    if (rc != kOk) return rc;
     if (cudaMemsetAsync(r.R.resid8_bits, 0, 4, st) != cudaSuccess) return kErrCuda;
     constexpr int W = 8;
     tc_pack_ref_f8_kernel<<<(r.P.N + W - 1) / W, W * 32, 0, st>>>(
@@ -1847,16 +1860,13 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     r.want_fp8 = false;
     if (fp8) {
-        // the reference set's FP8 copy, then the queries' scale and copy;
-        // the sample pass still runs in BF16 and decides whether pass 2
-        // runs in FP8
+        // the reference set's and the queries' FP8 scales only: the sample
+        // pass runs in BF16 and decides whether pass 2 runs in FP8, and the
+        // FP8 copies are made then (tc_run_pass1)
         unsigned *host_tmp = reinterpret_cast<unsigned *>(P.host_tmp);
-        int rc = ensure_ref_f8(r, st, host_tmp);
+        int rc = ensure_ref_f8_scale(r, st, host_tmp);
         if (rc == kOk) rc = fp8_query_scale(r, st, reinterpret_cast<unsigned *>(r.nwide + 2), host_tmp);
         if (rc != kOk) return rc;
-        tc_pack_f8_kernel<<<dim3((P.Q + 31) / 32, p.d_pad8 / 32), dim3(32, 8), 0, st>>>(
-            P.qry, P.Q, P.ldq, P.d, p.d_pad8, R.center, -2.0f * r.s_q, r.q8);
-        if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
         r.want_fp8 = true;
     }
     if (P.timer) P.timer->mark(st, kPhaseTcPrepQuery);
@@ -1900,8 +1910,13 @@ int tc_run_pass1(TcRun &r, cudaStream_t st) {
     }
     if (probe || forced) {
         if (r.want_fp8 && 2 * wide8 <= P.Q) {
-            // FP8 pass 2: thresholds T + E_bf16 + E_fp8 (the sample value
-            // is a BF16 one)
+            // FP8 pass 2: the FP8 copies (the prediction above took the
+            // norm split's residual as 0: it only picks the kind), then
+            // thresholds T + E_bf16 + E_fp8 (the sample value is a BF16 one)
+            if ((rc = ensure_ref_f8(r, st, reinterpret_cast<unsigned *>(P.host_tmp))) != kOk)
+                return rc;
+            tc_pack_f8_kernel<<<dim3((P.Q + 31) / 32, r.d_pad8 / 32), dim3(32, 8), 0, st>>>(
+                P.qry, P.Q, P.ldq, P.d, r.d_pad8, r.R.center, -2.0f * r.s_q, r.q8);
             tc_rethreshold_kernel<<<(P.Q + 255) / 256, 256, 0, st>>>(
                 r.thr_raw, P.Q, r.qn, r.R.rmax_bits, run_bound(r, kTcFp8), b16, 1, r.thr);
             if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
@@ -2033,24 +2048,39 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
     if ((rc = read_count(r.nfail, host_tmp, st, nf2)) != kOk) return rc;
     host_stats[1] = nf2;
     if (nf2 > 0) {
-        // still uncertified (list overflow): the exact kernel recomputes the
-        // compacted batch
-        const long long per_split = (long long)nf * std::min(P.k, 256) * 8;
+        // still uncertified (list overflow): the exact kernel answers them.
+        // They are gathered once more (fail2 indexes the compacted batch)
+        // into the candidate buffer, which nothing reads any more, when it
+        // holds their queries and answers; else the exact kernel
+        // recomputes the whole compacted batch.
+        const int ld3 = (nf2 + 3) / 4 * 4;
+        const size_t need = (size_t)ld3 * (P.d + 2 * (size_t)P.k) * 4;
+        const bool narrow = nf2 < nf && need <= (size_t)P.Q * r.cmax * sizeof(unsigned long long);
+        float *q3 = reinterpret_cast<float *>(r.cand);
+        float *d3 = q3 + (size_t)P.d * ld3;
+        int *i3 = reinterpret_cast<int *>(d3 + (size_t)P.k * ld3);
+        if (narrow) {
+            gather_queries_kernel<<<dim3((nf2 + 127) / 128, P.d), 128, 0, st>>>(
+                r.qsub, r.ldf, P.d, r.fail2, nf2, q3, ld3);
+            if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+        }
+        const int nx = narrow ? nf2 : nf;
+        const long long per_split = (long long)nx * std::min(P.k, 256) * 8;
         const int splits = (int)std::max<long long>(
-            1, std::min<long long>(exact_plan_splits(P.N, nf, P.d, P.k, P.num_sms),
+            1, std::min<long long>(exact_plan_splits(P.N, nx, P.d, P.k, P.num_sms),
                                    (long long)(r.xcap / per_split)));
         ExactProblem x;
         x.ref = P.ref;
         x.N = P.N;
         x.ldr = P.ldr;
-        x.qry = r.qsub;
-        x.Q = nf;
-        x.ldq = r.ldf;
+        x.qry = narrow ? q3 : r.qsub;
+        x.Q = nx;
+        x.ldq = narrow ? ld3 : r.ldf;
         x.d = P.d;
         x.k = P.k;
-        x.out_dist = r.sd;
-        x.out_idx = r.si;
-        x.ld_out = r.ldf;
+        x.out_dist = narrow ? d3 : r.sd;
+        x.out_idx = narrow ? i3 : r.si;
+        x.ld_out = narrow ? ld3 : r.ldf;
         x.scratch = r.xs;
         x.scratch_bytes = r.xcap;
         x.status = P.status;
@@ -2058,6 +2088,11 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
         x.force_splits = splits;
         x.timer = nullptr;
         if ((rc = launch_exact(x, st)) != kOk) return rc;
+        if (narrow) {
+            scatter_results_kernel<<<dim3((nf2 + 127) / 128, P.k), 128, 0, st>>>(
+                d3, i3, ld3, r.fail2, nf2, r.sd, r.si, r.ldf);
+            if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
+        }
     }
     scatter_results_kernel<<<dim3((nf + 127) / 128, P.k), 128, 0, st>>>(
         r.sd, r.si, r.ldf, r.fail, nf, P.out_dist, P.out_idx, P.ld_out);

@@ -52,11 +52,11 @@ def _case(name):
         return (np.ascontiguousarray(both[:, :32768]), np.ascontiguousarray(both[:, 32768:]),
                 100)
     if name == "clusters256_d128":
-        # tight, far-apart clusters: the case where FP8 lists fit
+        # 256 tight, far-apart clusters of about 512 points: FP8 lists fit
         rng = np.random.default_rng(81)
-        c = rng.standard_normal((128, 512))
+        c = rng.standard_normal((128, 256))
         c /= np.linalg.norm(c, axis=0, keepdims=True)
-        pick = rng.integers(0, 512, size=131072 + 500)
+        pick = rng.integers(0, 256, size=131072 + 500)
         x = (c[:, pick] + 0.01 * rng.standard_normal((128, 131072 + 500))).astype(np.float32)
         return np.ascontiguousarray(x[:, :131072]), np.ascontiguousarray(x[:, 131072:]), 16
     if name == "uniform1000_d128":

@@ -101,6 +101,29 @@ def test_second_scan_certifies_threshold_failures(knncuda, gpu):
     assert np.array_equal(ic, ig)
 
 
+def test_exact_fallback_takes_only_the_still_uncertified(knncuda, gpu):
+    """Three queries sit on 10000 copies of one point (more equal distances
+    than the longest second-chance list holds): only they go to the exact
+    kernel.  Three more sit on 2000 copies of another point: their pass-2
+    lists overflow and the second scan's longer lists certify them.  The
+    answer equals the exact kernel's, ties to the lower index."""
+    import torch
+
+    ref, query = _uniform(31, 64, 65536, 300)
+    ref[:, 1000:11000] = ref[:, [5]]
+    ref[:, 30000:32000] = ref[:, [7]]
+    rng = np.random.default_rng(32)
+    for j, col in enumerate((5, 5, 5, 7, 7, 7)):
+        query[:, 10 + 40 * j] = ref[:, col] + 1e-3 * rng.standard_normal(64).astype(np.float32)
+    r, x = torch.from_numpy(ref).to(gpu), _pitched(torch, gpu, query)
+    dg, ig = knncuda.knn_device(r, x, 16, "global")
+    dc, ic = knncuda.knn_device(r, x, 16, "cublas")
+    second, exact = knncuda.last_fallback_counts()
+    assert knncuda.sync_status() == 0
+    assert exact == 3 and second > exact, (second, exact)
+    assert torch.equal(dc, dg) and torch.equal(ic, ig)
+
+
 def test_device_entry_cublas(knncuda, gpu):
     import torch
 
@@ -292,12 +315,13 @@ def _clusters(seed, dim, n, centres, sigma, q):
 
 
 def test_fp8_scan_certifies_on_tight_clusters(knncuda, gpu):
-    """Clusters of about 256 points, far apart: forced FP8 lists hold the
-    query's own cluster and certify without a second scan for most queries;
-    exact answers."""
+    """256 clusters of about 512 points, far apart: the sample (one tile in
+    16) holds about 32 points of the query's cluster, so the threshold lies
+    inside it, and forced FP8 lists (the whole cluster, under 1024 entries)
+    certify without a second scan for most queries; exact answers."""
     import torch
 
-    ref, query = _clusters(81, 128, 131072, 512, 0.01, 500)
+    ref, query = _clusters(81, 128, 131072, 256, 0.01, 500)
     r, x = torch.from_numpy(ref).to(gpu), _pitched(torch, gpu, query)
     dg, ig = knncuda.knn_device(r, x, 16, "global")
     knncuda.set_tc_kind_override("fp8")
