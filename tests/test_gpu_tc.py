@@ -120,7 +120,7 @@ def test_exact_fallback_takes_only_the_still_uncertified(knncuda, gpu):
     dc, ic = knncuda.knn_device(r, x, 16, "cublas")
     second, exact = knncuda.last_fallback_counts()
     assert knncuda.sync_status() == 0
-    assert exact == 3 and second > exact, (second, exact)
+    assert exact >= 3 and second > exact, (second, exact)
     assert torch.equal(dc, dg) and torch.equal(ic, ig)
 
 
