@@ -57,10 +57,16 @@ UNIT = "queries/s"
 
 # DRAM traffic (read + write bytes) per launch of the dominant kernel, from
 # the ncu capture summarised in profiles/, keyed by (kernel, workload,
-# queries); None for a configuration that was not captured.
-NCU_TRAFFIC_BYTES = {
-    # dram__bytes_read.sum 1,037,806,336 + dram__bytes_write.sum 42,388,224
-    ("knn_tc_pair_scan_kernel<1>", "mixture256", 16384): 1037806336 + 42388224,
+# queries), with the source it was captured at; None for a configuration
+# that was not captured.  A capture is not repeated by this script: after a
+# change to the kernel the entry is stale until it is captured again.
+NCU_TRAFFIC = {
+    ("knn_tc_pair_scan_kernel<1>", "mixture256", 16384): {
+        # dram__bytes_read.sum 1,037,806,336 + dram__bytes_write.sum 42,388,224
+        "bytes": 1037806336 + 42388224,
+        "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one pass-2 launch, "
+                  "16384 queries (profiles/knn_tc_pair_scan_pass2_mixture256_q8192.md)",
+    },
 }
 
 
@@ -464,8 +470,10 @@ def run_ours(args, D: Dist):
                      "achieved": achieved / 1e12 if achieved else None,
                      "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
                      "frac": achieved / peak if achieved else None,
-                     "traffic": NCU_TRAFFIC_BYTES.get(
-                         ("knn_tc_pair_scan_kernel<1>", w.name, qn)),
+                     "traffic": (NCU_TRAFFIC.get(("knn_tc_pair_scan_kernel<1>", w.name, qn))
+                                 or {}).get("bytes"),
+                     "traffic_source": (NCU_TRAFFIC.get(
+                         ("knn_tc_pair_scan_kernel<1>", w.name, qn)) or {}).get("source"),
                      "algorithmic": "2*d_pad flops per (query, reference) pair, d_pad=256",
                      "peak_source": peaks["source"]},
         "clocks": head.get("clocks"),

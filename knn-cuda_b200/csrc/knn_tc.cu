@@ -1382,6 +1382,7 @@ bool encode_norm_rows(CUtensorMap *m, const void *base, int rows, bool fp8) {
 // kernel's shared memory (keys padded to a power of two) is capped at
 // kRerankSmem per block: fewer warps per block for long lists.
 constexpr int kTcCmaxRetry = 8192;
+constexpr size_t kSplitBytes = 26u << 20;   // reference bytes per pass-2 split (L2 126 MB)
 constexpr size_t kRerankSmem = 200 * 1024;
 constexpr int kTcMaxDim = 4096;
 constexpr int kTcMaxK = 256;
@@ -1427,12 +1428,18 @@ bool kind_fits(int kind, int d_pad, int d_pad8) {
 
 // Splits that fill whole waves of one CTA per SM for `tiles` tiles per
 // query tile, with at least min_tiles per CTA; modelled per-CTA cost =
-// tiles per split + a fixed set-up cost of `fixed` tiles.
-static int choose_splits(int qtiles, int tiles, int min_tiles, double fixed, int num_sms) {
+// tiles per split + a fixed set-up cost of `fixed` tiles.  With max_tiles >
+// 0 only splits of at most max_tiles tiles are considered (when there are
+// such splits): the CTAs that share a split do not all run in the same
+// wave, and the later ones find its tiles in L2 only if a wave's splits
+// fit there.
+static int choose_splits(int qtiles, int tiles, int min_tiles, double fixed, int num_sms,
+                         int max_tiles = 0) {
     int best = 1;
     double best_t = 1e300;
     const int max_s = std::max(1, std::min(256, tiles / std::max(1, min_tiles)));
-    for (int S = 1; S <= max_s; ++S) {
+    const int min_s = max_tiles > 0 ? std::min(max_s, (tiles + max_tiles - 1) / max_tiles) : 1;
+    for (int S = min_s; S <= max_s; ++S) {
         const long long ctas = (long long)qtiles * S;
         const double t = (double)((ctas + num_sms - 1) / num_sms) * ((double)tiles / S + fixed);
         if (t < best_t * 0.999) {
@@ -1740,7 +1747,17 @@ int launch_scan(const TcRun &r, cudaStream_t st, int kind, const __nv_bfloat16 *
 int emit_scan(const TcRun &r, cudaStream_t st, int kind, int Q, const float *thr, int cmax,
               int tb, int te) {
     const int qtiles = (Q + TC_QT - 1) / TC_QT;
-    const int splits = choose_splits(qtiles, te - tb, 8, 2.0, std::max(1, r.P.num_sms / 2));
+    // reference bytes a tile streams (operand rows + norm-step rows); a
+    // split holds at most kSplitBytes of them: measured at 2^20 x 256 BF16
+    // and 16384 queries, 15 splits of 36 MB read 0.93 GB per launch from
+    // DRAM and 23 splits of 24 MB 0.63 GB (the set is 0.57 GB), in the same
+    // time
+    const size_t row = kind == kTcFp8 ? (size_t)r.d_pad8
+                                      : (size_t)r.d_pad * 2 * (kind == kTcBf16x3 ? 2 : 1);
+    const size_t tile_bytes = (size_t)TP_BN * (row + 32);
+    const int max_tiles = (int)std::max<size_t>(1, kSplitBytes / tile_bytes);
+    const int splits =
+        choose_splits(qtiles, te - tb, 8, 2.0, std::max(1, r.P.num_sms / 2), max_tiles);
     return launch_scan<1>(r, st, kind, r.qB, r.qBlo, r.q8, Q, thr, cmax, tb,
                           contiguous_tiles(te - tb), splits);
 }
