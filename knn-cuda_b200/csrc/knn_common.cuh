@@ -96,14 +96,6 @@ KNN_DI void tma_load_2d(void *smem_dst, const CUtensorMap *map, uint64_t *bar, i
         : "memory");
 }
 
-// Prefetch a 2-D tensor box into L2 (no shared-memory destination).
-KNN_DI void tma_prefetch_l2_2d(const CUtensorMap *map, int x, int y) {
-    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
-                     reinterpret_cast<uint64_t>(map)),
-                 "r"(x), "r"(y)
-                 : "memory");
-}
-
 KNN_DI void prefetch_tensormap(const CUtensorMap *map) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }

@@ -191,6 +191,20 @@ struct TcProblem {
 struct TileRuns {
     int run, period, units;
     __host__ __device__ int tile(int u) const { return (u / run) * period + u % run; }
+    // tile(u), tile(u + 1), ... without a division per step
+    struct Iter {
+        int t, r, run, skip;
+        __host__ __device__ int operator*() const { return t; }
+        __host__ __device__ void next() {
+            if (++r == run) {
+                r = 0;
+                t += skip;
+            } else {
+                ++t;
+            }
+        }
+    };
+    __host__ __device__ Iter from(int u) const { return Iter{tile(u), u % run, run, period - run + 1}; }
     // units of the pattern among the tiles [0, t)
     __host__ __device__ int count_below(int t) const {
         return (t / period) * run + (t % period < run ? t % period : run);

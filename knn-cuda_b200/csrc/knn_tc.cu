@@ -165,7 +165,7 @@ constexpr int TP_COLS = TP_BN / (TP_EPI_WARPS / 4);   // columns per epilogue wa
 constexpr int TP_CHUNKS = TP_COLS / 32;
 constexpr int TP_THREADS = 32 * (2 + TP_EPI_WARPS);   // warp 0 TMA, warp 1 MMA, epilogue
 constexpr int TP_LISTS = TP_EPI_WARPS / 4;             // pass-1 lists per query and split
-constexpr int TP_NSLOTS = 4;
+constexpr int TP_NSLOTS = 2;          // norm-step ring slots
 
 // Operand kinds of the scan.  Every kind keeps the same epilogue: the
 // accumulator holds a (scaled for FP8) and the threshold test is the same.
@@ -181,14 +181,14 @@ enum TcKind : int {
 // ring whose stages carry an A tile and a B tile each; then the ones tile,
 // the norm-step ring and the barriers.
 constexpr int TP_TILE_BYTES = TC_BM * 128;            // 16 KB
-constexpr int TP_REGION_TILES = 12;
-constexpr int TP_MAX_RESIDENT_A = 8;                   // leaves >= 4 ring stages
+constexpr int TP_REGION_TILES = 13;
+constexpr int TP_MAX_RESIDENT_A = 8;                   // leaves >= 5 ring stages
 constexpr int TP_MAX_STAGES = TP_REGION_TILES - 1;
 constexpr int TP_NORM_BYTES = TC_BM * 32;              // 4 KB: 32-byte norm-step rows
 constexpr size_t TP_OFF_REGION = 0;
-constexpr size_t TP_OFF_ONES = (size_t)TP_REGION_TILES * TP_TILE_BYTES;   // 192 KB
+constexpr size_t TP_OFF_ONES = (size_t)TP_REGION_TILES * TP_TILE_BYTES;   // 208 KB
 constexpr size_t TP_OFF_N = TP_OFF_ONES + TP_NORM_BYTES;                   // +4 KB
-constexpr size_t TP_OFF_BAR = TP_OFF_N + (size_t)TP_NSLOTS * TP_NORM_BYTES;  // +16 KB
+constexpr size_t TP_OFF_BAR = TP_OFF_N + (size_t)TP_NSLOTS * TP_NORM_BYTES;  // +8 KB
 constexpr int TP_NBARS = 1 + 2 * TP_MAX_STAGES + 2 * TP_NSLOTS + 2 + 2 + 1;
 constexpr size_t TP_SMEM = 1024 + TP_OFF_BAR + TP_NBARS * 8 + 16;
 static_assert(TP_SMEM <= 232448, "pair scan kernel shared memory");
@@ -333,8 +333,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                 }
                 a_issued = true;
             }
-            for (int j = 0; j < n_my && ok; ++j) {
-                const int row0 = (a.tile_base + a.tiles.tile(u0 + j)) * TP_BN + half_row;
+            TileRuns::Iter tile = a.tiles.from(u0);
+            for (int j = 0; j < n_my && ok; ++j, tile.next()) {
+                const int row0 = (a.tile_base + *tile) * TP_BN + half_row;
                 const int ns = j % TP_NSLOTS;
                 if (j >= TP_NSLOTS && !mbar_wait(&n_empty[ns], ((j / TP_NSLOTS) - 1) & 1)) {
                     ok = false;
@@ -345,9 +346,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                 tma_load_2d_pair(sN + (size_t)ns * TP_NORM_BYTES, &tmN,
                                  mapa_shared(smem_u32(&n_full[ns]), 0), 0, row0);
                 n_issued = j + 1;
-                const int row_ahead =
-                    j + 2 < n_my ? (a.tile_base + a.tiles.tile(u0 + j + 2)) * TP_BN + half_row
-                                 : a.N;
                 for (int i = 0; i < ITEMS; ++i) {
                     const int it = j * ITEMS + i, s = ps;
                     const uint32_t ph = pph;
@@ -368,7 +366,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                         dst += TP_TILE_BYTES;
                     }
                     tma_load_2d_pair(dst, mb, bar, kb * kx, row0);
-                    if (row_ahead < a.N) tma_prefetch_l2_2d(mb, kb * kx, row_ahead);
                     issued = it + 1;
                 }
                 if (*abort_flag) break;
@@ -474,7 +471,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
 #pragma unroll
         for (int i = 0; i < TC_KS; ++i) L[i] = INFINITY;
         PendingCands pend;
-        for (int j = 0; j < n_my; ++j) {
+        TileRuns::Iter tile = a.tiles.from(u0);
+        for (int j = 0; j < n_my; ++j, tile.next()) {
             const int b = j & 1;
             const int pos = MODE == 1 ? pend.reserve(a.count, qrow) : 0;
             const bool got = mbar_wait(&acc_full[b], (j >> 1) & 1);
@@ -508,7 +506,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
             }
             if (MODE == 1) pend.commit(pos, a.cand, a.cmax, qrow);
             // first reference of this warp
-            const int col0 = (a.tile_base + a.tiles.tile(u0 + j)) * TP_BN + hc * TP_COLS;
+            const int col0 = (a.tile_base + *tile) * TP_BN + hc * TP_COLS;
             const int valid = a.N - col0;
 #pragma unroll
             for (int c = 0; c < TP_CHUNKS; ++c) {
