@@ -62,10 +62,10 @@ UNIT = "queries/s"
 # change to the kernel the entry is stale until it is captured again.
 NCU_TRAFFIC = {
     ("knn_tc_pair_scan_kernel<1>", "mixture256", 16384): {
-        # dram__bytes_read.sum 1,037,806,336 + dram__bytes_write.sum 42,388,224
-        "bytes": 1037806336 + 42388224,
+        # dram__bytes_read.sum 654,501,376 + dram__bytes_write.sum 41,818,880
+        "bytes": 654501376 + 41818880,
         "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one pass-2 launch, "
-                  "16384 queries (profiles/knn_tc_pair_scan_pass2_mixture256_q8192.md)",
+                  "16384 queries, 23 splits (profiles/knn_tc_pair_scan_pass2_mixture256.md)",
     },
 }
 
@@ -442,7 +442,7 @@ def run_ours(args, D: Dist):
     ex = tiers["exact_fp32"]
     ex_ms = ex["phase_ms"].get("exact_main", ex["ms_per_step"])
     fp32_peak = knncuda.measure_fp32_peak(8192)
-    ex["roofline"] = {"bound": "fp32", "kernel": "knn_exact_kernel<8,128>",
+    ex["roofline"] = {"bound": "fp32", "kernel": "knn_exact_kernel<4,128> (fused exact FP32)",
                       "achieved": 3.0 * dim * N * qn / (ex_ms * 1e-3) / 1e12,
                       "peak": fp32_peak / 1e12, "unit": "TFLOP/s",
                       "frac": 3.0 * dim * N * qn / (ex_ms * 1e-3) / fp32_peak,
