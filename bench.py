@@ -224,12 +224,12 @@ def cpu_sample_rate(ref, query, k, seconds_target: float, max_rounds: int = 1):
     rates = []
     for _ in range(max_rounds):
         t0 = time.perf_counter()
-        fn(ref, np.ascontiguousarray(query[:, :per_round]), k, threads=threads)
+        out = fn(ref, np.ascontiguousarray(query[:, :per_round]), k, threads=threads)
         rates.append(per_round / (time.perf_counter() - t0))
     desc = (f"first {per_round} queries of the workload against all {ref.shape[1]} reference "
             f"points, {threads} threads over contiguous query slices; per-query cost is "
             f"independent of the other queries, so queries/s scales to the full batch")
-    return rates, threads, desc, kind, per_round
+    return rates, threads, desc, kind, per_round, out
 
 
 # ---------------------------------------------------------------------------
@@ -485,9 +485,20 @@ def run_ours(args, D: Dist):
                                 "code/test.cpp)"},
     }
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
-        rates, threads, desc, kind, qs = cpu_sample_rate(ref, query, k, args.cpu_seconds)
+        rates, threads, desc, kind, qs, (gt_d, gt_i) = cpu_sample_rate(ref, query, k,
+                                                                        args.cpu_seconds)
         line["cpu_baseline"] = {"value": rates[0], "unit": UNIT, "cores": threads,
                                 "kind": kind, "sample": desc}
+        # the reference harness's pass rule (code/test.cpp:216-217, :256-272)
+        # on the sampled queries, against the knn_c outputs just timed
+        from oracle import oracle
+        for name, (dd, ii) in outs.items():
+            od = dd[:, :qs].cpu().numpy()
+            oi = ii[:, :qs].cpu().numpy()
+            ok, dacc, iacc = oracle.reference_criterion(od, oi, gt_d, gt_i)
+            tiers[name]["knn_c_criterion"] = {
+                "queries": int(qs), "passed": bool(ok), "dist_acc": dacc, "index_acc": iacc,
+                "max_abs_dist_diff": float(np.max(np.abs(od.astype(np.float64) - gt_d)))}
     if D.rank == 0:
         print(json.dumps(line), flush=True)
     D.close()
