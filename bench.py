@@ -474,7 +474,10 @@ def run_ours(args, D: Dist):
                                  or {}).get("bytes"),
                      "traffic_source": (NCU_TRAFFIC.get(
                          ("knn_tc_pair_scan_kernel<1>", w.name, qn)) or {}).get("source"),
-                     "algorithmic": "2*d_pad flops per (query, reference) pair, d_pad=256",
+                     "algorithmic": f"2*d_pad flops per (query, reference) pair, d_pad={d_pad}"
+                                    + (" (split BF16 issues 3 MMAs per K step: 3x this work on "
+                                       "the tensor pipe)" if head.get("scan_kinds", {}).get("pass2")
+                                       == "bf16x3" else ""),
                      "peak_source": peaks["source"]},
         "clocks": head.get("clocks"),
         "tiers": tiers,
