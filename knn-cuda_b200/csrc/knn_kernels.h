@@ -237,7 +237,7 @@ struct TcRun {
     __nv_bfloat16 *qB, *qBlo;
     unsigned char *q8;
     float *qn, *thr, *thr_raw, *retry, *retry_f, *p1, *qsub, *sd;
-    int *count, *fail, *fail2, *nfail, *si, *nwide;
+    int *count, *fail, *fail2, *nfail, *si, *nwide, *nsel;
     unsigned long long *cand_total, *cand;
     unsigned char *xs;
     size_t xcap;

@@ -715,7 +715,8 @@ __global__ void __launch_bounds__(256)
 // x itself) plus the norm-step row and the largest squared norm of
 // x - center, for the 256-point tiles tile0 + tiles.tile(u) (eight blocks
 // per tile).  A block owns 32 points and walks the dimensions in
-// 32 x 32 tiles through shared memory (coalesced on both sides); one thread
+// 32 x 32 tiles through shared memory (coalesced on both sides), the loads
+// of the next two tiles in flight meanwhile; one thread
 // per point accumulates the squared norm in increasing d with FP32 fma, the
 // order tc_norms_kernel uses.
 __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long ld, int d,
@@ -731,13 +732,14 @@ __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long
     const int p0 = (tile0 + tiles.tile((int)(blockIdx.x >> 3))) * TP_BN + (blockIdx.x & 7) * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     float s = 0.f;
-    // the next chunk's values are loaded into registers while this chunk
-    // is processed
-    float nx[4];
+    // the next two chunks' values are loaded into registers while this
+    // chunk is processed (two chunks in flight per block)
+    float nx[4], nx2[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int dd = ty + 8 * i, p = p0 + tx;
         nx[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
+        nx2[i] = (dd + 32 < d && p < n) ? x[(size_t)(dd + 32) * ld + p] : 0.f;
     }
     for (int d0 = 0; d0 < d_pad; d0 += 32) {
 #pragma unroll
@@ -746,8 +748,9 @@ __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int dd = d0 + 32 + ty + 8 * i, p = p0 + tx;
-            nx[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
+            const int dd = d0 + 64 + ty + 8 * i, p = p0 + tx;
+            nx[i] = nx2[i];
+            nx2[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
         }
         if (ty == 0) {
             const int dm = min(32, d - d0);
@@ -967,11 +970,17 @@ KNN_DI void warp_bitonic_sort(unsigned long long *keys, int P, int lane) {
     }
 }
 
-// Exact FP32 re-rank of each query's candidates + certification.
-// One warp per query (TC_RR_WARPS queries per block, no block-wide syncs).
+// Exact FP32 re-rank of each query's candidates + certification, in three
+// kernels of one warp per query: select (tc_rerank_select_kernel: the k-th
+// smallest a by radix selection, the pruning below, the kept candidates
+// compacted in place), gather (tc_rerank_gather_kernel: their exact
+// distances) and certify (tc_rerank_certify_kernel: sort, check, output).
+// The gather, which moves the bytes, then runs with nothing but its staging
+// ring and the query in shared memory, so the SM holds about twice the warps
+// (copies in flight) of one kernel that also keeps the sort keys there.
 //
-// Pruning: the candidates are first sorted by their BF16-expansion value a.
-// With a_k the k-th smallest, every candidate i of the first k has exact
+// Pruning: with a_k the k-th smallest BF16-expansion value a among the
+// candidates, every candidate i of the first k has exact
 // FP32 distance <= (a_k + ||q||^2 + E)(1 + gamma), and a candidate r has
 // exact FP32 distance >= (a_r + ||q||^2 - E)(1 - gamma) (E as for the
 // threshold, gamma the relative rounding of the FP32 distance chain).  A
@@ -979,9 +988,9 @@ KNN_DI void warp_bitonic_sort(unsigned long long *keys, int P, int lane) {
 // closer candidates and cannot be in the top-k, so only the prefix with
 // a_r <= a_k + 2 E + 2 g (|a_k| + ||q||^2 + E) (g = K 2^-22 >= 4 gamma, which
 // also absorbs the roundings of this bound) is re-ranked; the k-th exact
-// distance of that prefix is the k-th of all candidates.
+// distance of the kept candidates is the k-th of all candidates.
 //
-// The prefix is handled 32 candidates at a time, one per lane: the warp
+// The kept candidates are handled 32 at a time, one per lane: the warp
 // copies the 32 candidate rows of the FP32 point-major copy, TC_RR_DCH
 // dimensions at a time, into a padded shared tile with asynchronous 16-byte
 // copies (cp.async, several rows per instruction, coalesced), through a ring
@@ -990,7 +999,7 @@ KNN_DI void warp_bitonic_sort(unsigned long long *keys, int P, int lane) {
 // arithmetic and order, so distances are identical.  The (distance, index)
 // keys are bitonic-sorted by the warp.  One warp per block: the gather is
 // latency-bound, and single-warp blocks let the SM hold as many warps as
-// its shared memory allows (about 14 at d = 256).
+// its shared memory allows.
 //
 // An uncertified query is appended to fail_list and retry[q] receives a
 // threshold for a second scan: when it had at least k candidates, their k-th
@@ -1008,8 +1017,8 @@ constexpr int TC_RR_NBUF = 2;                 // staging buffers per warp (ring)
 constexpr int TC_RR_STRIDE = TC_RR_DCH + 4;
 constexpr int TC_RR_BUF = 32 * TC_RR_STRIDE;  // floats per staging buffer
 
-__host__ __device__ inline size_t tc_rr_warp_bytes(int d_pad, int cpow) {
-    return (size_t)d_pad * 4 + TC_RR_NBUF * TC_RR_BUF * 4 + (size_t)cpow * 8;
+__host__ __device__ inline size_t tc_rr_gather_bytes(int d_pad) {
+    return (size_t)d_pad * 4 + TC_RR_NBUF * TC_RR_BUF * 4;
 }
 
 KNN_DI void cp_async16(void *smem_dst, const void *gmem_src) {
@@ -1146,7 +1155,7 @@ KNN_DI void rr_exact_distances(unsigned long long *keys, int n, const float *__r
 // Certification from a query's k smallest exact keys (sorted; keys[k - 1]
 // the k-th): certified, the query's sqrt distances and indices are written;
 // otherwise it joins fail_list with the base threshold of a second scan
-// that certifies (see tc_rerank_kernel).  Warp-uniform.
+// that certifies (see tc_rerank_select_kernel).  Warp-uniform.
 KNN_DI void rr_certify(const unsigned long long *keys, int q, float qq, float r2, float T,
                        int d_pad, int k, const RrBounds &rb, float *__restrict__ out_dist,
                        int *__restrict__ out_idx, long long ld_out, int *fail_list, int *n_fail,
@@ -1171,69 +1180,156 @@ KNN_DI void rr_certify(const unsigned long long *keys, int q, float qq, float r2
     }
 }
 
-template <bool STAT>
-__global__ void __launch_bounds__(TC_RR_WARPS * 32)
-    tc_rerank_kernel(const float *__restrict__ refT, int d, int d_pad,
-                     const float *__restrict__ qry, long long ldq, const float *__restrict__ qn,
-                     const unsigned *__restrict__ rmax_bits, const float *__restrict__ thr,
-                     const float *__restrict__ thr_raw, RrBounds rb,
-                     const unsigned long long *__restrict__ cand, const int *__restrict__ count,
-                     int cmax, int cpow, int Q, int k, float *__restrict__ out_dist,
-                     int *__restrict__ out_idx, long long ld_out, int *__restrict__ fail_list,
-                     int *__restrict__ n_fail, float *__restrict__ retry,
-                     float *__restrict__ retry_f, unsigned long long *__restrict__ cand_total,
-                     int final_pass, unsigned *__restrict__ bound_stat) {
-    extern __shared__ unsigned char rsm[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int q = blockIdx.x * (blockDim.x >> 5) + warp;
+// Select: reject lists that cannot be re-ranked, find the k-th smallest
+// entry key (the order-preserving bits of a) by an 8-bit radix selection
+// over the list, and compact the entries with a <= the pruning limit to the
+// front of the list (in place: an entry moves only to a position already
+// read).  nsel[q] = their number, or -1 for a rejected list.
+__global__ void __launch_bounds__(32)
+    tc_rerank_select_kernel(unsigned long long *__restrict__ cand, const int *__restrict__ count,
+                            int cmax, int Q, int k, const float *__restrict__ qn,
+                            const unsigned *__restrict__ rmax_bits,
+                            const float *__restrict__ thr, const float *__restrict__ thr_raw,
+                            RrBounds rb, int d_pad, int final_pass, int *__restrict__ fail_list,
+                            int *__restrict__ n_fail, float *__restrict__ retry,
+                            float *__restrict__ retry_f,
+                            unsigned long long *__restrict__ cand_total, int *__restrict__ nsel) {
+    __shared__ unsigned hist[256];
+    const int q = blockIdx.x, lane = threadIdx.x;
     if (q >= Q) return;
-    unsigned char *mine = rsm + (size_t)warp * tc_rr_warp_bytes(d_pad, cpow);
-    float *qv = reinterpret_cast<float *>(mine);
-    float *rows = qv + d_pad;   // two staging buffers
-    unsigned long long *keys = reinterpret_cast<unsigned long long *>(rows + TC_RR_NBUF * TC_RR_BUF);
-
     const int c = count[q];
     if (lane == 0) atomicAdd(cand_total, (unsigned long long)c);
     const float qq = qn[q];
     const float r2 = __uint_as_float(*rmax_bits);
     const float T = thr[q];
     if (rr_reject_list(c, cmax, k, q, qq, r2, T, thr_raw ? thr_raw[q] : T, rb, final_pass,
-                       fail_list, n_fail, retry, retry_f, lane))
+                       fail_list, n_fail, retry, retry_f, lane)) {
+        if (lane == 0) nsel[q] = -1;
         return;
-    // candidates sorted by (a, index)
-    const unsigned long long *cq = cand + (size_t)q * cmax;
-    int P = 32;
-    while (P < c) P <<= 1;
-    for (int t = lane; t < P; t += 32) keys[t] = t < c ? cq[t] : ~0ull;
-    for (int dd = lane; dd < d_pad; dd += 32) qv[dd] = dd < d ? qry[(size_t)dd * ldq + q] : 0.f;
-    __syncwarp();
-    warp_bitonic_sort(keys, P, lane);
-    // the prefix that can still reach the top-k
-    int n_s;
-    {
-        const float ak = ord_float((uint32_t)(keys[k - 1] >> 32)) * rb.a_scale;
-        const float E = tc_error_bound(qq, r2, ak, rb.cur);
-        const float g = tc_fp32_gamma(d_pad);
-        const float lim = (ak + 2.f * E + 2.f * g * (fabsf(ak) + qq + E)) / rb.a_scale;
-        const uint32_t lim_o = ord_bits(__float_as_uint(lim));
-        int cnt = 0;
+    }
+    unsigned long long *cq = cand + (size_t)q * cmax;
+    // k-th smallest key, 8 bits per round from the top
+    uint32_t prefix = 0, hmask = 0;
+    unsigned rank = (unsigned)k;   // 1-based rank among the keys matching prefix
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = lane; i < 256; i += 32) hist[i] = 0u;
+        __syncwarp();
+        for (int t = lane; t < c; t += 32) {
+            const uint32_t key = (uint32_t)(cq[t] >> 32);
+            if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+        }
+        __syncwarp();
+        unsigned h[8], sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            h[j] = hist[8 * lane + j];
+            sum += h[j];
+        }
+        unsigned incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const unsigned excl = incl - sum;
+        const unsigned owner = __ballot_sync(0xffffffffu, excl < rank && rank <= incl);
+        const int src = __ffs(owner) - 1;
+        int bin = 0;
+        unsigned below = 0;
+        if (lane == src) {
+            unsigned run = excl;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (bin == 0 && run + h[j] >= rank) {
+                    bin = 8 * lane + j + 1;   // +1: found
+                    below = run;
+                }
+                run += h[j];
+            }
+        }
+        bin = __shfl_sync(0xffffffffu, bin, src) - 1;
+        below = __shfl_sync(0xffffffffu, below, src);
+        prefix |= (uint32_t)bin << shift;
+        hmask |= 255u << shift;
+        rank -= below;
+        __syncwarp();
+    }
+    const float ak = ord_float(prefix) * rb.a_scale;
+    const float E = tc_error_bound(qq, r2, ak, rb.cur);
+    const float g = tc_fp32_gamma(d_pad);
+    const float lim = (ak + 2.f * E + 2.f * g * (fabsf(ak) + qq + E)) / rb.a_scale;
+    const uint32_t lim_o = ord_bits(__float_as_uint(lim));
+    int kept = 0;
+    for (int t0 = 0; t0 < c; t0 += 32) {
+        const int t = t0 + lane;
+        kept += __popc(__ballot_sync(0xffffffffu, t < c && (uint32_t)(cq[t] >> 32) <= lim_o));
+    }
+    if (kept >= k) {
+        int pos0 = 0;
         for (int t0 = 0; t0 < c; t0 += 32) {
             const int t = t0 + lane;
-            const bool in = t < c && (uint32_t)(keys[t] >> 32) <= lim_o;
-            cnt += __popc(__ballot_sync(0xffffffffu, in));
+            const unsigned long long e = t < c ? cq[t] : kKeyInf;
+            const bool in = t < c && (uint32_t)(e >> 32) <= lim_o;
+            const unsigned b = __ballot_sync(0xffffffffu, in);
+            if (in) cq[pos0 + __popc(b & ((1u << lane) - 1u))] = e;
+            pos0 += __popc(b);
         }
-        n_s = max(cnt, k);   // keys are sorted, so the kept ones are a prefix
+    } else {
+        kept = c;   // not reached for finite values (lim >= a_k); keep the whole list
     }
-    rr_exact_distances<STAT>(keys, n_s, refT, d_pad, qv, rows, lane,
-                             BoundStat{qq, tc_error_bound(qq, r2, T, rb.cur), rb.a_scale,
-                                       bound_stat});
-    int P2 = 32;
-    while (P2 < n_s) P2 <<= 1;
-    for (int t = n_s + lane; t < P2; t += 32) keys[t] = kKeyInf;
+    if (lane == 0) nsel[q] = kept;
+}
+
+// Gather: exact FP32 distances of the nsel[q] selected candidates, keys
+// replaced in place by (distance, index).  Shared memory: the query and the
+// staging ring (rr_exact_distances).
+template <bool STAT>
+__global__ void __launch_bounds__(32)
+    tc_rerank_gather_kernel(const float *__restrict__ refT, int d, int d_pad,
+                            const float *__restrict__ qry, long long ldq,
+                            const float *__restrict__ qn, const unsigned *__restrict__ rmax_bits,
+                            const float *__restrict__ thr, RrBounds rb,
+                            unsigned long long *__restrict__ cand, const int *__restrict__ nsel,
+                            int cmax, int Q, unsigned *__restrict__ bound_stat) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    const int q = blockIdx.x, lane = threadIdx.x;
+    if (q >= Q) return;
+    const int n = nsel[q];
+    if (n <= 0) return;
+    float *qv = reinterpret_cast<float *>(rsm);
+    float *rows = qv + d_pad;
+    for (int dd = lane; dd < d_pad; dd += 32) qv[dd] = dd < d ? qry[(size_t)dd * ldq + q] : 0.f;
     __syncwarp();
-    warp_bitonic_sort(keys, P2, lane);
-    rr_certify(keys, q, qq, r2, T, d_pad, k, rb, out_dist, out_idx, ld_out, fail_list, n_fail,
-               retry, retry_f, lane);
+    const float qq = qn[q];
+    const float E = STAT ? tc_error_bound(qq, __uint_as_float(*rmax_bits), thr[q], rb.cur) : 0.f;
+    rr_exact_distances<STAT>(cand + (size_t)q * cmax, n, refT, d_pad, qv, rows, lane,
+                             BoundStat{qq, E, rb.a_scale, bound_stat});
+}
+
+// Certify: sort the exact keys of the selected candidates (their k-th is
+// the k-th of all candidates) and certify (rr_certify).
+__global__ void __launch_bounds__(32)
+    tc_rerank_certify_kernel(const unsigned long long *__restrict__ cand,
+                             const int *__restrict__ nsel, int cmax, int Q, int k, int d_pad,
+                             const float *__restrict__ qn, const unsigned *__restrict__ rmax_bits,
+                             const float *__restrict__ thr, RrBounds rb,
+                             float *__restrict__ out_dist, int *__restrict__ out_idx,
+                             long long ld_out, int *__restrict__ fail_list,
+                             int *__restrict__ n_fail, float *__restrict__ retry,
+                             float *__restrict__ retry_f) {
+    extern __shared__ unsigned long long keys[];
+    const int q = blockIdx.x, lane = threadIdx.x;
+    if (q >= Q) return;
+    const int n = nsel[q];
+    if (n < 0) return;
+    const unsigned long long *cq = cand + (size_t)q * cmax;
+    int P = 32;
+    while (P < n) P <<= 1;
+    for (int t = lane; t < P; t += 32) keys[t] = t < n ? cq[t] : kKeyInf;
+    __syncwarp();
+    warp_bitonic_sort(keys, P, lane);
+    rr_certify(keys, q, qn[q], __uint_as_float(*rmax_bits), thr[q], d_pad, k, rb, out_dist,
+               out_idx, ld_out, fail_list, n_fail, retry, retry_f, lane);
 }
 
 // Incremental re-rank for a reference set that arrives in pieces (the
@@ -1242,11 +1338,11 @@ __global__ void __launch_bounds__(TC_RR_WARPS * 32)
 // their exact FP32 distances and are merged into its running k smallest
 // keys run[q][0..k) (a sort of the new keys, then every key placed at its
 // index plus its rank in the other array).  Nothing is pruned -- the k-th a
-// is not known yet -- so about twice the rows of tc_rerank_kernel are
-// gathered, while the rest of the set is still being copied in.  After the
-// last piece run[q] holds the k smallest exact keys of all candidates: the
-// certification and the output are those of tc_rerank_kernel.  One warp
-// (block) per query.
+// is not known yet -- so about twice the rows of the select and gather
+// kernels are gathered, while the rest of the set is still being copied in.
+// After the last piece run[q] holds the k smallest exact keys of all
+// candidates: the certification and the output are those of
+// tc_rerank_certify_kernel.  One warp (block) per query.
 template <int KCAP>
 __global__ void __launch_bounds__(32)
     tc_rerank_piece_kernel(const float *__restrict__ refT, int d, int d_pad,
@@ -1279,9 +1375,9 @@ __global__ void __launch_bounds__(32)
     if (lane == 0) done[q] = c;
 }
 
-// Certification after the last piece: tc_rerank_kernel's first-pass checks
-// on the running k smallest keys of tc_rerank_piece_kernel.  One warp per
-// query.
+// Certification after the last piece: the first-pass checks of
+// tc_rerank_select_kernel and tc_rerank_certify_kernel on the running k
+// smallest keys of tc_rerank_piece_kernel.  One warp per query.
 __global__ void tc_certify_pieces_kernel(const int *__restrict__ count, int cmax,
                                          const float *__restrict__ qn,
                                          const unsigned *__restrict__ rmax_bits,
@@ -1544,7 +1640,7 @@ static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
 size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     const TcPlan p = plan_tc(N, Q, d, k, num_sms);
     const size_t rows = (size_t)p.qtiles * TC_QT;
-    size_t b = rows * p.d_pad * 2 * 2 + rows * p.d_pad8 + (size_t)Q * 4 * 8 + 64;
+    size_t b = rows * p.d_pad * 2 * 2 + rows * p.d_pad8 + (size_t)Q * 4 * 9 + 64;
     b += (size_t)TP_LISTS * p.splits1 * Q * TC_KS * 4;
     b += (size_t)Q * p.cmax * 8;
     b += fallback_bytes(N, Q, d, k, num_sms);   // worst case: every query uncertified
@@ -1765,33 +1861,39 @@ TcBound run_bound(const TcRun &r, int kind) {
     return bound_of(kind, r.P.d, r.d_pad, r.d_pad8, r.s_q, s ? s->s_r : 1.f, s ? s->resid8 : 0.f);
 }
 
-// Exact re-rank + certification of Q queries (see tc_rerank_kernel) whose
-// candidate lists (from a scan of `kind`) have stride cmax.
+// Exact re-rank + certification of Q queries (tc_rerank_select_kernel,
+// tc_rerank_gather_kernel, tc_rerank_certify_kernel) whose candidate lists
+// (from a scan of `kind`) have stride cmax.
 int rerank(const TcRun &r, cudaStream_t st, int kind, int Q, int cmax, const float *qry,
            long long ldq, const float *qn, const float *thr, const float *thr_raw,
            float *out_dist, int *out_idx, long long ld_out, int *fail, bool final_pass) {
     const TcProblem &P = r.P;
     if (cudaMemsetAsync(r.nfail, 0, 2 * sizeof(int), st) != cudaSuccess) return kErrCuda;
-    int cpow = 1;
+    int cpow = 32;
     while (cpow < cmax) cpow <<= 1;
-    int warps = TC_RR_WARPS;
-    while (warps > 1 && (size_t)warps * tc_rr_warp_bytes(r.d_pad, cpow) > kRerankSmem) warps >>= 1;
-    const size_t rsmem = (size_t)warps * tc_rr_warp_bytes(r.d_pad, cpow);
+    const size_t gsmem = tc_rr_gather_bytes(r.d_pad);
+    const size_t csmem = (size_t)cpow * 8;
     RrBounds rb;
     rb.cur = run_bound(r, kind);
     rb.a_scale = kind == kTcFp8 ? 1.f / r.scale : 1.f;
     // the bound statistic runs in its own instantiation, only when asked for
-    auto kern = P.bound_stat ? tc_rerank_kernel<true> : tc_rerank_kernel<false>;
+    auto gather = P.bound_stat ? tc_rerank_gather_kernel<true> : tc_rerank_gather_kernel<false>;
     // one fixed limit for every launch, so that calls from several host
     // threads never lower it under each other
-    if (rsmem > kRerankSmem ||
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (gsmem > kRerankSmem || csmem > kRerankSmem ||
+        cudaFuncSetAttribute(gather, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kRerankSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(tc_rerank_certify_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kRerankSmem) != cudaSuccess)
         return kErrLaunch;
-    kern<<<(Q + warps - 1) / warps, warps * 32, rsmem, st>>>(
-        r.R.refT, P.d, r.d_pad, qry, ldq, qn, r.R.rmax_bits, thr, thr_raw, rb, r.cand, r.count,
-        cmax, cpow, Q, P.k, out_dist, out_idx, ld_out, fail, r.nfail, r.retry, r.retry_f,
-        r.cand_total, final_pass ? 1 : 0, P.bound_stat);
+    tc_rerank_select_kernel<<<Q, 32, 0, st>>>(r.cand, r.count, cmax, Q, P.k, qn, r.R.rmax_bits,
+                                              thr, thr_raw, rb, r.d_pad, final_pass ? 1 : 0, fail,
+                                              r.nfail, r.retry, r.retry_f, r.cand_total, r.nsel);
+    gather<<<Q, 32, gsmem, st>>>(r.R.refT, P.d, r.d_pad, qry, ldq, qn, r.R.rmax_bits, thr, rb,
+                                 r.cand, r.nsel, cmax, Q, P.bound_stat);
+    tc_rerank_certify_kernel<<<Q, 32, csmem, st>>>(r.cand, r.nsel, cmax, Q, P.k, r.d_pad, qn,
+                                                   r.R.rmax_bits, thr, rb, out_dist, out_idx,
+                                                   ld_out, fail, r.nfail, r.retry, r.retry_f);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
@@ -1849,6 +1951,7 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     r.count = cv.take<int>(P.Q);
     r.fail = cv.take<int>(P.Q);
     r.fail2 = cv.take<int>(P.Q);
+    r.nsel = cv.take<int>(P.Q);
     r.nfail = cv.take<int>(4);
     r.nwide = cv.take<int>(4);   // [0] predicted overflows, [2] query max |q - c| bits
     r.cand_total = cv.take<unsigned long long>(1);
