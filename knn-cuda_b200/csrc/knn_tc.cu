@@ -715,8 +715,7 @@ __global__ void __launch_bounds__(256)
 // x itself) plus the norm-step row and the largest squared norm of
 // x - center, for the 256-point tiles tile0 + tiles.tile(u) (eight blocks
 // per tile).  A block owns 32 points and walks the dimensions in
-// 32 x 32 tiles through shared memory (coalesced on both sides), the loads
-// of the next two tiles in flight meanwhile; one thread
+// 32 x 32 tiles through shared memory (coalesced on both sides); one thread
 // per point accumulates the squared norm in increasing d with FP32 fma, the
 // order tc_norms_kernel uses.
 __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long ld, int d,
@@ -732,14 +731,13 @@ __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long
     const int p0 = (tile0 + tiles.tile((int)(blockIdx.x >> 3))) * TP_BN + (blockIdx.x & 7) * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     float s = 0.f;
-    // the next two chunks' values are loaded into registers while this
-    // chunk is processed (two chunks in flight per block)
-    float nx[4], nx2[4];
+    // the next chunk's values are loaded into registers while this chunk
+    // is processed
+    float nx[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int dd = ty + 8 * i, p = p0 + tx;
         nx[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
-        nx2[i] = (dd + 32 < d && p < n) ? x[(size_t)(dd + 32) * ld + p] : 0.f;
     }
     for (int d0 = 0; d0 < d_pad; d0 += 32) {
 #pragma unroll
@@ -748,9 +746,8 @@ __global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int dd = d0 + 64 + ty + 8 * i, p = p0 + tx;
-            nx[i] = nx2[i];
-            nx2[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
+            const int dd = d0 + 32 + ty + 8 * i, p = p0 + tx;
+            nx[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
         }
         if (ty == 0) {
             const int dm = min(32, d - d0);
