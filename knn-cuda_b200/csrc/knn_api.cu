@@ -20,6 +20,10 @@
 #include <thread>
 #include <vector>
 
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
+
 #include <cudaTypedefs.h>
 
 #include "../../include/knn_b200.h"
@@ -165,6 +169,33 @@ class HostPool {
 // buffers; the host gathers a piece of the reference set into one while the
 // other's copy is in flight.
 constexpr size_t kStageBytes = 32u << 20;
+
+// count floats from src to a 16-byte aligned dst with non-temporal stores:
+// the staging buffer is read next by the copy engine, not by this core, so
+// the stores skip the read-for-ownership of a cached write (with the copy
+// engine reading the buffer meanwhile, the host's memory bandwidth is what
+// bounds the gather).
+static void stage_row(float *dst, const float *src, size_t count) {
+#if defined(__SSE2__)
+    if ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+        size_t i = 0;
+        for (; i + 16 <= count; i += 16) {
+            const __m128i a = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i));
+            const __m128i b = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i + 4));
+            const __m128i c = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i + 8));
+            const __m128i d = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i + 12));
+            _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i), a);
+            _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 4), b);
+            _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 8), c);
+            _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 12), d);
+        }
+        if (i < count) std::memcpy(dst + i, src + i, (count - i) * sizeof(float));
+        _mm_sfence();   // the stores are visible before the copy is queued
+        return;
+    }
+#endif
+    std::memcpy(dst, src, count * sizeof(float));
+}
 
 // Host entry of knn_cublas on large sets: the reference set is copied in
 // this many chunks (after the sample runs of the threshold pass), each
@@ -364,7 +395,7 @@ int enqueue_tc_streamed(Workspace &ws, const ExactProblem &p, const float *ref_h
             if (cudaEventSynchronize(ws.stage_done[slot]) != cudaSuccess) return kErrCuda;
             float *dst = ws.stage[slot];
             const std::function<void(int)> rows = [&](int dd) {
-                std::memcpy(dst + (size_t)dd * n, ref_host + (size_t)dd * p.N + q0, n * fb);
+                stage_row(dst + (size_t)dd * n, ref_host + (size_t)dd * p.N + q0, n);
             };
             ws.pool->run(p.d, rows);
             if (cudaMemcpy2DAsync(ref_d + q0, (size_t)p.ldr * fb, dst, n * fb, n * fb, p.d,
