@@ -354,7 +354,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                         ok = false;
                         break;
                     }
-                    if (*abort_flag) break;
                     if (lead) mbar_arrive_expect_tx(&b_full[s], 2 * stage_bytes);
                     const uint32_t bar = mapa_shared(smem_u32(&b_full[s]), 0);
                     unsigned char *dst = stage_ptr(s);
@@ -398,6 +397,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
             uint32_t mph = 0;    // its phase parity
             tc_fence_after();
             const uint64_t odesc = umma_desc_sw32(sOnes);
+            // descriptors advance by the operand offset in 16-byte units
+            const uint64_t a_desc0 = umma_desc_sw128(sR);
+            const uint64_t s_desc0 = umma_desc_sw128(stage_ptr(0));
+            constexpr uint64_t kTileDesc = TP_TILE_BYTES >> 4;
             for (int j = 0; j < n_my && ok; ++j) {
                 const int b = j & 1;
                 const uint32_t acc = tmem + (uint32_t)(b * TP_BN);
@@ -418,30 +421,29 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                     const int s = ms;
                     const uint32_t ph = mph;
                     if (++ms == NST) { ms = 0; mph ^= 1u; }
-                    if (!mbar_wait(&b_full[s], ph) || *abort_flag) {
+                    // (an abort elsewhere ends this wait by its time limit)
+                    if (!mbar_wait(&b_full[s], ph)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const unsigned char *st = stage_ptr(s);
-                    const uint64_t bdesc = umma_desc_sw128(st + (streamed ? TP_TILE_BYTES : 0));
+                    const uint64_t sdesc = s_desc0 + (uint64_t)(s * stage_tiles) * kTileDesc;
+                    const uint64_t bdesc = sdesc + (streamed ? kTileDesc : 0);
                     if (streamed) {
-                        tp_mma_block<KIND>(acc, umma_desc_sw128(st), bdesc);
+                        tp_mma_block<KIND>(acc, sdesc, bdesc);
                     } else if (KIND == kTcBf16x3) {
                         const int kb = i >> 1;
-                        const uint64_t ahi = umma_desc_sw128(sR + (size_t)kb * TP_TILE_BYTES);
+                        const uint64_t ahi = a_desc0 + (uint64_t)kb * kTileDesc;
                         if ((i & 1) == 0) {
                             // B hi: A hi . B hi + A lo . B hi
                             tp_mma_block<KIND>(acc, ahi, bdesc);
-                            tp_mma_block<KIND>(
-                                acc, umma_desc_sw128(sR + (size_t)(KB + kb) * TP_TILE_BYTES),
-                                bdesc);
+                            tp_mma_block<KIND>(acc, a_desc0 + (uint64_t)(KB + kb) * kTileDesc,
+                                               bdesc);
                         } else {
                             tp_mma_block<KIND>(acc, ahi, bdesc);   // A hi . B lo
                         }
                     } else {
-                        tp_mma_block<KIND>(acc, umma_desc_sw128(sR + (size_t)i * TP_TILE_BYTES),
-                                           bdesc);
+                        tp_mma_block<KIND>(acc, a_desc0 + (uint64_t)i * kTileDesc, bdesc);
                     }
                     umma_commit_pair_mc(&b_empty[s], 0x3);
                 }
