@@ -334,6 +334,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                 a_issued = true;
             }
             TileRuns::Iter tile = a.tiles.from(u0);
+            // the even CTA's full barriers (shared::cluster addresses) and
+            // the ring's first stage; stage s is 8 B and s stage_bytes on
+            const uint32_t bfull0 = mapa_shared(smem_u32(&b_full[0]), 0);
+            unsigned char *const stage0 = stage_ptr(0);
             for (int j = 0; j < n_my && ok; ++j, tile.next()) {
                 const int row0 = (a.tile_base + *tile) * TP_BN + half_row;
                 const int ns = j % TP_NSLOTS;
@@ -355,8 +359,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                         break;
                     }
                     if (lead) mbar_arrive_expect_tx(&b_full[s], 2 * stage_bytes);
-                    const uint32_t bar = mapa_shared(smem_u32(&b_full[s]), 0);
-                    unsigned char *dst = stage_ptr(s);
+                    const uint32_t bar = bfull0 + 8u * (uint32_t)s;
+                    unsigned char *dst = stage0 + (size_t)s * stage_bytes;
                     // split BF16: items alternate hi, lo of K block i / 2
                     const int kb = KIND == kTcBf16x3 ? (i >> 1) : i;
                     const CUtensorMap *mb = (KIND == kTcBf16x3 && (i & 1)) ? &tmB2 : &tmB;
