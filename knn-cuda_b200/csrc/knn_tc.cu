@@ -536,9 +536,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TP_THREADS, 1)
                     } else {
                         const float x = __uint_as_float(xb);
                         if (x < L[TC_KS - 1]) {
+                            // sorted insertion: L[i] becomes the median of
+                            // L[i - 1], x, L[i] (no NaN reaches here)
 #pragma unroll
                             for (int i = TC_KS - 1; i > 0; --i)
-                                L[i] = x < L[i - 1] ? L[i - 1] : (x < L[i] ? x : L[i]);
+                                L[i] = fmaxf(L[i - 1], fminf(x, L[i]));
                             L[0] = fminf(L[0], x);
                         }
                     }
@@ -2070,8 +2072,11 @@ int tc_run_rerank_piece(TcRun &r, cudaStream_t st) {
     const TcProblem &P = r.P;
     if (!r.pieces) {
         // the running lists take the exact-fallback scratch, which nothing
-        // uses before the certification; without room the full re-rank
-        // runs in tc_run_finish instead
+        // uses before the certification.  tc_scratch_bytes sizes that
+        // scratch for the fallback's query copy (d * Q floats) and result
+        // keys (k * Q), so Q * k keys plus Q flags always fit; the check
+        // only guards a caller-sized scratch, for which the full re-rank
+        // then runs in tc_run_finish instead
         Carve cv{r.xs, 0, r.xcap};
         unsigned long long *keys = cv.take<unsigned long long>((size_t)P.Q * P.k);
         int *done = cv.take<int>(P.Q);
