@@ -50,6 +50,15 @@ class Workload:
             d.update(centres=self.centres, sigma=self.sigma, centre_kind=self.centre_kind)
         return d
 
+    def data_text(self) -> str:
+        """One line naming the synthetic distribution of this workload."""
+        if self.dist == "mixture":
+            kind = {"unitnorm": "unit-norm", "uniform11": "U[-1,1]^d"}.get(self.centre_kind,
+                                                                          self.centre_kind)
+            return (f"synthetic (seeded Gaussian mixture, {self.centres} {kind} centres, "
+                    f"sigma {self.sigma})")
+        return "synthetic (seeded i.i.d. U[0,1))"
+
 
 WORKLOADS = {
     "readme": Workload("readme", 16384, 4096, 128, 16, "uniform", 1),
