@@ -721,76 +721,95 @@ __global__ void __launch_bounds__(256)
 // Reference-set prep in one pass over the input: point-major BF16 and FP32
 // copies (zero-padded to d_pad; the BF16 one of x - center, the FP32 one of
 // x itself) plus the norm-step row and the largest squared norm of
-// x - center, for the 256-point tiles tile0 + tiles.tile(u) (eight blocks
-// per tile).  A block owns 32 points and walks the dimensions in
-// 32 x 32 tiles through shared memory (coalesced on both sides); one thread
-// per point accumulates the squared norm in increasing d with FP32 fma, the
-// order tc_norms_kernel uses.
-__global__ void tc_prep_ref_kernel(const float *__restrict__ x, int n, long long ld, int d,
-                                   int d_pad, int tile0, TileRuns tiles,
-                                   const float *__restrict__ center,
-                                   __nv_bfloat16 *__restrict__ xb, float *__restrict__ xt,
-                                   __nv_bfloat16 *__restrict__ parts,
-                                   unsigned *__restrict__ max_bits,
-                                   unsigned *__restrict__ absmax_bits) {
-    __shared__ float tile[32][33];
-    __shared__ float cs[32];   // the chunk's translation
-    float am = 0.f;            // largest |x - c| this thread wrote
-    const int p0 = (tile0 + tiles.tile((int)(blockIdx.x >> 3))) * TP_BN + (blockIdx.x & 7) * 32;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    float s = 0.f;
-    // the next chunk's values are loaded into registers while this chunk
-    // is processed
-    float nx[4];
+// x - center, for the 256-point tiles tile0 + tiles.tile(u) (two blocks of
+// four warps per tile).  A warp owns 32 points (one per lane) and walks the
+// dimensions in chunks of 32: each lane loads its point's 32 values of the
+// chunk (coalesced rows, the next chunk's loads in flight meanwhile),
+// accumulates its squared norm in increasing d with FP32 fma (the order
+// tc_norms_kernel uses), and the chunk is transposed through a padded
+// shared tile so that every store writes four points' 128-byte rows.
+constexpr int TC_PREP_WARPS = 4;
+constexpr int TC_PREP_LD = 36;   // floats per point row of the transpose tile
+__global__ void __launch_bounds__(32 * TC_PREP_WARPS)
+    tc_prep_ref_kernel(const float *__restrict__ x, int n, long long ld, int d, int d_pad,
+                       int tile0, TileRuns tiles, const float *__restrict__ center,
+                       __nv_bfloat16 *__restrict__ xb, float *__restrict__ xt,
+                       __nv_bfloat16 *__restrict__ parts, unsigned *__restrict__ max_bits,
+                       unsigned *__restrict__ absmax_bits) {
+    __shared__ __align__(16) float tile_all[TC_PREP_WARPS][32 * TC_PREP_LD];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *tt = tile_all[warp];
+    const int p0 = (tile0 + tiles.tile((int)(blockIdx.x >> 1))) * TP_BN +
+                   (int)(blockIdx.x & 1) * (TP_BN / 2) + warp * 32;
+    const int p = p0 + lane;       // this lane's point (loads, norm)
+    const bool pin = p < n;
+    float s = 0.f;                 // squared norm of x_p - c
+    float am = 0.f;                // largest |x - c| this lane wrote
+    float cur[32], nxt[32];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int dd = ty + 8 * i, p = p0 + tx;
-        nx[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
-    }
+    for (int j = 0; j < 32; ++j) cur[j] = (j < d && pin) ? x[(size_t)j * ld + p] : 0.f;
+    // write-out roles: 8 rounds of 4 points, lane -> point 4 r + lane / 8,
+    // dimensions 4 (lane % 8) .. + 3
+    const int wp = lane >> 3, wm = lane & 7;
     for (int d0 = 0; d0 < d_pad; d0 += 32) {
+        if (d0 + 32 < d_pad) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) tile[ty + 8 * i][tx] = nx[i];
-        if (ty == 1) cs[tx] = d0 + tx < d ? center[d0 + tx] : 0.f;
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int dd = d0 + 32 + ty + 8 * i, p = p0 + tx;
-            nx[i] = (dd < d && p < n) ? x[(size_t)dd * ld + p] : 0.f;
+            for (int j = 0; j < 32; ++j) {
+                const int dd = d0 + 32 + j;
+                nxt[j] = (dd < d && pin) ? x[(size_t)dd * ld + p] : 0.f;
+            }
         }
-        if (ty == 0) {
-            const int dm = min(32, d - d0);
-            for (int dd = 0; dd < dm; ++dd) {
-                const float v = tile[dd][tx] - cs[dd];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            if (d0 + j < d) {
+                const float v = cur[j] - __ldg(center + d0 + j);
                 s = fmaf(v, v, s);
             }
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int p = p0 + ty + 8 * i, dd = d0 + tx;
-            if (p < n) {
-                const float v = tile[tx][ty + 8 * i];
-                const float y = dd < d ? v - cs[tx] : 0.f;
-                xb[(size_t)p * d_pad + dd] = __float2bfloat16_rn(y);
-                xt[(size_t)p * d_pad + dd] = v;
-                am = fmaxf(am, fabsf(y));
+        for (int m = 0; m < 8; ++m)
+            *reinterpret_cast<float4 *>(tt + lane * TC_PREP_LD + 4 * m) =
+                make_float4(cur[4 * m], cur[4 * m + 1], cur[4 * m + 2], cur[4 * m + 3]);
+        __syncwarp();
+        const int dd = d0 + 4 * wm;
+        float c4[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) c4[e] = dd + e < d ? __ldg(center + dd + e) : 0.f;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int pp = 4 * r + wp, q = p0 + pp;
+            const float4 v = *reinterpret_cast<const float4 *>(tt + pp * TC_PREP_LD + 4 * wm);
+            if (q < n) {
+                const float ve[4] = {v.x, v.y, v.z, v.w};
+                __nv_bfloat16 yb[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const float y = dd + e < d ? ve[e] - c4[e] : 0.f;
+                    yb[e] = __float2bfloat16_rn(y);
+                    am = fmaxf(am, fabsf(y));
+                }
+                *reinterpret_cast<float4 *>(xt + (size_t)q * d_pad + dd) = v;
+                *reinterpret_cast<uint2 *>(xb + (size_t)q * d_pad + dd) =
+                    *reinterpret_cast<const uint2 *>(yb);
             }
         }
-        __syncthreads();
+        __syncwarp();
+        if (d0 + 32 < d_pad) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) cur[j] = nxt[j];
+        }
     }
     {
         unsigned ma = __float_as_uint(am);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) ma = max(ma, __shfl_xor_sync(0xffffffffu, ma, o));
-        if (tx == 0) atomicMax(absmax_bits, ma);
+        if (lane == 0) atomicMax(absmax_bits, ma);
     }
-    if (ty == 0) {
-        const int p = p0 + tx;
-        if (p < n) write_norm_row(parts, p, s);
-        unsigned m = p < n ? __float_as_uint(s) : 0u;
+    if (pin) write_norm_row(parts, p, s);
+    unsigned m = pin ? __float_as_uint(s) : 0u;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if (tx == 0) atomicMax(max_bits, m);
-    }
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) atomicMax(max_bits, m);
 }
 
 // Lo parts of split BF16 for the whole prepared set: from the FP32
@@ -1677,7 +1696,7 @@ int tc_prepare_ref_tiles(const TcRefView &v, const float *ref, int N, long long 
     if (tiles.units <= 0) return kOk;
     if (tiles.run < 1 || tiles.period < tiles.run) return kErrInvalid;
     const int d_pad = (d + 63) / 64 * 64;
-    tc_prep_ref_kernel<<<tiles.units * 8, dim3(32, 8), 0, st>>>(
+    tc_prep_ref_kernel<<<tiles.units * 2, 32 * TC_PREP_WARPS, 0, st>>>(
         ref, N, ldr, d, d_pad, tile0, tiles, v.center, v.refB, v.refT, v.refN, v.rmax_bits,
         v.absmax_bits);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
