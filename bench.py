@@ -442,9 +442,11 @@ def run_ours(args, D: Dist):
     achieved = flops / (pass2_ms * 1e-3) if pass2_ms else None
     peak = peaks["bf16_tflops"] * 1e12
     fb = head["uncertified_queries_per_step"]
-    # prep 4 + pass 1 + threshold + pass 2 + re-rank; second scan 7 more;
-    # exact fallback 2 more (fused kernel + split merge)
-    launches = 8 + (7 if fb["second_scan"] > 0 else 0) + (2 if fb["exact"] > 0 else 0)
+    # reference prep 3 (center, prep, sample rows) + query prep 2 + pass 1 +
+    # threshold + pass 2 + re-rank 3 (select, gather, certify); second scan
+    # 7 more; exact fallback 5 more (gather, query copy, fused kernel, split
+    # merge, scatter)
+    launches = 11 + (7 if fb["second_scan"] > 0 else 0) + (5 if fb["exact"] > 0 else 0)
     ex = tiers["exact_fp32"]
     ex_ms = ex["phase_ms"].get("exact_main", ex["ms_per_step"])
     fp32_peak = knncuda.measure_fp32_peak(8192)

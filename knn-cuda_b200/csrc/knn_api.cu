@@ -328,6 +328,7 @@ int enqueue(Workspace &ws, const ExactProblem &p0, int method, cudaStream_t st,
     t.timer = &ws.timer;
     t.request = (method == KNNB200_METHOD_FP8 && tc_fp8_supported(p.d)) ? kTcReqFp8 : kTcReqBf16;
     t.force_kind = g_force_kind;
+    t.point_sample = true;   // the whole set is prepared before pass 1
     if (ws.bound_check) {
         if (cudaMemsetAsync(ws.bound.ptr, 0, 16, st) != cudaSuccess) return kErrCuda;
         t.bound_stat = static_cast<unsigned *>(ws.bound.ptr);

@@ -145,6 +145,11 @@ struct TcRefView {
     __nv_bfloat16 *refBlo;  // [N][d_pad] split-BF16 lo parts (prepared when first needed)
     unsigned char *ref8;    // [N][d_pad8] FP8 e4m3 of s_r (r - c) (prepared when first needed)
     unsigned char *refN8;   // [N][32] FP8 norm-step parts
+    // every TC_SAMPLE_EVERY-th point's BF16 row and norm-step row
+    // ([ceil(N / TC_SAMPLE_EVERY)][d_pad] and [..][16]), written by the
+    // preparation: the threshold sample of a set prepared as a whole
+    __nv_bfloat16 *sampB;
+    __nv_bfloat16 *sampN;
     TcRefState *state;      // host-side flags and scales
 };
 
@@ -182,6 +187,11 @@ struct TcProblem {
     // pass-2 kind forced regardless of the overflow prediction (-1: none;
     // a kind that does not fit the shape is ignored); tests and benchmarks
     int force_kind = -1;
+    // the threshold sample is every (16 m)-th point of the prepared set
+    // (TcRefView::sampB, whole set prepared before pass 1) rather than runs
+    // of tiles (a set still streaming in): a sample spread over every part
+    // of the set, whatever its order
+    bool point_sample = false;
 };
 
 // A sample of the 256-point tiles: `run` consecutive tiles out of every
@@ -229,6 +239,7 @@ struct TcRun {
     TcProblem P;
     TcRefView R;
     TileRuns sample;
+    int p1_rows, p1_every;  // point sample: rows scanned by pass 1, in units of 16 points
     int d_pad, d_pad8, qtiles, n_tiles2, splits1, cmax;
     int kind;               // kind of the first scan's pass 2 (TcKind in knn_tc.cu)
     bool want_fp8;          // FP8 requested: pass 2 in FP8 if predicted to fit

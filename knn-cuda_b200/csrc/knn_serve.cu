@@ -148,6 +148,7 @@ int run_refset(knnb200_refset *rs, Slot &slot, const float *query, int Q, long l
         t.timer = nullptr;
         t.request = (method == KNNB200_METHOD_FP8 && tc_fp8_supported(rs->d)) ? kTcReqFp8
                                                                              : kTcReqBf16;
+        t.point_sample = true;   // the resident set was prepared as a whole
         return launch_tc(t, rs->tc, st, slot.host_stats);
     }
     ExactProblem p;

@@ -64,6 +64,7 @@ constexpr int TC_QT = 2 * TC_BM;      // queries per CTA pair
 constexpr int TC_BK = 64;             // K block: 64 bf16 = 128 B (one swizzle row)
 constexpr int TC_NK = 16;             // norm step: K = 16 (h, m, l, 13 zeros)
 constexpr int TC_KS = 16;             // pass-1 per-row list length
+constexpr int TC_SAMPLE_EVERY = 16;   // point sample: every 16th point (pass 1 takes every m-th of those)
 constexpr uint32_t TC_TMEM_COLS = 512;   // 2 accumulator buffers x 256 columns
 constexpr int kCenterStride = 64;     // the translation is the mean of every 64th tile
 
@@ -812,6 +813,24 @@ __global__ void __launch_bounds__(32 * TC_PREP_WARPS)
     if (lane == 0) atomicMax(max_bits, m);
 }
 
+// The threshold sample of a prepared set: the BF16 row and the norm-step row
+// of every TC_SAMPLE_EVERY-th point, copied into compact arrays (16-byte
+// words; one warp per row).
+__global__ void tc_sample_rows_kernel(const __nv_bfloat16 *__restrict__ xb,
+                                      const __nv_bfloat16 *__restrict__ parts, int ns,
+                                      int d_pad, __nv_bfloat16 *__restrict__ sb,
+                                      __nv_bfloat16 *__restrict__ sparts) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= ns) return;
+    const size_t p = (size_t)row * TC_SAMPLE_EVERY;
+    const uint4 *src = reinterpret_cast<const uint4 *>(xb + p * d_pad);
+    uint4 *dst = reinterpret_cast<uint4 *>(sb + (size_t)row * d_pad);
+    for (int w = lane; w < d_pad / 8; w += 32) dst[w] = src[w];
+    if (lane < TC_NK / 8)
+        reinterpret_cast<uint4 *>(sparts + (size_t)row * TC_NK)[lane] =
+            reinterpret_cast<const uint4 *>(parts + p * TC_NK)[lane];
+}
+
 // Lo parts of split BF16 for the whole prepared set: from the FP32
 // point-major copy r and the translation c, lo = bf16(y - bf16(y)) with
 // y = r - c computed as tc_prep_ref_kernel computes it (so hi + lo splits
@@ -1509,6 +1528,8 @@ struct TcPlan {
     int d_pad, d_pad8, qtiles, cmax;
     int n_tiles2, splits1;   // 256-point tiles; pass-1 splits over CTA pairs
     TileRuns sample;         // pass-1 tiles
+    int p1_rows, p1_every;   // point sample: pass 1 scans rows 0, m, 2m, ... of
+                             // the every-16th-point copy (p1_every = m; 0: tile runs)
 };
 
 // Operand feed of one scan kind: K blocks of 128 bytes per operand row,
@@ -1568,7 +1589,7 @@ static int choose_splits(int qtiles, int tiles, int min_tiles, double fixed, int
     return best;
 }
 
-TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
+TcPlan plan_tc(int N, int Q, int d, int k, int num_sms, bool point_sample = false) {
     TcPlan p;
     p.d_pad = (d + 63) / 64 * 64;
     p.d_pad8 = (d + 127) / 128 * 128;
@@ -1584,6 +1605,16 @@ TcPlan plan_tc(int N, int Q, int d, int k, int num_sms) {
     p.sample.run = run;
     p.sample.period = run * stride;
     p.sample.units = p.sample.count_below(p.n_tiles2);
+    p.p1_rows = p.p1_every = 0;
+    if (point_sample) {
+        // every (16 m)-th point, 16 m >= stride: rows 0, m, 2m, ... of the
+        // every-16th-point copy, scanned as contiguous 256-row tiles
+        const int m = (stride + TC_SAMPLE_EVERY - 1) / TC_SAMPLE_EVERY;
+        const int ns = (N + TC_SAMPLE_EVERY - 1) / TC_SAMPLE_EVERY;
+        p.p1_every = m;
+        p.p1_rows = (ns + m - 1) / m;
+        p.sample = contiguous_tiles((p.p1_rows + TP_BN - 1) / TP_BN);
+    }
     // coarser pass-1 splits amortise each pair's set-up (query tile load,
     // TMEM allocation, pipeline fill)
     p.splits1 = choose_splits(p.qtiles, p.sample.units, 16, 8.0, std::max(1, num_sms / 2));
@@ -1651,8 +1682,9 @@ size_t tc_ref_bytes(int N, int d) {
     const int d_pad = (d + 63) / 64 * 64, d_pad8 = (d + 127) / 128 * 128;
     const size_t lo = kind_fits(kTcBf16x3, d_pad, d_pad8) ? (size_t)N * d_pad * 2 : 0;
     const size_t f8 = kind_fits(kTcFp8, d_pad, d_pad8) ? (size_t)N * d_pad8 + (size_t)N * 32 : 0;
+    const size_t ns = (size_t)(N + TC_SAMPLE_EVERY - 1) / TC_SAMPLE_EVERY;
     return (size_t)N * d_pad * 2 + (size_t)N * d_pad * 4 + (size_t)N * TC_NK * 2 +
-           (size_t)d_pad * 4 + lo + f8 + 12 * 256;
+           (size_t)d_pad * 4 + lo + f8 + ns * (d_pad + TC_NK) * 2 + 14 * 256;
 }
 
 static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
@@ -1662,7 +1694,9 @@ static size_t fallback_bytes(int N, int Q, int d, int k, int num_sms) {
 }
 
 size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
-    const TcPlan p = plan_tc(N, Q, d, k, num_sms);
+    TcPlan p = plan_tc(N, Q, d, k, num_sms);
+    // the point sample's pass 1 may choose other splits: room for either
+    p.splits1 = std::max(p.splits1, plan_tc(N, Q, d, k, num_sms, true).splits1);
     const size_t rows = (size_t)p.qtiles * TC_QT;
     size_t b = rows * p.d_pad * 2 * 2 + rows * p.d_pad8 + (size_t)Q * 4 * 9 + 64;
     b += (size_t)TP_LISTS * p.splits1 * Q * TC_KS * 4;
@@ -1676,10 +1710,16 @@ int tc_prepare_ref(const TcRefView &v, const float *ref, int N, long long ldr, i
     if (cudaMemsetAsync(v.rmax_bits, 0, 3 * 256, st) != cudaSuccess) return kErrCuda;
     if (v.state) *v.state = TcRefState{};
     const int n_tiles = (N + TP_BN - 1) / TP_BN;
-    const int rc = tc_center_from_tiles(v, ref, N, ldr, d, contiguous_tiles(n_tiles),
-                                        kCenterStride, st);
-    return rc != kOk ? rc
-                     : tc_prepare_ref_tiles(v, ref, N, ldr, d, 0, contiguous_tiles(n_tiles), st);
+    int rc = tc_center_from_tiles(v, ref, N, ldr, d, contiguous_tiles(n_tiles), kCenterStride,
+                                  st);
+    if (rc == kOk) rc = tc_prepare_ref_tiles(v, ref, N, ldr, d, 0, contiguous_tiles(n_tiles), st);
+    if (rc != kOk || !v.sampB || !v.sampN) return rc;
+    // the point sample of pass 1: every 16th point's rows
+    const int ns = (N + TC_SAMPLE_EVERY - 1) / TC_SAMPLE_EVERY;
+    const int d_pad = (d + 63) / 64 * 64;
+    tc_sample_rows_kernel<<<(ns + 7) / 8, 256, 0, st>>>(v.refB, v.refN, ns, d_pad, v.sampB,
+                                                        v.sampN);
+    return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
 int tc_center_from_tiles(const TcRefView &v, const float *ref, int N, long long ldr, int d,
@@ -1721,6 +1761,9 @@ TcRefView tc_carve_ref(void *mem, int N, int d, TcRefState *state) {
     const bool f8 = kind_fits(kTcFp8, d_pad, d_pad8);
     v.ref8 = f8 ? cv.take<unsigned char>((size_t)N * d_pad8) : nullptr;
     v.refN8 = f8 ? cv.take<unsigned char>((size_t)N * 32) : nullptr;
+    const size_t ns = (size_t)(N + TC_SAMPLE_EVERY - 1) / TC_SAMPLE_EVERY;
+    v.sampB = cv.take<__nv_bfloat16>(ns * d_pad);
+    v.sampN = cv.take<__nv_bfloat16>(ns * TC_NK);
     v.state = state;
     if (state) *state = TcRefState{};
     return v;
@@ -1809,6 +1852,17 @@ int launch_scan(const TcRun &r, cudaStream_t st, int kind, const __nv_bfloat16 *
              encode_norm_rows(&tmN, r.R.refN8, P.N, true);
         tmA2 = tmA;
         tmB2 = tmB;
+    } else if (MODE == 0 && r.p1_every > 0) {
+        // the point sample: rows 0, m, 2m, ... of the every-16th-point copy
+        ok = encode_bf16_kmajor(&tmA, qB, Q, r.d_pad) &&
+             encode_2d(&tmB, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, r.R.sampB, (uint64_t)r.d_pad,
+                       (uint64_t)r.p1_rows, (uint64_t)r.p1_every * r.d_pad, TC_BK, TC_BM,
+                       CU_TENSOR_MAP_SWIZZLE_128B) &&
+             encode_2d(&tmN, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, r.R.sampN, (uint64_t)TC_NK,
+                       (uint64_t)r.p1_rows, (uint64_t)r.p1_every * TC_NK, TC_NK, TC_BM,
+                       CU_TENSOR_MAP_SWIZZLE_32B);
+        tmA2 = tmA;
+        tmB2 = tmB;
     } else {
         ok = encode_bf16_kmajor(&tmA, qB, Q, r.d_pad) &&
              encode_bf16_kmajor(&tmB, r.R.refB, P.N, r.d_pad) &&
@@ -1823,7 +1877,7 @@ int launch_scan(const TcRun &r, cudaStream_t st, int kind, const __nv_bfloat16 *
     }
     if (!ok) return kErrTensorMap;
     TpArgs a;
-    a.N = P.N;
+    a.N = (MODE == 0 && r.p1_every > 0) ? r.p1_rows : P.N;
     a.Q = Q;
     a.kb = op.kb;
     a.ka = op.ka;
@@ -1947,9 +2001,12 @@ TileRuns tc_sample_runs(int N, int Q, int d, int k, int num_sms) {
 
 int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun &r) {
     if (!tc_supported(P.N, P.Q, P.d, P.k)) return kErrUnsupported;
-    const TcPlan p = plan_tc(P.N, P.Q, P.d, P.k, P.num_sms);
+    const bool points = P.point_sample && R.sampB && R.sampN;
+    const TcPlan p = plan_tc(P.N, P.Q, P.d, P.k, P.num_sms, points);
     r.P = P;
     r.R = R;
+    r.p1_rows = p.p1_rows;
+    r.p1_every = p.p1_every;
     r.d_pad = p.d_pad;
     r.d_pad8 = p.d_pad8;
     r.qtiles = p.qtiles;

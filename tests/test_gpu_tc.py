@@ -137,6 +137,46 @@ def test_device_entry_cublas(knncuda, gpu):
     assert np.array_equal(i.cpu().numpy(), hi)
 
 
+def _unit_clusters(seed, dim, n, q, centres, sigma, sort):
+    """Unit-norm centres plus N(0, sigma^2) noise; with sort, the reference
+    points are stored cluster by cluster (each cluster's points contiguous)."""
+    rng = np.random.default_rng(seed)
+    c = rng.standard_normal((dim, centres)).astype(np.float32)
+    c /= np.linalg.norm(c, axis=0, keepdims=True)
+    pick = rng.integers(0, centres, size=n)
+    if sort:
+        pick = np.sort(pick)
+    ref = c[:, pick] + np.float32(sigma) * rng.standard_normal((dim, n), dtype=np.float32)
+    qry = c[:, rng.integers(0, centres, size=q)] + np.float32(sigma) * rng.standard_normal(
+        (dim, q), dtype=np.float32)
+    return np.ascontiguousarray(ref, dtype=np.float32), np.ascontiguousarray(qry, dtype=np.float32)
+
+
+def test_threshold_sample_spans_a_cluster_sorted_set(knncuda, gpu):
+    """A reference set stored cluster by cluster gets thresholds as good as
+    the same kind of set in random order: the threshold sample of a set
+    prepared as a whole is every 16th point, spread over all clusters, not
+    runs of consecutive tiles (which would see a few clusters only and make
+    every list of the other clusters' queries overflow).  The answers are
+    knn_cuda_global's, bit for bit."""
+    import torch
+
+    n, q, dim, k = 131072, 512, 64, 32
+    stats = {}
+    for sort in (False, True):
+        ref, query = _unit_clusters(31, dim, n, q, 128, 0.1, sort)
+        r = torch.from_numpy(ref).to(gpu)
+        qq = torch.from_numpy(query).to(gpu)
+        dg, ig = knncuda.knn_device(r, qq, k, "global")
+        dc, ic = knncuda.knn_device(r, qq, k, "cublas")
+        st = knncuda.last_tc_stats()
+        assert torch.equal(dc, dg) and torch.equal(ic, ig)
+        stats[sort] = st
+    assert stats[True]["exact"] == 0, stats
+    assert stats[True]["second_scan"] <= stats[False]["second_scan"] + q // 50, stats
+    assert stats[True]["candidates"] <= 1.5 * stats[False]["candidates"], stats
+
+
 def _far_clusters(seed, dim, n, centres, radius, sigma):
     """Tight clusters around centres in random directions at distance radius
     from the origin: the set's mean is near 0, so translating it does not
