@@ -247,7 +247,7 @@ struct TcRun {
     long long ldf;
     __nv_bfloat16 *qB, *qBlo;
     unsigned char *q8;
-    float *qn, *thr, *thr_raw, *retry, *retry_f, *p1, *qsub, *sd;
+    float *qn, *thr, *thr_raw, *retry, *retry_f, *retry_s, *p1, *qsub, *sd;
     int *count, *fail, *fail2, *nfail, *si, *nwide, *nsel;
     unsigned long long *cand_total, *cand;
     unsigned char *xs;

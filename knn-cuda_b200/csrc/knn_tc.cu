@@ -1091,13 +1091,24 @@ struct RrBounds {
 // A query that fails leaves the threshold of its second scan as a base
 // value and a factor: thr = base + f E_q(base) under the bound of the kind
 // the second scan uses (chosen once the failures are counted; f = 0: base
-// is the threshold, NaN: exact kernel).  Overflowing lists count in n_fail[1].
-KNN_DI bool rr_reject_list(int c, int cmax, int k, int q, float qq, float r2, float T,
-                           float T_raw, const RrBounds &rb, int final_pass, int *fail_list,
-                           int *n_fail, float *retry, float *retry_f, int lane) {
-    if (c <= cmax && c >= k) return false;
+// is the threshold, NaN: exact kernel), and optionally a "sure" base s:
+// then thr = min(that, s + 2.5 E_q(s)).  Overflowing lists count in
+// n_fail[1].
+//
+// Returns 0 for a list to re-rank and certify, 1 for a list rejected here,
+// 2 for an overflowing list of the first scan: its cmax entries are
+// re-ranked all the same, and their k-th exact distance D -- not below the
+// true k-th, since they are genuine points -- gives the sure base
+// D (1 + g) - ||q||^2 (rr_certify), which keeps every point of the exact
+// top-k below the second scan's threshold and certifies it there.
+KNN_DI int rr_reject_list(int c, int cmax, int k, int q, float qq, float r2, float T,
+                          float T_raw, const RrBounds &rb, int final_pass, int *fail_list,
+                          int *n_fail, float *retry, float *retry_f, float *retry_s,
+                          int lane) {
+    if (c <= cmax && c >= k) return 0;
     if (lane == 0) {
         fail_list[atomicAdd(n_fail, 1)] = q;
+        retry_s[q] = INFINITY;
         if (c < k) {
             retry[q] = T + 8.f * tc_error_bound(qq, r2, T, rb.cur);
             retry_f[q] = 0.f;
@@ -1107,7 +1118,7 @@ KNN_DI bool rr_reject_list(int c, int cmax, int k, int q, float qq, float r2, fl
             retry_f[q] = final_pass ? 0.f : 1.f;
         }
     }
-    return true;
+    return (c > cmax && !final_pass) ? 2 : 1;
 }
 // Exact FP32 distances of the candidates keys[0..n) (point index in the low
 // 32 bits), in place: keys[t] = (distance, index).  One warp, 32 candidates
@@ -1202,17 +1213,25 @@ KNN_DI void rr_exact_distances(unsigned long long *keys, int n, const float *__r
 KNN_DI void rr_certify(const unsigned long long *keys, int q, float qq, float r2, float T,
                        int d_pad, int k, const RrBounds &rb, float *__restrict__ out_dist,
                        int *__restrict__ out_idx, long long ld_out, int *fail_list, int *n_fail,
-                       float *retry, float *retry_f, int lane) {
+                       float *retry, float *retry_f, float *retry_s, bool overflow, int lane) {
     int failed = 0;
     if (lane == 0) {
         const float dk = key_dist2(keys[k - 1]);
         const float E = tc_error_bound(qq, r2, T, rb.cur);
         const float dkg = dk * (1.f + (float)d_pad * 2.384185791015625e-07f);
-        failed = !(dkg + E < T + qq);
-        if (failed) {
-            fail_list[atomicAdd(n_fail, 1)] = q;
-            retry[q] = dkg - qq;
-            retry_f[q] = 2.5f;
+        if (overflow) {
+            // an overflowing list (already counted as a failure): the sure
+            // base from its entries' k-th exact distance
+            retry_s[q] = dkg - qq;
+            failed = 1;
+        } else {
+            failed = !(dkg + E < T + qq);
+            if (failed) {
+                fail_list[atomicAdd(n_fail, 1)] = q;
+                retry[q] = dkg - qq;
+                retry_f[q] = 2.5f;
+                retry_s[q] = INFINITY;
+            }
         }
     }
     if (__shfl_sync(0xffffffffu, failed, 0)) return;
@@ -1235,21 +1254,23 @@ __global__ void __launch_bounds__(32)
                             const float *__restrict__ thr, const float *__restrict__ thr_raw,
                             RrBounds rb, int d_pad, int final_pass, int *__restrict__ fail_list,
                             int *__restrict__ n_fail, float *__restrict__ retry,
-                            float *__restrict__ retry_f,
+                            float *__restrict__ retry_f, float *__restrict__ retry_s,
                             unsigned long long *__restrict__ cand_total, int *__restrict__ nsel) {
     __shared__ unsigned hist[256];
     const int q = blockIdx.x, lane = threadIdx.x;
     if (q >= Q) return;
-    const int c = count[q];
+    int c = count[q];
     if (lane == 0) atomicAdd(cand_total, (unsigned long long)c);
     const float qq = qn[q];
     const float r2 = __uint_as_float(*rmax_bits);
     const float T = thr[q];
-    if (rr_reject_list(c, cmax, k, q, qq, r2, T, thr_raw ? thr_raw[q] : T, rb, final_pass,
-                       fail_list, n_fail, retry, retry_f, lane)) {
+    const int rj = rr_reject_list(c, cmax, k, q, qq, r2, T, thr_raw ? thr_raw[q] : T, rb,
+                                  final_pass, fail_list, n_fail, retry, retry_f, retry_s, lane);
+    if (rj == 1) {
         if (lane == 0) nsel[q] = -1;
         return;
     }
+    if (rj == 2) c = cmax;   // the entries that were kept
     unsigned long long *cq = cand + (size_t)q * cmax;
     // k-th smallest key, 8 bits per round from the top
     uint32_t prefix = 0, hmask = 0;
@@ -1353,13 +1374,14 @@ __global__ void __launch_bounds__(32)
 // the k-th of all candidates) and certify (rr_certify).
 __global__ void __launch_bounds__(32)
     tc_rerank_certify_kernel(const unsigned long long *__restrict__ cand,
-                             const int *__restrict__ nsel, int cmax, int Q, int k, int d_pad,
+                             const int *__restrict__ nsel, const int *__restrict__ count,
+                             int cmax, int Q, int k, int d_pad,
                              const float *__restrict__ qn, const unsigned *__restrict__ rmax_bits,
                              const float *__restrict__ thr, RrBounds rb,
                              float *__restrict__ out_dist, int *__restrict__ out_idx,
                              long long ld_out, int *__restrict__ fail_list,
                              int *__restrict__ n_fail, float *__restrict__ retry,
-                             float *__restrict__ retry_f) {
+                             float *__restrict__ retry_f, float *__restrict__ retry_s) {
     extern __shared__ unsigned long long keys[];
     const int q = blockIdx.x, lane = threadIdx.x;
     if (q >= Q) return;
@@ -1372,7 +1394,8 @@ __global__ void __launch_bounds__(32)
     __syncwarp();
     warp_bitonic_sort(keys, P, lane);
     rr_certify(keys, q, qn[q], __uint_as_float(*rmax_bits), thr[q], d_pad, k, rb, out_dist,
-               out_idx, ld_out, fail_list, n_fail, retry, retry_f, lane);
+               out_idx, ld_out, fail_list, n_fail, retry, retry_f, retry_s, count[q] > cmax,
+               lane);
 }
 
 // Incremental re-rank for a reference set that arrives in pieces (the
@@ -1431,6 +1454,7 @@ __global__ void tc_certify_pieces_kernel(const int *__restrict__ count, int cmax
                                          int *__restrict__ out_idx, long long ld_out,
                                          int *__restrict__ fail_list, int *__restrict__ n_fail,
                                          float *__restrict__ retry, float *__restrict__ retry_f,
+                                         float *__restrict__ retry_s,
                                          unsigned long long *__restrict__ cand_total) {
     const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (q >= Q) return;
@@ -1439,11 +1463,13 @@ __global__ void tc_certify_pieces_kernel(const int *__restrict__ count, int cmax
     const float qq = qn[q];
     const float r2 = __uint_as_float(*rmax_bits);
     const float T = thr[q];
-    if (rr_reject_list(c, cmax, k, q, qq, r2, T, thr_raw[q], rb, 0, fail_list, n_fail, retry,
-                       retry_f, lane))
-        return;
+    const int rj = rr_reject_list(c, cmax, k, q, qq, r2, T, thr_raw[q], rb, 0, fail_list,
+                                  n_fail, retry, retry_f, retry_s, lane);
+    if (rj == 1) return;
+    // run holds the k smallest exact keys of the list's entries (all of
+    // them, or the cmax kept of an overflowing list)
     rr_certify(run + (size_t)q * k, q, qq, r2, T, d_pad, k, rb, out_dist, out_idx, ld_out,
-               fail_list, n_fail, retry, retry_f, lane);
+               fail_list, n_fail, retry, retry_f, retry_s, rj == 2, lane);
 }
 
 // Fallback plumbing: gather the uncertified queries into a dense d x m set
@@ -1474,15 +1500,17 @@ __global__ void scatter_results_kernel(const float *__restrict__ sd, const int *
 __global__ void tc_retry_prep_kernel(const int *__restrict__ list, int m,
                                      const float *__restrict__ retry,
                                      const float *__restrict__ retry_f,
+                                     const float *__restrict__ retry_s,
                                      const float *__restrict__ qn,
                                      const unsigned *__restrict__ rmax_bits, TcBound bound,
                                      float *__restrict__ thr, int *__restrict__ count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m) {
-        const float base = retry[list[i]], f = retry_f[list[i]];
-        thr[i] = f == 0.f ? base
-                          : base + f * tc_error_bound(qn[i], __uint_as_float(*rmax_bits), base,
-                                                      bound);
+        const float r2 = __uint_as_float(*rmax_bits);
+        const float base = retry[list[i]], f = retry_f[list[i]], sure = retry_s[list[i]];
+        float t = f == 0.f ? base : base + f * tc_error_bound(qn[i], r2, base, bound);
+        if (isfinite(sure)) t = fminf(t, sure + 2.5f * tc_error_bound(qn[i], r2, sure, bound));
+        thr[i] = t;
         count[i] = 0;
     }
 }
@@ -1698,7 +1726,7 @@ size_t tc_scratch_bytes(int N, int Q, int d, int k, int num_sms) {
     // the point sample's pass 1 may choose other splits: room for either
     p.splits1 = std::max(p.splits1, plan_tc(N, Q, d, k, num_sms, true).splits1);
     const size_t rows = (size_t)p.qtiles * TC_QT;
-    size_t b = rows * p.d_pad * 2 * 2 + rows * p.d_pad8 + (size_t)Q * 4 * 9 + 64;
+    size_t b = rows * p.d_pad * 2 * 2 + rows * p.d_pad8 + (size_t)Q * 4 * 10 + 64;
     b += (size_t)TP_LISTS * p.splits1 * Q * TC_KS * 4;
     b += (size_t)Q * p.cmax * 8;
     b += fallback_bytes(N, Q, d, k, num_sms);   // worst case: every query uncertified
@@ -1966,12 +1994,14 @@ int rerank(const TcRun &r, cudaStream_t st, int kind, int Q, int cmax, const flo
         return kErrLaunch;
     tc_rerank_select_kernel<<<Q, 32, 0, st>>>(r.cand, r.count, cmax, Q, P.k, qn, r.R.rmax_bits,
                                               thr, thr_raw, rb, r.d_pad, final_pass ? 1 : 0, fail,
-                                              r.nfail, r.retry, r.retry_f, r.cand_total, r.nsel);
+                                              r.nfail, r.retry, r.retry_f, r.retry_s, r.cand_total,
+                                              r.nsel);
     gather<<<Q, 32, gsmem, st>>>(r.R.refT, P.d, r.d_pad, qry, ldq, qn, r.R.rmax_bits, thr, rb,
                                  r.cand, r.nsel, cmax, Q, P.bound_stat);
-    tc_rerank_certify_kernel<<<Q, 32, csmem, st>>>(r.cand, r.nsel, cmax, Q, P.k, r.d_pad, qn,
-                                                   r.R.rmax_bits, thr, rb, out_dist, out_idx,
-                                                   ld_out, fail, r.nfail, r.retry, r.retry_f);
+    tc_rerank_certify_kernel<<<Q, 32, csmem, st>>>(r.cand, r.nsel, r.count, cmax, Q, P.k,
+                                                   r.d_pad, qn, r.R.rmax_bits, thr, rb, out_dist,
+                                                   out_idx, ld_out, fail, r.nfail, r.retry,
+                                                   r.retry_f, r.retry_s);
     return cudaGetLastError() == cudaSuccess ? kOk : kErrLaunch;
 }
 
@@ -2029,6 +2059,7 @@ int tc_run_begin(const TcProblem &P, const TcRefView &R, cudaStream_t st, TcRun 
     r.thr_raw = cv.take<float>(P.Q);
     r.retry = cv.take<float>(P.Q);
     r.retry_f = cv.take<float>(P.Q);
+    r.retry_s = cv.take<float>(P.Q);
     r.count = cv.take<int>(P.Q);
     r.fail = cv.take<int>(P.Q);
     r.fail2 = cv.take<int>(P.Q);
@@ -2201,7 +2232,7 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
         tc_certify_pieces_kernel<<<(P.Q + W - 1) / W, W * 32, 0, st>>>(
             r.count, r.cmax, r.qn, r.R.rmax_bits, r.thr, r.thr_raw, rb, r.run_keys, P.Q, P.k,
             r.d_pad, P.out_dist, P.out_idx, P.ld_out, r.fail, r.nfail, r.retry, r.retry_f,
-            r.cand_total);
+            r.retry_s, r.cand_total);
         if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     } else {
         rc = rerank(r, st, r.kind, P.Q, r.cmax, P.qry, P.ldq, r.qn, r.thr, r.thr_raw, P.out_dist,
@@ -2235,7 +2266,8 @@ int tc_run_finish(TcRun &r, cudaStream_t st, int *host_stats) {
         r.qsub, nf, r.ldf, P.d, r.d_pad, r.R.center, -2.0f, r.qB,
         kind2 == kTcBf16x3 ? r.qBlo : nullptr);
     tc_retry_prep_kernel<<<(nf + 255) / 256, 256, 0, st>>>(
-        r.fail, nf, r.retry, r.retry_f, r.qn, r.R.rmax_bits, run_bound(r, kind2), r.thr, r.count);
+        r.fail, nf, r.retry, r.retry_f, r.retry_s, r.qn, r.R.rmax_bits, run_bound(r, kind2), r.thr,
+        r.count);
     if (cudaGetLastError() != cudaSuccess) return kErrLaunch;
     // the compacted queries share the whole list buffer (Q * cmax entries)
     const int cmax2 = (int)std::min<long long>(

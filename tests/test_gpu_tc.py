@@ -177,6 +177,30 @@ def test_threshold_sample_spans_a_cluster_sorted_set(knncuda, gpu):
     assert stats[True]["candidates"] <= 1.5 * stats[False]["candidates"], stats
 
 
+def test_streamed_cluster_sorted_set_needs_no_exact_fallback(knncuda, gpu):
+    """knn_cublas from page-locked host buffers samples runs of tiles (pass 1
+    starts before the set has arrived), so on a set stored cluster by
+    cluster most queries' lists overflow.  The k-th exact distance of the
+    entries an overflowing list kept bounds the true k-th from above, so the
+    second scan gets thresholds that certify: no query goes to the exact
+    kernel, and the answers are knn_cuda_global's bit for bit."""
+    import torch
+
+    n, q, dim, k = 262144, 512, 64, 32
+    ref, query = _unit_clusters(7, dim, n, q, 256, 0.1, True)
+    ref_p = torch.from_numpy(ref).pin_memory().numpy()
+    qry_p = torch.from_numpy(query).pin_memory().numpy()
+    d = torch.empty((k, q), dtype=torch.float32).pin_memory().numpy()
+    i = torch.empty((k, q), dtype=torch.int32).pin_memory().numpy()
+    assert knncuda.knn_cublas(ref_p, n, qry_p, q, dim, k, d, i)
+    second, exact = knncuda.last_fallback_counts()
+    dg, ig = np.empty((k, q), np.float32), np.empty((k, q), np.int32)
+    assert knncuda.knn_cuda_global(ref, n, query, q, dim, k, dg, ig)
+    assert np.array_equal(d.view(np.uint32), dg.view(np.uint32))
+    assert np.array_equal(i, ig)
+    assert second > 0 and exact == 0, (second, exact)
+
+
 def _far_clusters(seed, dim, n, centres, radius, sigma):
     """Tight clusters around centres in random directions at distance radius
     from the origin: the set's mean is near 0, so translating it does not
