@@ -237,11 +237,12 @@ KNN_DI bool consume_ref_tile(f32x2_t (&acc)[QPW][4], const float *stages, uint64
     for (int dc = 0; dc < n_dchunks; ++dc, ++it) {
         const int s = it % EX_STAGES;
         const bool got = mbar_wait(&full[s], (it / EX_STAGES) & 1);
-        // warp-uniform decision: every lane leaves together or none does
-        const bool timed_out = __any_sync(0xffffffffu, !got);
-        if (timed_out || __any_sync(0xffffffffu, *abort_flag != 0)) {
+        // warp-uniform decision: every lane leaves together or none does.
+        // No per-stage check of the abort flag: when another warp gives up,
+        // the producer stops refilling and this wait ends by its time limit.
+        if (__any_sync(0xffffffffu, !got)) {
             if (lane == 0) {
-                if (timed_out) atomicMax(status, (int)kDevTimeoutFull);
+                atomicMax(status, (int)kDevTimeoutFull);
                 *abort_flag = 1;
             }
             return false;
